@@ -1,0 +1,349 @@
+#!/usr/bin/env python3
+"""Benchmark of the MPMEngine substep on B200 (one JSON line on rank 0).
+
+Workload (default): the 1,000,000-particle Drucker-Prager slope over a 256^3
+terrain SDF (seeded synthetic scene; APIC, dt = 2e-5).  One bench "step" is one
+MPMEngine::step call of ``--substeps`` substeps.  ``value`` is the whole-job
+particle-substeps/s with the state resident in HBM, timed by CUDA events on the
+engine's stream (max over ranks); ``e2e`` is the same metric through the C ABI
+with the particle state copied host->device before and device->host after every
+step.  ``--impl reference`` times the reference's algorithm on the host cores
+(the CPU oracle, which restates the reference shaders) on the same workload.
+
+Multi-GPU: the single scene does not shard; each rank runs a replica
+(weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-substeps/sec/GPU, plain vs batched; adjoint step time; % of HBM peak"
+UNIT = "particle-substeps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nebula", choices=["nebula", "reference"])
+    ap.add_argument("--workload", default="slope", choices=["slope", "elastic", "multimaterial"])
+    ap.add_argument("--substeps", type=int, default=10, help="substeps per step() call")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-substeps", type=int, default=0, help="oracle substeps timed for cpu_baseline (0 = auto)")
+    return ap.parse_args()
+
+
+def make_scene(name):
+    from nebula_b200 import scenes as S
+    if name == "slope":
+        return S.slope_flow()
+    if name == "elastic":
+        return S.elastic_block()
+    return S.multimaterial()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path("/tmp/nebula_clocks_%d_%d.csv" % (os.getpid(), index))
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- algorithmic bytes
+def algorithmic_bytes(phase: str, n: int, active: int, nc: int, flip: bool, sdf: bool) -> float:
+    """Minimal DRAM bytes one launch of each phase must move (documented in DESIGN.md)."""
+    a = active
+    if phase == "g2p":
+        b = n * (80 + 128) + a * 20
+        if flip:
+            b += 16 * a + 0 * n
+        if sdf:
+            b += 4 * n
+        return float(b)
+    if phase == "g2p2g":
+        b = 208 * n + 64 * a
+        if flip:
+            b += 12 * n + 32 * a
+        if sdf:
+            b += 4 * a + 4 * n
+        return float(b)
+    if phase == "p2g":
+        return float(n * 132 + a * 16)
+    if phase == "grid":
+        return float(nc * 4 + a * 48 + (4 * a if sdf else 0))
+    if phase == "bin":
+        return float(52 * n + 12 * nc)
+    return 0.0
+
+
+def canonical_bytes(n, active, flip, sdf):
+    """Per-substep canonical algorithmic bytes: 208 N + 64 A (+FLIP, +SDF adders)."""
+    b = 208 * n + 64 * active
+    if flip:
+        b += 12 * n + 32 * active
+    if sdf:
+        b += 4 * active + 4 * n
+    return float(b)
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    sc = make_scene(args.workload)
+    o = oracle.Oracle("ref32")
+    o.set_params(sc.params)
+    o.set_sdf(sc.sdf)
+    o.set_state(sc.state)
+    cores = oracle.num_threads()
+    for _ in range(args.warmup):
+        o.substep()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.substep()
+    dt = time.perf_counter() - t0
+    v = sc.n * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": sc.name, "particles": sc.n, "grid": list(sc.params.grid_res), "substeps_per_step": 1,
+                   "note": "each step is one substep of the workload (a bounded sample); the reference's shaders cannot run here "
+                           "(no graphics API on the box), so its algorithm runs as the CPU oracle restating them"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "%d substeps of %s after %d warm-up" % (args.steps, sc.name, args.warmup)},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- nebula arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from nebula_b200 import build as nbuild
+    if rank == 0 or world == 1:
+        nbuild.build()
+    if dist:
+        dist.barrier()
+    from nebula_b200.engine import engine_for_scene
+
+    sc = make_scene(args.workload)
+    sp = sc.params
+    n = sc.n
+    S = args.substeps
+    eng = engine_for_scene(sc)
+    eng.numSubsteps = S
+    stream = torch.cuda.current_stream()
+    dt_frame = sp.dt * S
+
+    # active nodes A (nodes with mass >= 1e-10 after P2G of the initial state)
+    mom, mass = eng.export_grid(sp.dt)
+    active = int((mass >= 1e-10).sum())
+    del mom, mass
+
+    for _ in range(args.warmup):
+        eng.step(dt_frame, stream)
+    eng.sync()
+
+    # ---- device-timed region
+    eng.profile(True)
+    eng.profile_read(reset=True)
+    st0 = eng.stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.step(dt_frame, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    eng.sync()
+    ms = e0.elapsed_time(e1)
+    st1 = eng.stats()
+    phases = eng.profile_read(reset=True)
+    eng.profile(False)
+    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_ps = float(n) * S * args.steps * world
+    value = total_ps / (ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers (pinned)
+    pinned = {f: torch.empty((n, 4), dtype=torch.float32, pin_memory=True) for f in sc.state}
+    for f, a in sc.state.items():
+        pinned[f].copy_(torch.from_numpy(a))
+    host_state = {f: t.numpy() for f, t in pinned.items()}
+    out = {f: torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy() for f in sc.state}
+    from nebula_b200 import _capi
+    import ctypes as C
+    e2e_steps = max(2, min(args.steps, 10))
+    eng.sync()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        eng.upload_state(host_state)
+        eng.step(dt_frame, stream)
+        for k, f in enumerate(sc.state):
+            _capi.call("nebula_mpm_download", eng._h, k, out[f].ctypes.data_as(C.c_void_p), out[f].size)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = float(n) * S * e2e_steps * world / (ms_e2e * 1e-3)
+    state_bytes = n * 16 * 8
+
+    # ---- roofline of the dominant phase
+    hbm, src = peaks()
+    flip = sp.flip_ratio > 0.01
+    sdf = sc.sdf is not None
+    dom = max((p for p in phases if phases[p][1] > 0), key=lambda p: phases[p][0])
+    dom_ms, dom_launches = phases[dom]
+    calls = args.steps * S
+    per_launch_ms = dom_ms / calls
+    alg = algorithmic_bytes(dom, n, active, sp.hash_cells, flip, sdf)
+    achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / ("traffic_%s_%s.json" % (dom, sc.name))
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "kernel": dom, "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "peak_source": src + " (hbm_gbs)"}
+    substep_ms = ms / (args.steps * S)
+    canon = canonical_bytes(n, active, flip, sdf)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": sc.name, "particles": n, "grid": list(sp.grid_res), "substeps_per_step": S, "dt": sp.dt,
+                   "transfer": "APIC" if sp.flip_ratio < -0.5 else ("FLIP" if flip else "PIC"), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (128 MB particle state + 16.7M-cell grid, 126 MB L2)", "active_nodes": active},
+        "roofline": roofline,
+        "substep": {"ms": substep_ms, "canonical_bytes": canon, "canonical_frac": canon / (substep_ms * 1e-3) / 1e9 / hbm,
+                    "phases_ms_per_substep": {p: v[0] / calls for p, v in phases.items() if v[1] > 0}},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "clocks": ck,
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        o = oracle.Oracle("ref32")
+        o.set_params(sp)
+        o.set_sdf(sc.sdf)
+        o.set_state(sc.state)
+        k = args.cpu_sample_substeps or 0
+        t0 = time.perf_counter()
+        o.substep()
+        one = time.perf_counter() - t0
+        if k == 0:
+            k = max(1, min(30, int(15.0 / max(one, 1e-3))))
+        t0 = time.perf_counter()
+        o.run(k)
+        cdt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n * k / cdt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+                                "sample": "%d substeps of %s (after one untimed), CPU oracle ref32 mode, OpenMP" % (k, sc.name)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.cleanup()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

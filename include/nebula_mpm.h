@@ -1,0 +1,245 @@
+/* nebula_mpm.h -- C ABI of the B200-native MPMEngine substep.
+ *
+ * This is the drop-in boundary for nebula's MLS-MPM path.  The reference
+ * exposes it as the C++ class `MPMEngine` (src/engine/MPMEngine.h:59-186) whose
+ * `step` records Vulkan dispatches; here the same parameter surface is a plain
+ * C ABI (no CUDA or torch types in the signatures; streams are `void*` holding a
+ * cudaStream_t) over hand-written sm_100a CUDA kernels.
+ *
+ * Conventions
+ *   - Every call returns NEBULA_MPM_OK (0) or an error code; the message of the
+ *     last failure on the calling thread is returned by nebula_mpm_last_error().
+ *     No C++ exception crosses this boundary.
+ *   - Particle arrays use the reference layout (MPMEngine.cpp:46-53): 8 float4
+ *     per particle -- P=(x,Vp), v=(v, material id bits), F0..F2 = columns of F
+ *     with the Kirchhoff stress diagonal in w, B0..B2 = APIC B columns with the
+ *     stress off-diagonals (xy, xz, yz) in w (mpm_common.glsl:98-122).
+ *   - The engine owns its device memory; the caller owns the stream.  Host
+ *     setters copy synchronously.  nebula_mpm_step is stream-ordered and does
+ *     not synchronize.
+ */
+#ifndef NEBULA_MPM_H
+#define NEBULA_MPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define NEBULA_MPM_OK 0
+#define NEBULA_MPM_ERR_INVALID 1     /* bad argument or size */
+#define NEBULA_MPM_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define NEBULA_MPM_ERR_OOM 3         /* device allocation failed */
+#define NEBULA_MPM_ERR_DEVICE 4      /* a kernel raised its error flag (bounded wait expired, non-finite state) */
+#define NEBULA_MPM_ERR_UNSUPPORTED 5 /* feature outside this build (e.g. a noise force) */
+
+/* ---------------------------------------------------------------- records */
+/* MPMConfig (src/engine/MPMEngine.h:22-55): initial nx*ny*nz lattice, domain
+ * size [m], cell size [m], buffer capacity (0 = nx*ny*nz), E, nu, rho0. */
+typedef struct nebula_mpm_config {
+  uint32_t nx, ny, nz;
+  float domainSize[3];
+  float cellSize;
+  uint32_t maxParticles;
+  float E, nu, rho0;
+} nebula_mpm_config;
+
+/* MaterialParams (src/core/MaterialParams.h:16-38), 64 bytes. model:
+ * 0 ELASTIC (Hencky), 1 VON_MISES, 2 DRUCKER_PRAGER, 3 GRANULAR_POWDER,
+ * 4 FLUID, 5 VISCOPLASTIC_MUD. */
+typedef struct nebula_mpm_material {
+  float mu, lambda, rho0;
+  uint32_t model;
+  float M_friction, q_cohesion, q_max, bulkK;
+  float fluidGamma, viscosity, hardening, xi;
+  float pad[4];
+} nebula_mpm_material;
+
+/* ColliderPrimitive (src/core/Collider.h:19-29), 64 bytes. type: 0 plane
+ * (p, n), 1 sphere (p, radius), 2 box (centre p, half extents n), 3 capsule
+ * (start p, axis vector n, radius). */
+typedef struct nebula_mpm_collider {
+  uint32_t type;
+  float px, py, pz;
+  float nx, ny, nz;
+  float radius;
+  float vx, vy, vz;
+  float restitution, friction;
+  float pad[3];
+} nebula_mpm_collider;
+
+/* ForceGPU (src/core/Force.h:27-32), 32 bytes.  Supported types: 0 GRAVITY and
+ * 1 CONSTANT_WIND (data[0..2] = direction, data[3] = strength; both add
+ * direction*strength*dt to every grid velocity, Force.h:136-141).  affectMask 0
+ * or with bit 0 set applies to MPM nodes (typeFlag 0). */
+typedef struct nebula_mpm_force {
+  uint16_t type, affectMask;
+  float data[7];
+} nebula_mpm_force;
+
+/* The public tunables of MPMEngine (src/engine/MPMEngine.h:72-80).
+ * flip_ratio: 0 PIC, -1 APIC, (0.01, 1] FLIP blend. restitution and
+ * wall_friction are carried but read by no substep kernel, as in the reference. */
+typedef struct nebula_mpm_params {
+  float restitution;
+  float wall_friction;
+  int32_t numSubsteps;
+  uint32_t plasticModel;
+  float q_max;
+  float M_friction;
+  float q_cohesion;
+  float flip_ratio;
+} nebula_mpm_params;
+
+/* Particle fields for upload/download/device pointers. */
+typedef enum nebula_mpm_field {
+  NEBULA_MPM_P = 0, NEBULA_MPM_V = 1,
+  NEBULA_MPM_F0 = 2, NEBULA_MPM_F1 = 3, NEBULA_MPM_F2 = 4,
+  NEBULA_MPM_B0 = 5, NEBULA_MPM_B1 = 6, NEBULA_MPM_B2 = 7
+} nebula_mpm_field;
+
+/* Engine-internal counters (for measurement and tests). */
+typedef struct nebula_mpm_stats {
+  uint64_t substeps;          /* substeps run since create */
+  uint32_t live_particles;
+  uint32_t active_bricks;     /* 4x4x4-cell grid bricks touched by the last P2G */
+  uint32_t particle_bricks;   /* bricks holding particles at the last binning */
+  uint32_t grid_res[3];
+  uint32_t cube_res;
+  uint32_t hash_cells;
+  uint64_t kernel_launches;   /* kernels this engine has launched */
+  uint32_t overflow_particles;/* particles whose P2G stencil left their block tile (slow path) */
+  uint32_t error_flags;       /* device error bits seen at the last check */
+} nebula_mpm_stats;
+
+typedef struct nebula_mpm nebula_mpm;
+
+/* ---------------------------------------------------------------- engine (MPMEngine) */
+/* MPMEngine::init (MPMEngine.cpp:34-156): allocates state for
+ * cfg->maxParticles (or nx*ny*nz) particles and places the default lattice. */
+int nebula_mpm_create(const nebula_mpm_config* cfg, nebula_mpm** out);
+/* MPMEngine::cleanup (MPMEngine.cpp:160-163). */
+int nebula_mpm_destroy(nebula_mpm* e);
+const char* nebula_mpm_last_error(void);
+
+/* The public fields of MPMEngine (MPMEngine.h:72-80). */
+int nebula_mpm_set_params(nebula_mpm* e, const nebula_mpm_params* p);
+int nebula_mpm_get_params(const nebula_mpm* e, nebula_mpm_params* p);
+
+/* MPMEngine::setMaterials (MPMEngine.cpp:239-243): n in [1, 16]; n == 0 is ignored. */
+int nebula_mpm_set_materials(nebula_mpm* e, const nebula_mpm_material* mats, uint32_t n);
+/* MPMEngine::setParticleMaterialIds (MPMEngine.cpp:245-256): overwrites v with
+ * (0, 0, 0, id bits) for particles [0, n). */
+int nebula_mpm_set_particle_material_ids(nebula_mpm* e, const uint32_t* ids, uint32_t n);
+/* MPMEngine::setColliders / clearAnalyticColliders (MPMEngine.cpp:260-267): n <= 64. */
+int nebula_mpm_set_colliders(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t n);
+int nebula_mpm_clear_analytic_colliders(nebula_mpm* e);
+/* MPMEngine::setColliderSDF (MPMEngine.cpp:204-209): n == hashCells floats,
+ * indexed by Morton code, world units, negative inside. */
+int nebula_mpm_set_collider_sdf(nebula_mpm* e, const float* morton_sdf, uint64_t n);
+/* MPMEngine::setColliderSphere / clearCollider (MPMEngine.cpp:180-202). */
+int nebula_mpm_set_collider_sphere(nebula_mpm* e, float radius, float cx, float cy, float cz);
+int nebula_mpm_clear_collider(nebula_mpm* e);
+/* EngineBase::setForces / addForce / clearForces (EngineBase.cpp:22-40):
+ * replaces the force table (n <= 16).  No shader is rebuilt: forces are a
+ * kernel parameter table. */
+int nebula_mpm_set_forces(nebula_mpm* e, const nebula_mpm_force* f, uint32_t n);
+/* MPMEngine::appendParticles (MPMEngine.cpp:211-235): pos4=(x,Vp),
+ * vel4=(v, id bits); F=I, B=0, stress=0; truncated at capacity.  *appended
+ * (may be NULL) receives the count actually added. */
+int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* vel4, uint32_t n, uint32_t* appended);
+/* MPMEngine::resetParticles (MPMEngine.cpp:281-287). */
+int nebula_mpm_reset_particles(nebula_mpm* e);
+/* Replace the full state of particles [0, n) (n <= capacity; sets the live
+ * count to n) from 8 host float4 arrays in the reference layout (P, v, F0..B2). */
+int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_t n);
+/* Copy field `f` of the live particles (original particle order) to host:
+ * count = 4 * live floats. */
+int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count);
+/* MPMEngine::step (MPMEngine.cpp:404-474): numSubsteps substeps of dt/numSubsteps,
+ * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream). */
+int nebula_mpm_step(nebula_mpm* e, float dt, void* stream);
+/* MPMEngine::liveParticleCount (MPMEngine.h:67). */
+int nebula_mpm_live_count(const nebula_mpm* e, uint32_t* n);
+int nebula_mpm_get_stats(nebula_mpm* e, nebula_mpm_stats* s);
+/* Synchronize the engine's last stream and report device-side error flags. */
+int nebula_mpm_sync(nebula_mpm* e);
+/* Binning of the current positions in the reference's output format
+ * (MPMHarness::buildHashGridCPU, MPMHarness.cpp:132-178): cellCount[hashCells],
+ * cellOffset[hashCells] = END of each cell's range, sorted[live] = particle
+ * indices, ascending inside each cell.  Host arrays. */
+int nebula_mpm_export_bins(nebula_mpm* e, uint32_t* cellCount, uint32_t* cellOffset, uint32_t* sorted);
+/* The grid that P2G of the current particle state produces with substep
+ * length `dt` (mpm_zero_grid.comp + mpm_p2g.comp), in the reference layout:
+ * mom[4*hashCells] (w = 0) and mass[hashCells].  Host arrays.  The particle
+ * state is not advanced. */
+int nebula_mpm_export_grid(nebula_mpm* e, float dt, float* mom, float* mass);
+
+/* Per-phase device timing (no counterpart in the reference, which has no MPM
+ * timers): when enabled, the engine brackets each kernel phase of every
+ * substep with CUDA events on the launching stream.  Phases: 0 binning,
+ * 1 P2G, 2 grid update, 3 G2P, 4 fused G2P+P2G, 5 other.  Reading synchronizes
+ * and returns milliseconds and launch counts accumulated since the last reset. */
+#define NEBULA_MPM_PHASES 6
+int nebula_mpm_profile_enable(nebula_mpm* e, int enable);
+int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_t launches[NEBULA_MPM_PHASES], int reset);
+
+/* Domain helpers (src/core/Domain.h:14-39). */
+void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint32_t out[3]);
+uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]);
+uint32_t nebula_mpm_domain_hash_cells(const uint32_t res[3]);
+uint32_t nebula_mpm_domain_n_groups(uint32_t cells);
+
+/* ---------------------------------------------------------------- single passes
+ * One reference dispatch each, on caller-owned DEVICE buffers in the reference
+ * layout, mirroring the per-pass harness (MPMHarness::runP2G / runGridUpdate /
+ * runG2P, MPMHarness.cpp:260-282).  `pass` carries the MPMSimPC scalars. */
+typedef struct nebula_mpm_pass {
+  float dt;
+  float cellSize;
+  uint32_t gridRes[3];
+  uint32_t hashCells;      /* cubeRes^3 */
+  float worldMin[3];
+  float worldMax[3];
+  float flip_ratio;
+  uint32_t particleCount;
+  uint32_t materialCount;  /* 0 = use the global fallbacks below */
+  uint32_t colliderCount;
+  uint32_t forceCount;
+  float mu_lame, lambda_lame, rho0, M_friction, q_cohesion, q_max;
+  uint32_t plasticModel;
+} nebula_mpm_pass;
+
+/* Particle state: 8 device float4 arrays (P, v, F0, F1, F2, B0, B1, B2). */
+typedef struct nebula_mpm_particles {
+  float* f[8];
+} nebula_mpm_particles;
+
+/* zero_cells + mpm_hash_count + scan + mpm_hash_sort (zero_cells.comp,
+ * mpm_hash_count.comp, hash_scan_*.comp, hash_add_base.comp, mpm_hash_sort.comp):
+ * cellCount[hashCells], cellOffset[hashCells] (range END), sorted[particleCount]
+ * ascending inside each cell.  Uses a caller-visible workspace from
+ * nebula_mpm_bin_workspace_size(). */
+size_t nebula_mpm_bin_workspace_size(uint32_t hashCells, uint32_t particleCount);
+int nebula_mpm_bin(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSorted,
+                   void* dWorkspace, size_t workspaceBytes, void* stream);
+/* mpm_zero_grid.comp + mpm_p2g.comp: writes gridMom[0, hashCells) (w = 0) and
+ * gridMass; clears gridMom[hashCells, 2 hashCells). */
+int nebula_mpm_p2g(const nebula_mpm_pass* pass, const nebula_mpm_particles* parts, const uint32_t* dCellCount, const uint32_t* dCellOffset,
+                   const uint32_t* dSorted, const nebula_mpm_material* dMaterials, float* dGridMom, float* dGridMass, void* stream);
+/* mpm_grid_update.comp (+ forces, walls, analytic colliders) and, when dSdf is
+ * non-NULL, mpm_nanovdb_bc.comp, fused per node. */
+int nebula_mpm_grid_update(const nebula_mpm_pass* pass, float* dGridMom, const float* dGridMass, const nebula_mpm_collider* dColliders,
+                           const nebula_mpm_force* dForces, const float* dSdf, void* stream);
+/* mpm_g2p.comp: gather, F update, return maps, stress, position update. */
+int nebula_mpm_g2p(const nebula_mpm_pass* pass, const nebula_mpm_particles* parts, const float* dGridMom, const float* dGridMass,
+                   const nebula_mpm_material* dMaterials, const float* dSdf, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEBULA_MPM_H */

@@ -1,0 +1,460 @@
+// mpm_device.cuh -- device math shared by every MPM kernel (sm_100a).
+//
+// Restates, for CUDA, the math of the reference's shader library:
+//   Morton codes              shaders/mpm_common.glsl:161-195
+//   quadratic B-spline        shaders/mpm_common.glsl:198-210
+//   Jacobi eigen / svd3       shaders/mpm_common.glsl:213-281
+//   Hencky / fluid stress     shaders/mpm_common.glsl:284-302
+//   Von Mises / Drucker-Prager return maps  shaders/mpm_g2p.comp:19-68
+//   analytic collider SDFs + Coulomb BC     shaders/collider_common.glsl:22-85
+//
+// Matrices use GLSL's column-major indexing, m[c][r] = column c, row r, so the
+// products below compute exactly what the shaders' `U * diag * transpose(U)`
+// and `U * diag * transpose(V)` compute with svd3's layout (singular vectors
+// stored as U[.][i], i.e. as rows of the GLSL matrix).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nebula_mpm.h"
+
+namespace nebula {
+
+// ------------------------------------------------------------------ records
+struct Material {  // MaterialParams, 64 B
+  float mu, lambda, rho0;
+  uint32_t model;
+  float M_friction, q_cohesion, q_max, bulkK, fluidGamma, viscosity, hardening, xi, pad[4];
+};
+struct Collider {  // ColliderPrimitive, 64 B
+  uint32_t type;
+  float px, py, pz, nx, ny, nz, radius, vx, vy, vz, restitution, friction, pad[3];
+};
+struct Force {  // ForceGPU, 32 B
+  uint16_t type, affectMask;
+  float data[7];
+};
+static_assert(sizeof(Material) == 64, "Material");
+static_assert(sizeof(Collider) == 64, "Collider");
+static_assert(sizeof(Force) == 32, "Force");
+
+enum : uint32_t { MAT_ELASTIC = 0, MAT_VON_MISES = 1, MAT_DRUCKER_PRAGER = 2, MAT_GRANULAR_POWDER = 3, MAT_FLUID = 4, MAT_VISCOPLASTIC_MUD = 5 };
+enum : uint32_t { COLL_PLANE = 0, COLL_SPHERE = 1, COLL_BOX = 2, COLL_CAPSULE = 3 };
+enum : uint32_t { FORCE_GRAVITY = 0, FORCE_CONSTANT_WIND = 1 };
+
+constexpr int kMaxMaterials = 16;
+constexpr int kMaxColliders = 64;
+constexpr int kMaxForces = 16;
+
+// Every scalar a substep kernel reads (the MPMSimPC fields, MPMSimPC.h:14-77),
+// passed by value.  Tables live in device memory.
+struct SubstepParams {
+  float dt;
+  float cellSize;
+  int gridRes[3];
+  uint32_t cubeRes;
+  uint32_t hashCells;
+  float worldMin[3];
+  float worldMax[3];
+  float flip_ratio;
+  uint32_t materialCount;
+  uint32_t colliderCount;
+  uint32_t forceCount;
+  float mu_lame, lambda_lame, rho0, M_friction, q_cohesion, q_max;
+  uint32_t plasticModel;
+  const Material* materials;
+  const Collider* colliders;
+  const Force* forces;
+  const float* sdf;  // dense Morton-ordered SDF or nullptr
+};
+
+// ------------------------------------------------------------------ Morton
+__host__ __device__ __forceinline__ uint32_t mortonExpand(uint32_t v) {
+  v = (v | (v << 16u)) & 0x030000FFu;
+  v = (v | (v << 8u)) & 0x0300F00Fu;
+  v = (v | (v << 4u)) & 0x030C30C3u;
+  v = (v | (v << 2u)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t mortonCompact(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2u)) & 0x030C30C3u;
+  v = (v | (v >> 4u)) & 0x0300F00Fu;
+  v = (v | (v >> 8u)) & 0x030000FFu;
+  v = (v | (v >> 16u)) & 0x000003FFu;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t mortonEncode(int x, int y, int z) {
+  return mortonExpand(uint32_t(x)) | (mortonExpand(uint32_t(y)) << 1u) | (mortonExpand(uint32_t(z)) << 2u);
+}
+__host__ __device__ __forceinline__ void mortonDecode(uint32_t c, int& x, int& y, int& z) {
+  x = int(mortonCompact(c));
+  y = int(mortonCompact(c >> 1u));
+  z = int(mortonCompact(c >> 2u));
+}
+
+// cellIdFromPos (mpm_common.glsl:190-195): clamp((p - worldMin)/h, 0, gridRes-1), truncate.
+__device__ __forceinline__ void cellCoords(const SubstepParams& P, float x, float y, float z, int& cx, int& cy, int& cz) {
+  float lx = fminf(fmaxf(__fdiv_rn(x - P.worldMin[0], P.cellSize), 0.0f), float(P.gridRes[0]) - 1.0f);
+  float ly = fminf(fmaxf(__fdiv_rn(y - P.worldMin[1], P.cellSize), 0.0f), float(P.gridRes[1]) - 1.0f);
+  float lz = fminf(fmaxf(__fdiv_rn(z - P.worldMin[2], P.cellSize), 0.0f), float(P.gridRes[2]) - 1.0f);
+  cx = int(uint32_t(lx));
+  cy = int(uint32_t(ly));
+  cz = int(uint32_t(lz));
+}
+
+// ------------------------------------------------------------------ B-spline
+__device__ __forceinline__ float gsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+__device__ __forceinline__ double gsign(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+
+__device__ __forceinline__ float bspline2(float d) {
+  float ad = fabsf(d);
+  if (ad < 0.5f) return 0.75f - ad * ad;
+  if (ad < 1.5f) { float t = 1.5f - ad; return 0.5f * t * t; }
+  return 0.0f;
+}
+__device__ __forceinline__ float bspline2g(float d) {
+  float ad = fabsf(d);
+  if (ad < 0.5f) return -2.0f * d;
+  if (ad < 1.5f) return -gsign(d) * (1.5f - ad);
+  return 0.0f;
+}
+
+// ------------------------------------------------------------------ small matrices (GLSL indexing)
+template <class T> struct m3 {
+  T m[3][3];
+};
+template <class T> __device__ __forceinline__ m3<T> m3zero() {
+  m3<T> r;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r.m[c][k] = T(0);
+  return r;
+}
+template <class T> __device__ __forceinline__ m3<T> m3ident() {
+  m3<T> r = m3zero<T>();
+  r.m[0][0] = r.m[1][1] = r.m[2][2] = T(1);
+  return r;
+}
+// GLSL A * B
+template <class T> __device__ __forceinline__ m3<T> m3mul(const m3<T>& A, const m3<T>& B) {
+  m3<T> C;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) C.m[j][i] = A.m[0][i] * B.m[j][0] + A.m[1][i] * B.m[j][1] + A.m[2][i] * B.m[j][2];
+  return C;
+}
+template <class T> __device__ __forceinline__ T m3det(const m3<T>& A) {
+  const T* a = A.m[0];
+  const T* b = A.m[1];
+  const T* c = A.m[2];
+  return a[0] * (b[1] * c[2] - c[1] * b[2]) - b[0] * (a[1] * c[2] - c[1] * a[2]) + c[0] * (a[1] * b[2] - b[1] * a[2]);
+}
+template <class A, class B> __device__ __forceinline__ m3<A> m3cast(const m3<B>& s) {
+  m3<A> r;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r.m[c][k] = A(s.m[c][k]);
+  return r;
+}
+
+template <class T> __device__ __forceinline__ T dsqrt(T x);
+template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
+template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+template <class T> __device__ __forceinline__ T dlog(T x);
+template <> __device__ __forceinline__ float dlog<float>(float x) { return logf(x); }
+template <> __device__ __forceinline__ double dlog<double>(double x) { return log(x); }
+template <class T> __device__ __forceinline__ T dexp(T x);
+template <> __device__ __forceinline__ float dexp<float>(float x) { return expf(x); }
+template <> __device__ __forceinline__ double dexp<double>(double x) { return exp(x); }
+
+// jacobiEigen3 (mpm_common.glsl:213-247): cyclic-max Jacobi, <= 20 rotations,
+// stop when every off-diagonal of A is below 1e-8.
+template <class T> __device__ __forceinline__ void jacobiEigen3(m3<T> A, T D[3], m3<T>& V) {
+  V = m3ident<T>();
+#pragma unroll 1
+  for (int iter = 0; iter < 20; iter++) {
+    T a01 = A.m[0][1], a02 = A.m[0][2], a12 = A.m[1][2];
+    T b01 = fabs(a01), b02 = fabs(a02), b12 = fabs(a12);
+    if (fmax(b01, fmax(b02, b12)) < T(1e-8)) break;
+    int p0, p1;
+    T apq;
+    if (b01 >= fmax(b02, b12)) { p0 = 0; p1 = 1; apq = a01; }
+    else if (b02 >= b12) { p0 = 0; p1 = 2; apq = a02; }
+    else { p0 = 1; p1 = 2; apq = a12; }
+    const int r = 3 - p0 - p1;  // the untouched index
+    T app = A.m[p0][p0], aqq = A.m[p1][p1];
+    T tau = (aqq - app) / (T(2) * apq);
+    T t = gsign(tau) / (fabs(tau) + dsqrt<T>(T(1) + tau * tau));
+    T c = T(1) / dsqrt<T>(T(1) + t * t);
+    T s = t * c;
+    A.m[p0][p0] = app - t * apq;
+    A.m[p1][p1] = aqq + t * apq;
+    A.m[p0][p1] = T(0);
+    A.m[p1][p0] = T(0);
+    {
+      T arp = A.m[r][p0], arq = A.m[r][p1];
+      A.m[r][p0] = c * arp - s * arq;
+      A.m[p0][r] = A.m[r][p0];
+      A.m[r][p1] = s * arp + c * arq;
+      A.m[p1][r] = A.m[r][p1];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      T vrp = V.m[q][p0], vrq = V.m[q][p1];
+      V.m[q][p0] = c * vrp - s * vrq;
+      V.m[q][p1] = s * vrp + c * vrq;
+    }
+  }
+  D[0] = A.m[0][0];
+  D[1] = A.m[1][1];
+  D[2] = A.m[2][2];
+}
+
+// svd3 (mpm_common.glsl:250-281) on F^T F; sigma sorted descending.
+template <class T> __device__ __forceinline__ void svd3(const m3<T>& F, m3<T>& U, T sigma[3], m3<T>& V) {
+  m3<T> FtF;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) FtF.m[j][i] = F.m[i][0] * F.m[j][0] + F.m[i][1] * F.m[j][1] + F.m[i][2] * F.m[j][2];
+  T sig2[3];
+  jacobiEigen3(FtF, sig2, V);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sigma[i] = dsqrt<T>(fmax(sig2[i], T(0)));
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = i + 1; j < 3; j++) {
+      if (sigma[j] > sigma[i]) {
+        T tmp = sigma[i]; sigma[i] = sigma[j]; sigma[j] = tmp;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { T v = V.m[k][i]; V.m[k][i] = V.m[k][j]; V.m[k][j] = v; }
+      }
+    }
+  U = m3zero<T>();
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    if (sigma[i] > T(1e-8)) {
+      T v0 = V.m[0][i], v1 = V.m[1][i], v2 = V.m[2][i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) U.m[k][i] = (F.m[0][k] * v0 + F.m[1][k] * v1 + F.m[2][k] * v2) / sigma[i];
+    } else {
+      U.m[i][i] = T(1);
+    }
+  }
+  if (m3det(U) < T(0)) {
+    U.m[0][2] = -U.m[0][2];
+    U.m[1][2] = -U.m[1][2];
+    U.m[2][2] = -U.m[2][2];
+    sigma[2] = -sigma[2];
+  }
+}
+
+// Hencky principal Kirchhoff stresses k_i = lam*tr(eps) + 2 mu eps_i with
+// eps = log(max(|sigma|, 1e-6)).
+template <class T> __device__ __forceinline__ void henckyPrincipal(const T sigma[3], T mu, T lam, T k[3]) {
+  T e[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) e[i] = dlog<T>(fmax(fabs(sigma[i]), T(1e-6)));
+  T tr = e[0] + e[1] + e[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) k[i] = lam * tr + T(2) * mu * e[i];
+}
+
+// The shaders' `U * diag(k) * transpose(U)` with svd3's U layout:
+//   tau[c][r] = sum_m k_m U[m][r] U[m][c]
+template <class T> __device__ __forceinline__ m3<T> stressUDUt(const m3<T>& U, const T k[3]) {
+  m3<T> t;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) t.m[c][r] = k[0] * U.m[0][r] * U.m[0][c] + k[1] * U.m[1][r] * U.m[1][c] + k[2] * U.m[2][r] * U.m[2][c];
+  return t;
+}
+
+// Stress of a rebuilt F = U diag(s) V^T (shader layout), evaluated from the same
+// decomposition: svd3 of the rebuilt matrix returns the transpose-paired
+// vectors, so the shaders' second `U * diag * transpose(U)` equals
+//   tau[c][r] = sum_i k_i U[r][i] U[c][i]
+template <class T> __device__ __forceinline__ m3<T> stressRebuilt(const m3<T>& U, const T k[3]) {
+  m3<T> t;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) t.m[c][r] = k[0] * U.m[r][0] * U.m[c][0] + k[1] * U.m[r][1] * U.m[c][1] + k[2] * U.m[r][2] * U.m[c][2];
+  return t;
+}
+
+// `U * diag(s) * transpose(V)` (GLSL): F[c][r] = sum_m s_m U[m][r] V[m][c]
+template <class T> __device__ __forceinline__ m3<T> rebuildUSVt(const m3<T>& U, const T s[3], const m3<T>& V) {
+  m3<T> F;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) F.m[c][r] = s[0] * U.m[0][r] * V.m[0][c] + s[1] * U.m[1][r] * V.m[1][c] + s[2] * U.m[2][r] * V.m[2][c];
+  return F;
+}
+
+// henckyStress (mpm_common.glsl:284-293)
+template <class T> __device__ __forceinline__ m3<T> henckyStress(const m3<T>& F, T mu, T lam) {
+  m3<T> U, V;
+  T s[3], k[3];
+  svd3(F, U, s, V);
+  henckyPrincipal(s, mu, lam, k);
+  return stressUDUt(U, k);
+}
+
+// Plastic return map + Kirchhoff stress with ONE decomposition (double).
+// model VON_MISES: mpm_g2p.comp:19-38 then henckyStress; DRUCKER_PRAGER /
+// POWDER / MUD: mpm_g2p.comp:41-68 then henckyStress.  Where the shader
+// rebuilds F it decomposes again; that second decomposition is the rebuilt
+// F's own SVD, so the stress is taken from the first one via stressRebuilt.
+__device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<float>& tau, float mu_f, float lam_f, float M_f, float qc_f,
+                                              float qmax_f) {
+  const double mu = mu_f, lam = lam_f;
+  m3<double> Fd = m3cast<double>(F), U, V;
+  double s[3];
+  svd3(Fd, U, s, V);
+  double eps[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eps[i] = log(fmax(fabs(s[i]), 1e-6));
+  double trEps = eps[0] + eps[1] + eps[2];
+  double dev[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) dev[i] = eps[i] - (trEps / 3.0);
+  double normDev = sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  bool rebuild;
+  if (model == MAT_VON_MISES) {
+    double delta = normDev - double(qmax_f) / (2.0 * mu);
+    rebuild = delta > 0.0 && normDev > 1e-8;
+    if (rebuild) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - (delta / normDev) * dev[i]) + (trEps / 3.0);
+    }
+  } else {
+    double K = lam + 2.0 * mu / 3.0;
+    double p = -K * trEps;
+    double q_yield = double(M_f) * p + double(qc_f);
+    rebuild = true;
+    if (q_yield <= 1e-8) {
+      double p_proj = -double(qc_f) / fmax(double(M_f), 1e-8);
+      double tr = -p_proj / K;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) eps[i] = tr / 3.0;
+    } else {
+      double delta = normDev - q_yield / (2.0 * mu);
+      if (delta > 0.0 && normDev > 1e-8) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - (delta / normDev) * dev[i]) + (trEps / 3.0);
+      }
+    }
+  }
+  double k[3];
+  if (rebuild) {
+    double sp[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sp[i] = exp(eps[i]);
+    m3<double> Fn = rebuildUSVt(U, sp, V);
+    F = m3cast<float>(Fn);
+    henckyPrincipal(sp, mu, lam, k);
+    tau = m3cast<float>(stressRebuilt(U, k));
+  } else {
+    henckyPrincipal(s, mu, lam, k);
+    tau = m3cast<float>(stressUDUt(U, k));
+  }
+}
+
+// ------------------------------------------------------------------ colliders
+struct f3 {
+  float x, y, z;
+};
+__device__ __forceinline__ f3 mkf3(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float len3(f3 a) { return sqrtf(dot3(a, a)); }
+
+__device__ __forceinline__ float colliderSDF(const Collider& c, f3 p, f3& n) {
+  if (c.type == COLL_SPHERE) {
+    f3 d = mkf3(p.x - c.px, p.y - c.py, p.z - c.pz);
+    float dist = len3(d);
+    n = dist > 1e-8f ? mkf3(d.x / dist, d.y / dist, d.z / dist) : mkf3(0.f, 1.f, 0.f);
+    return dist - c.radius;
+  }
+  if (c.type == COLL_BOX) {
+    f3 rel = mkf3(p.x - c.px, p.y - c.py, p.z - c.pz);
+    f3 q = mkf3(fabsf(rel.x) - c.nx, fabsf(rel.y) - c.ny, fabsf(rel.z) - c.nz);
+    f3 qp = mkf3(fmaxf(q.x, 0.f), fmaxf(q.y, 0.f), fmaxf(q.z, 0.f));
+    float sdf = len3(qp) + fminf(fmaxf(q.x, fmaxf(q.y, q.z)), 0.f);
+    if (sdf < 0.f) {
+      f3 diff = mkf3(c.nx - fabsf(rel.x), c.ny - fabsf(rel.y), c.nz - fabsf(rel.z));
+      if (diff.x < diff.y && diff.x < diff.z) n = mkf3(gsign(rel.x + 1e-8f), 0.f, 0.f);
+      else if (diff.y < diff.z) n = mkf3(0.f, gsign(rel.y + 1e-8f), 0.f);
+      else n = mkf3(0.f, 0.f, gsign(rel.z + 1e-8f));
+    } else {
+      float qLen = len3(qp);
+      f3 sg = mkf3(gsign(rel.x + 1e-8f), gsign(rel.y + 1e-8f), gsign(rel.z + 1e-8f));
+      f3 a = qLen > 1e-8f ? mkf3(qp.x * sg.x, qp.y * sg.y, qp.z * sg.z) : sg;
+      float l = len3(a);
+      n = mkf3(a.x / l, a.y / l, a.z / l);
+    }
+    return sdf;
+  }
+  if (c.type == COLL_CAPSULE) {
+    f3 ax = mkf3(c.nx, c.ny, c.nz);
+    float axisLen = len3(ax);
+    f3 dir = axisLen > 1e-8f ? mkf3(ax.x / axisLen, ax.y / axisLen, ax.z / axisLen) : mkf3(0.f, 1.f, 0.f);
+    float t = fminf(fmaxf(dot3(mkf3(p.x - c.px, p.y - c.py, p.z - c.pz), dir), 0.f), axisLen);
+    f3 d = mkf3(p.x - (c.px + t * dir.x), p.y - (c.py + t * dir.y), p.z - (c.pz + t * dir.z));
+    float dist = len3(d);
+    n = dist > 1e-8f ? mkf3(d.x / dist, d.y / dist, d.z / dist) : mkf3(0.f, 1.f, 0.f);
+    return dist - c.radius;
+  }
+  // plane (default)
+  f3 nn = mkf3(c.nx, c.ny, c.nz);
+  float l = len3(nn);
+  n = mkf3(nn.x / l, nn.y / l, nn.z / l);
+  return dot3(mkf3(p.x - c.px, p.y - c.py, p.z - c.pz), n);
+}
+
+__device__ __forceinline__ void applyColliderBC(f3& v, f3 n, f3 vc, float restitution, float friction) {
+  f3 vr = mkf3(v.x - vc.x, v.y - vc.y, v.z - vc.z);
+  float vn = dot3(vr, n);
+  if (vn < 0.f) {
+    f3 vnv = mkf3(vn * n.x, vn * n.y, vn * n.z);
+    f3 vt = mkf3(vr.x - vnv.x, vr.y - vnv.y, vr.z - vnv.z);
+    float vtLen = len3(vt);
+    if (vtLen > 1e-8f) {
+      float s = fmaxf(0.f, 1.f - friction * fabsf(vn) / vtLen);
+      vt = mkf3(s * vt.x, s * vt.y, s * vt.z);
+    }
+    v = mkf3(vc.x + vt.x - restitution * vnv.x, vc.y + vt.y - restitution * vnv.y, vc.z + vt.z - restitution * vnv.z);
+  }
+}
+
+// ------------------------------------------------------------------ per-particle material
+struct MatSample {
+  float mu, lam, rho0, M, qc, qmax, bulkK, visc;
+  uint32_t model;
+};
+__device__ __forceinline__ MatSample fetchMaterial(const SubstepParams& P, uint32_t id) {
+  MatSample s;
+  if (P.materialCount > 0u) {
+    id = min(id, P.materialCount - 1u);
+    const Material& m = P.materials[id];
+    s.mu = m.mu; s.lam = m.lambda; s.rho0 = m.rho0; s.model = m.model;
+    s.M = m.M_friction; s.qc = m.q_cohesion; s.qmax = m.q_max; s.bulkK = m.bulkK; s.visc = m.viscosity;
+  } else {
+    s.mu = P.mu_lame; s.lam = P.lambda_lame; s.rho0 = P.rho0; s.model = P.plasticModel;
+    s.M = P.M_friction; s.qc = P.q_cohesion; s.qmax = P.q_max; s.bulkK = 0.f; s.visc = 0.f;
+  }
+  return s;
+}
+__device__ __forceinline__ float fetchRho0(const SubstepParams& P, uint32_t id) {
+  if (P.materialCount > 0u) return P.materials[min(id, P.materialCount - 1u)].rho0;
+  return P.rho0;
+}
+
+}  // namespace nebula

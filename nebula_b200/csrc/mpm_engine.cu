@@ -1,0 +1,625 @@
+// mpm_engine.cu -- nebula::MPMEngine: the C++ host side of the substep and the
+// C ABI declared in include/nebula_mpm.h.
+//
+// The class keeps the reference's parameter surface (src/engine/MPMEngine.h:59-186):
+// config, public tunables, material / collider / SDF / force tables, particle
+// append / reset, and step(dt) running numSubsteps substeps
+// (src/engine/MPMEngine.cpp:404-474).  Device memory is owned here; the caller
+// owns the stream.  Errors are C++ exceptions inside and status codes at the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mpm_engine.h"
+#include "mpm_internal.h"
+#include "mpm_scan.cuh"
+
+namespace nebula {
+
+// ------------------------------------------------------------------ errors
+thread_local std::string g_last_error;
+
+Error::Error(int code, const std::string& msg) : std::runtime_error(msg), code(code) {}
+
+void check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  int code = e == cudaErrorMemoryAllocation ? NEBULA_MPM_ERR_OOM : NEBULA_MPM_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ domain (src/core/Domain.h:14-39)
+void domainGridRes(const float size[3], float h, uint32_t out[3]) {
+  const float hh = std::max(h, 1e-6f);
+  for (int a = 0; a < 3; ++a) {
+    float r = std::ceil(size[a] / hh);
+    out[a] = r < 1.0f ? 1u : uint32_t(r);
+  }
+}
+uint32_t domainCubeRes(const uint32_t res[3]) {
+  uint32_t m = std::max({res[0], res[1], res[2], 1u});
+  uint32_t p = 1;
+  while (p < m) p <<= 1u;
+  return p;
+}
+uint32_t domainHashCells(const uint32_t res[3]) {
+  uint32_t c = domainCubeRes(res);
+  return c * c * c;
+}
+
+// ------------------------------------------------------------------ device buffer
+DevBuf::~DevBuf() { reset(); }
+void DevBuf::reset() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+void DevBuf::alloc(size_t n) {
+  reset();
+  if (n == 0) return;
+  check(cudaMalloc(&ptr, n), "cudaMalloc");
+  bytes = n;
+}
+void DevBuf::ensure(size_t n) {
+  if (n > bytes) alloc(n);
+}
+
+// ------------------------------------------------------------------ engine
+MPMEngine::MPMEngine(const nebula_mpm_config& cfg) : cfg_(cfg) {
+  if (!(cfg.cellSize > 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "cellSize must be > 0");
+  for (int a = 0; a < 3; ++a)
+    if (!(cfg.domainSize[a] >= 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "domainSize must be >= 0");
+  check(cudaGetDevice(&device_), "cudaGetDevice");
+  domainGridRes(cfg.domainSize, cfg.cellSize, gridRes_);
+  cubeRes_ = domainCubeRes(gridRes_);
+  if (cubeRes_ > 1024u) throw Error(NEBULA_MPM_ERR_INVALID, "grid resolution above 1024 per axis (10-bit Morton code)");
+  hashCells_ = cubeRes_ * cubeRes_ * cubeRes_;
+  const uint64_t lattice = uint64_t(cfg.nx) * cfg.ny * cfg.nz;
+  capacity_ = cfg.maxParticles > 0 ? cfg.maxParticles : uint32_t(lattice);
+  if (lattice > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "nx*ny*nz exceeds maxParticles");
+
+  for (int k = 0; k < 8; ++k) state_[k].alloc(size_t(std::max(capacity_, 1u)) * sizeof(float4));
+  const size_t nc = hashCells_;
+  gridMom_.alloc(nc * 2 * sizeof(float4));
+  gridMass_.alloc(nc * sizeof(float));
+  cellCount_.alloc(nc * sizeof(uint32_t));
+  cellStart_.alloc(nc * sizeof(uint32_t));
+  cellEnd_.alloc(nc * sizeof(uint32_t));
+  const size_t pc = size_t(std::max(capacity_, 1u)) * sizeof(uint32_t);
+  key_.alloc(pc);
+  rank_.alloc(pc);
+  sortedTmp_.alloc(pc);
+  sorted_.alloc(pc);
+  scanWs_.alloc(scanWorkspaceBytes(nc));
+  materials_.alloc(kMaxMaterials * sizeof(Material));
+  colliders_.alloc(kMaxColliders * sizeof(Collider));
+  forces_.alloc(kMaxForces * sizeof(Force));
+  err_.alloc(sizeof(uint32_t));
+  check(cudaMemset(err_.ptr, 0, sizeof(uint32_t)), "cudaMemset");
+  check(cudaMemset(gridMom_.ptr, 0, gridMom_.bytes), "cudaMemset");
+  check(cudaMemset(gridMass_.ptr, 0, gridMass_.bytes), "cudaMemset");
+
+  // default material: presetJelly(E, nu, rho0) with model ELASTIC and the
+  // public DP/VM defaults (MPMEngine.cpp:67-78)
+  Material m{};
+  m.mu = cfg.E / (2.0f * (1.0f + cfg.nu));
+  m.lambda = cfg.E * cfg.nu / ((1.0f + cfg.nu) * (1.0f - 2.0f * cfg.nu));
+  m.rho0 = cfg.rho0;
+  m.model = MAT_ELASTIC;
+  m.M_friction = params_.M_friction;
+  m.q_cohesion = params_.q_cohesion;
+  m.q_max = params_.q_max;
+  hostMaterials_.assign(1, m);
+  check(cudaMemcpy(materials_.ptr, &m, sizeof(m), cudaMemcpyHostToDevice), "upload materials");
+
+  // default lattice (MPMEngine.cpp:86-137)
+  live_ = uint32_t(lattice);
+  if (live_ > 0) {
+    const float blockFrac = 0.40f;
+    const float minDomain = std::min({cfg.domainSize[0], cfg.domainSize[1], cfg.domainSize[2]});
+    const float sp = minDomain * blockFrac / float(std::max({cfg.nx, cfg.ny, cfg.nz}));
+    const float Vp = sp * sp * sp;
+    const float cx = cfg.domainSize[0] * 0.5f, cz = cfg.domainSize[2] * 0.5f, cy = cfg.domainSize[1] * 0.70f;
+    const float halfX = sp * float(cfg.nx - 1) / 2.0f, halfY = sp * float(cfg.ny - 1) / 2.0f, halfZ = sp * float(cfg.nz - 1) / 2.0f;
+    std::vector<float4> host[8];
+    for (auto& h : host) h.assign(live_, make_float4(0.f, 0.f, 0.f, 0.f));
+    uint32_t idx = 0;
+    for (uint32_t iz = 0; iz < cfg.nz; iz++)
+      for (uint32_t iy = 0; iy < cfg.ny; iy++)
+        for (uint32_t ix = 0; ix < cfg.nx; ix++, idx++) {
+          host[0][idx] = make_float4(cx - halfX + ix * sp, cy - halfY + iy * sp, cz - halfZ + iz * sp, Vp);
+          host[2][idx] = make_float4(1.f, 0.f, 0.f, 0.f);
+          host[3][idx] = make_float4(0.f, 1.f, 0.f, 0.f);
+          host[4][idx] = make_float4(0.f, 0.f, 1.f, 0.f);
+        }
+    for (int k = 0; k < 8; ++k) check(cudaMemcpy(state_[k].ptr, host[k].data(), live_ * sizeof(float4), cudaMemcpyHostToDevice), "upload state");
+  }
+}
+
+MPMEngine::~MPMEngine() {
+  if (lastStream_) cudaStreamSynchronize(lastStream_);
+  else cudaDeviceSynchronize();
+  for (auto& t : timed_) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  for (auto ev : freeEvents_) cudaEventDestroy(ev);
+  if (openEvent_) cudaEventDestroy(openEvent_);
+}
+
+// ------------------------------------------------------------------ phase timing
+cudaEvent_t MPMEngine::takeEvent() {
+  if (!freeEvents_.empty()) {
+    cudaEvent_t e = freeEvents_.back();
+    freeEvents_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  check(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+void MPMEngine::phaseBegin(int phase, cudaStream_t s) {
+  (void)phase;
+  if (!profile_) return;
+  openEvent_ = takeEvent();
+  check(cudaEventRecord(openEvent_, s), "cudaEventRecord");
+}
+
+void MPMEngine::phaseEnd(int phase, cudaStream_t s, uint64_t launchesBefore) {
+  if (!profile_ || !openEvent_) return;
+  cudaEvent_t b = takeEvent();
+  check(cudaEventRecord(b, s), "cudaEventRecord");
+  timed_.push_back(Timed{phase, openEvent_, b, launches_ - launchesBefore});
+  openEvent_ = nullptr;
+}
+
+void MPMEngine::profileEnable(bool on) { profile_ = on; }
+
+void MPMEngine::profileRead(double* ms, uint64_t* launches, bool reset) {
+  quiesce();
+  for (auto& t : timed_) {
+    float m = 0.f;
+    check(cudaEventElapsedTime(&m, t.a, t.b), "cudaEventElapsedTime");
+    phaseMs_[t.phase] += m;
+    phaseLaunches_[t.phase] += t.launches;
+    freeEvents_.push_back(t.a);
+    freeEvents_.push_back(t.b);
+  }
+  timed_.clear();
+  for (int i = 0; i < NEBULA_MPM_PHASES; ++i) {
+    ms[i] = phaseMs_[i];
+    launches[i] = phaseLaunches_[i];
+  }
+  if (reset)
+    for (int i = 0; i < NEBULA_MPM_PHASES; ++i) {
+      phaseMs_[i] = 0.0;
+      phaseLaunches_[i] = 0;
+    }
+}
+
+void MPMEngine::bindDevice() const { check(cudaSetDevice(device_), "cudaSetDevice"); }
+
+void MPMEngine::quiesce() {
+  bindDevice();
+  check(lastStream_ ? cudaStreamSynchronize(lastStream_) : cudaDeviceSynchronize(), "synchronize");
+}
+
+void MPMEngine::setParams(const nebula_mpm_params& p) {
+  if (p.numSubsteps < 0) throw Error(NEBULA_MPM_ERR_INVALID, "numSubsteps must be >= 0");
+  params_ = p;
+}
+
+void MPMEngine::setMaterials(const nebula_mpm_material* mats, uint32_t n) {
+  if (n == 0) return;  // MPMEngine.cpp:240
+  if (n > uint32_t(kMaxMaterials)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 16 materials");
+  if (!mats) throw Error(NEBULA_MPM_ERR_INVALID, "null materials");
+  quiesce();
+  hostMaterials_.assign(reinterpret_cast<const Material*>(mats), reinterpret_cast<const Material*>(mats) + n);
+  check(cudaMemcpy(materials_.ptr, mats, n * sizeof(Material), cudaMemcpyHostToDevice), "upload materials");
+}
+
+void MPMEngine::setParticleMaterialIds(const uint32_t* ids, uint32_t n) {
+  if (n > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "more ids than particle capacity");
+  if (n && !ids) throw Error(NEBULA_MPM_ERR_INVALID, "null ids");
+  quiesce();
+  std::vector<float4> v(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    float w;
+    std::memcpy(&w, ids + i, 4);
+    v[i] = make_float4(0.f, 0.f, 0.f, w);
+  }
+  if (n) check(cudaMemcpy(state_[1].ptr, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "upload ids");
+}
+
+void MPMEngine::setColliders(const nebula_mpm_collider* c, uint32_t n) {
+  if (n > uint32_t(kMaxColliders)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 64 colliders");
+  if (n && !c) throw Error(NEBULA_MPM_ERR_INVALID, "null colliders");
+  quiesce();
+  colliderCount_ = n;
+  if (n) check(cudaMemcpy(colliders_.ptr, c, n * sizeof(Collider), cudaMemcpyHostToDevice), "upload colliders");
+}
+
+void MPMEngine::clearAnalyticColliders() { colliderCount_ = 0; }
+
+void MPMEngine::setColliderSDF(const float* sdf, uint64_t n) {
+  if (!sdf || n != hashCells_) throw Error(NEBULA_MPM_ERR_INVALID, "SDF must hold hashCells floats");
+  quiesce();
+  sdf_.ensure(size_t(hashCells_) * sizeof(float));
+  check(cudaMemcpy(sdf_.ptr, sdf, size_t(hashCells_) * sizeof(float), cudaMemcpyHostToDevice), "upload sdf");
+  hasSdf_ = true;
+}
+
+// MPMEngine::setColliderSphere (MPMEngine.cpp:180-200): cell-centre distances on the gridRes box
+void MPMEngine::setColliderSphere(float radius, float cx, float cy, float cz) {
+  std::vector<float> s(hashCells_, 0.0f);
+  const float h = cfg_.cellSize;
+  for (uint32_t iz = 0; iz < gridRes_[2]; iz++)
+    for (uint32_t iy = 0; iy < gridRes_[1]; iy++)
+      for (uint32_t ix = 0; ix < gridRes_[0]; ix++) {
+        float wx = (ix + 0.5f) * h, wy = (iy + 0.5f) * h, wz = (iz + 0.5f) * h;
+        float d = std::sqrt((wx - cx) * (wx - cx) + (wy - cy) * (wy - cy) + (wz - cz) * (wz - cz));
+        s[mortonEncode(int(ix), int(iy), int(iz))] = d - radius;
+      }
+  setColliderSDF(s.data(), s.size());
+}
+
+void MPMEngine::clearCollider() { hasSdf_ = false; }
+
+void MPMEngine::setForces(const nebula_mpm_force* f, uint32_t n) {
+  if (n > uint32_t(kMaxForces)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 16 forces");
+  if (n && !f) throw Error(NEBULA_MPM_ERR_INVALID, "null forces");
+  for (uint32_t i = 0; i < n; ++i)
+    if (f[i].type != FORCE_GRAVITY && f[i].type != FORCE_CONSTANT_WIND)
+      throw Error(NEBULA_MPM_ERR_UNSUPPORTED, "only GRAVITY and CONSTANT_WIND forces act on the MPM grid in this build");
+  quiesce();
+  forceCount_ = n;
+  if (n) check(cudaMemcpy(forces_.ptr, f, n * sizeof(Force), cudaMemcpyHostToDevice), "upload forces");
+}
+
+uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32_t n) {
+  const uint32_t nNew = std::min(n, capacity_ - live_);  // MPMEngine.cpp:212-214
+  if (nNew == 0) return 0;
+  if (!pos4 || !vel4) throw Error(NEBULA_MPM_ERR_INVALID, "null particle arrays");
+  quiesce();
+  std::vector<float4> F0(nNew, make_float4(1, 0, 0, 0)), F1(nNew, make_float4(0, 1, 0, 0)), F2(nNew, make_float4(0, 0, 1, 0)),
+      Z(nNew, make_float4(0, 0, 0, 0));
+  const size_t off = size_t(live_) * sizeof(float4), bytes = size_t(nNew) * sizeof(float4);
+  auto up = [&](int k, const void* src) {
+    check(cudaMemcpy(static_cast<char*>(state_[k].ptr) + off, src, bytes, cudaMemcpyHostToDevice), "append");
+  };
+  up(0, pos4);
+  up(1, vel4);
+  up(2, F0.data());
+  up(3, F1.data());
+  up(4, F2.data());
+  up(5, Z.data());
+  up(6, Z.data());
+  up(7, Z.data());
+  live_ += nNew;
+  return nNew;
+}
+
+void MPMEngine::resetParticles() {
+  quiesce();
+  live_ = 0;
+}
+
+void MPMEngine::uploadState(const float* const f[8], uint32_t n) {
+  if (n > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "more particles than capacity");
+  for (int k = 0; k < 8; ++k)
+    if (n && !f[k]) throw Error(NEBULA_MPM_ERR_INVALID, "null field");
+  quiesce();
+  for (int k = 0; k < 8; ++k)
+    if (n) check(cudaMemcpy(state_[k].ptr, f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice), "upload state");
+  live_ = n;
+}
+
+void MPMEngine::download(int field, float* host, uint64_t count) {
+  if (field < 0 || field > 7) throw Error(NEBULA_MPM_ERR_INVALID, "field index out of range");
+  if (count != uint64_t(live_) * 4) throw Error(NEBULA_MPM_ERR_INVALID, "count must be 4 * live particles");
+  if (count && !host) throw Error(NEBULA_MPM_ERR_INVALID, "null host buffer");
+  quiesce();
+  if (count) check(cudaMemcpy(host, state_[field].ptr, count * sizeof(float), cudaMemcpyDeviceToHost), "download");
+}
+
+SubstepParams MPMEngine::buildParams(float subDt) const {
+  SubstepParams P{};
+  P.dt = subDt;
+  P.cellSize = cfg_.cellSize;
+  for (int a = 0; a < 3; ++a) {
+    P.gridRes[a] = int(gridRes_[a]);
+    P.worldMin[a] = 0.0f;
+    P.worldMax[a] = cfg_.domainSize[a];
+  }
+  P.cubeRes = cubeRes_;
+  P.hashCells = hashCells_;
+  P.flip_ratio = params_.flip_ratio;
+  P.materialCount = uint32_t(hostMaterials_.size());
+  P.colliderCount = colliderCount_;
+  P.forceCount = forceCount_;
+  P.mu_lame = cfg_.E / (2.0f * (1.0f + cfg_.nu));
+  P.lambda_lame = cfg_.E * cfg_.nu / ((1.0f + cfg_.nu) * (1.0f - 2.0f * cfg_.nu));
+  P.rho0 = cfg_.rho0;
+  P.M_friction = params_.M_friction;
+  P.q_cohesion = params_.q_cohesion;
+  P.q_max = params_.q_max;
+  P.plasticModel = params_.plasticModel;
+  P.materials = static_cast<const Material*>(materials_.ptr);
+  P.colliders = static_cast<const Collider*>(colliders_.ptr);
+  P.forces = static_cast<const Force*>(forces_.ptr);
+  P.sdf = hasSdf_ ? static_cast<const float*>(sdf_.ptr) : nullptr;
+  return P;
+}
+
+StatePtrs MPMEngine::statePtrs() {
+  StatePtrs s;
+  for (int k = 0; k < 8; ++k) s.f[k] = static_cast<float4*>(state_[k].ptr);
+  return s;
+}
+
+BinBuffers MPMEngine::binBuffers() {
+  BinBuffers b;
+  b.cellCount = static_cast<uint32_t*>(cellCount_.ptr);
+  b.cellStart = static_cast<uint32_t*>(cellStart_.ptr);
+  b.cellEnd = static_cast<uint32_t*>(cellEnd_.ptr);
+  b.key = static_cast<uint32_t*>(key_.ptr);
+  b.rank = static_cast<uint32_t*>(rank_.ptr);
+  b.sortedTmp = static_cast<uint32_t*>(sortedTmp_.ptr);
+  b.sorted = static_cast<uint32_t*>(sorted_.ptr);
+  b.tileState = static_cast<unsigned long long*>(scanWs_.ptr);
+  b.tileCounter = reinterpret_cast<uint32_t*>(b.tileState + scanTiles(hashCells_));
+  b.err = static_cast<uint32_t*>(err_.ptr);
+  return b;
+}
+
+// One substep in the reference's pass order (MPMEngine.cpp:419-472): zero the
+// grid, bin, P2G, grid update (+ SDF boundary fused per node), G2P.
+void MPMEngine::substepDense(const SubstepParams& P, cudaStream_t s) {
+  BinBuffers b = binBuffers();
+  StatePtrs st = statePtrs();
+  uint64_t l0 = launches_;
+  phaseBegin(kPhaseBin, s);
+  check(launchBin(P, st.f[0], live_, b, s, &launches_), "bin");
+  phaseEnd(kPhaseBin, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseP2G, s);
+  check(cudaMemsetAsync(gridMom_.ptr, 0, gridMom_.bytes, s), "zero grid");
+  check(cudaMemsetAsync(gridMass_.ptr, 0, gridMass_.bytes, s), "zero grid");
+  check(launchP2GDense(P, st, b.sorted, live_, static_cast<float4*>(gridMom_.ptr), static_cast<float*>(gridMass_.ptr), s, &launches_), "p2g");
+  phaseEnd(kPhaseP2G, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseGrid, s);
+  check(launchGridDense(P, static_cast<float4*>(gridMom_.ptr), static_cast<const float*>(gridMass_.ptr), s, &launches_), "grid");
+  phaseEnd(kPhaseGrid, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseG2P, s);
+  check(launchG2PDense(P, st, live_, static_cast<const float4*>(gridMom_.ptr), static_cast<const float*>(gridMass_.ptr), b.err, s, &launches_),
+        "g2p");
+  phaseEnd(kPhaseG2P, s, l0);
+  ++substeps_;
+}
+
+void MPMEngine::step(float dt, cudaStream_t s) {
+  bindDevice();
+  if (!(dt >= 0.f) || !std::isfinite(dt)) throw Error(NEBULA_MPM_ERR_INVALID, "dt must be finite and >= 0");
+  lastStream_ = s;
+  const int n = std::max(1, params_.numSubsteps);
+  const float subDt = dt / float(n);  // MPMEngine.cpp:413
+  const SubstepParams P = buildParams(subDt);
+  for (int k = 0; k < params_.numSubsteps; ++k) substepDense(P, s);
+}
+
+void MPMEngine::exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt) {
+  bindDevice();
+  const SubstepParams P = buildParams(0.f);
+  BinBuffers b = binBuffers();
+  check(launchBin(P, static_cast<const float4*>(state_[0].ptr), live_, b, lastStream_, &launches_), "bin");
+  quiesce();
+  check(cudaMemcpy(cnt, b.cellCount, size_t(hashCells_) * 4, cudaMemcpyDeviceToHost), "download bins");
+  check(cudaMemcpy(off, b.cellEnd, size_t(hashCells_) * 4, cudaMemcpyDeviceToHost), "download bins");
+  if (live_) check(cudaMemcpy(srt, b.sorted, size_t(live_) * 4, cudaMemcpyDeviceToHost), "download bins");
+}
+
+void MPMEngine::exportGrid(float dt, float* mom, float* mass) {
+  bindDevice();
+  const SubstepParams P = buildParams(dt);
+  cudaStream_t s = lastStream_;
+  check(cudaMemsetAsync(gridMom_.ptr, 0, gridMom_.bytes, s), "zero grid");
+  check(cudaMemsetAsync(gridMass_.ptr, 0, gridMass_.bytes, s), "zero grid");
+  BinBuffers b = binBuffers();
+  StatePtrs st = statePtrs();
+  check(launchBin(P, st.f[0], live_, b, s, &launches_), "bin");
+  check(launchP2GDense(P, st, b.sorted, live_, static_cast<float4*>(gridMom_.ptr), static_cast<float*>(gridMass_.ptr), s, &launches_), "p2g");
+  quiesce();
+  check(cudaMemcpy(mom, gridMom_.ptr, size_t(hashCells_) * sizeof(float4), cudaMemcpyDeviceToHost), "download grid");
+  check(cudaMemcpy(mass, gridMass_.ptr, size_t(hashCells_) * sizeof(float), cudaMemcpyDeviceToHost), "download grid");
+}
+
+uint32_t MPMEngine::syncAndCheck() {
+  quiesce();
+  uint32_t e = 0;
+  check(cudaMemcpy(&e, err_.ptr, 4, cudaMemcpyDeviceToHost), "read error flags");
+  errorFlags_ = e;
+  return e;
+}
+
+void MPMEngine::stats(nebula_mpm_stats* s) {
+  std::memset(s, 0, sizeof(*s));
+  s->substeps = substeps_;
+  s->live_particles = live_;
+  s->active_bricks = activeBricks_;
+  s->particle_bricks = particleBricks_;
+  for (int a = 0; a < 3; ++a) s->grid_res[a] = gridRes_[a];
+  s->cube_res = cubeRes_;
+  s->hash_cells = hashCells_;
+  s->kernel_launches = launches_;
+  s->overflow_particles = overflow_;
+  s->error_flags = errorFlags_;
+}
+
+}  // namespace nebula
+
+// ====================================================================== C ABI
+using nebula::Error;
+using nebula::g_last_error;
+
+struct nebula_mpm {
+  std::unique_ptr<nebula::MPMEngine> eng;
+};
+
+namespace {
+template <class F> int guarded(F&& f) {
+  try {
+    f();
+    return NEBULA_MPM_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return NEBULA_MPM_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return NEBULA_MPM_ERR_INVALID;
+  }
+}
+nebula::MPMEngine& E(nebula_mpm* e) {
+  if (!e || !e->eng) throw Error(NEBULA_MPM_ERR_INVALID, "null engine handle");
+  return *e->eng;
+}
+const nebula::MPMEngine& E(const nebula_mpm* e) {
+  if (!e || !e->eng) throw Error(NEBULA_MPM_ERR_INVALID, "null engine handle");
+  return *e->eng;
+}
+}  // namespace
+
+extern "C" {
+
+const char* nebula_mpm_last_error(void) { return g_last_error.c_str(); }
+
+int nebula_mpm_create(const nebula_mpm_config* cfg, nebula_mpm** out) {
+  return guarded([&] {
+    if (!cfg || !out) throw Error(NEBULA_MPM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto h = std::make_unique<nebula_mpm>();
+    h->eng = std::make_unique<nebula::MPMEngine>(*cfg);
+    *out = h.release();
+  });
+}
+int nebula_mpm_destroy(nebula_mpm* e) {
+  return guarded([&] { delete e; });
+}
+int nebula_mpm_set_params(nebula_mpm* e, const nebula_mpm_params* p) {
+  return guarded([&] {
+    if (!p) throw Error(NEBULA_MPM_ERR_INVALID, "null params");
+    E(e).setParams(*p);
+  });
+}
+int nebula_mpm_get_params(const nebula_mpm* e, nebula_mpm_params* p) {
+  return guarded([&] {
+    if (!p) throw Error(NEBULA_MPM_ERR_INVALID, "null params");
+    *p = E(e).params();
+  });
+}
+int nebula_mpm_set_materials(nebula_mpm* e, const nebula_mpm_material* m, uint32_t n) {
+  return guarded([&] { E(e).setMaterials(m, n); });
+}
+int nebula_mpm_set_particle_material_ids(nebula_mpm* e, const uint32_t* ids, uint32_t n) {
+  return guarded([&] { E(e).setParticleMaterialIds(ids, n); });
+}
+int nebula_mpm_set_colliders(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t n) {
+  return guarded([&] { E(e).setColliders(c, n); });
+}
+int nebula_mpm_clear_analytic_colliders(nebula_mpm* e) {
+  return guarded([&] { E(e).clearAnalyticColliders(); });
+}
+int nebula_mpm_set_collider_sdf(nebula_mpm* e, const float* sdf, uint64_t n) {
+  return guarded([&] { E(e).setColliderSDF(sdf, n); });
+}
+int nebula_mpm_set_collider_sphere(nebula_mpm* e, float r, float cx, float cy, float cz) {
+  return guarded([&] { E(e).setColliderSphere(r, cx, cy, cz); });
+}
+int nebula_mpm_clear_collider(nebula_mpm* e) {
+  return guarded([&] { E(e).clearCollider(); });
+}
+int nebula_mpm_set_forces(nebula_mpm* e, const nebula_mpm_force* f, uint32_t n) {
+  return guarded([&] { E(e).setForces(f, n); });
+}
+int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* vel4, uint32_t n, uint32_t* appended) {
+  return guarded([&] {
+    uint32_t k = E(e).appendParticles(pos4, vel4, n);
+    if (appended) *appended = k;
+  });
+}
+int nebula_mpm_reset_particles(nebula_mpm* e) {
+  return guarded([&] { E(e).resetParticles(); });
+}
+int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_t n) {
+  return guarded([&] {
+    if (!fields) throw Error(NEBULA_MPM_ERR_INVALID, "null fields");
+    E(e).uploadState(fields, n);
+  });
+}
+int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count) {
+  return guarded([&] { E(e).download(field, host, count); });
+}
+int nebula_mpm_step(nebula_mpm* e, float dt, void* stream) {
+  return guarded([&] { E(e).step(dt, static_cast<cudaStream_t>(stream)); });
+}
+int nebula_mpm_live_count(const nebula_mpm* e, uint32_t* n) {
+  return guarded([&] {
+    if (!n) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    *n = E(e).liveCount();
+  });
+}
+int nebula_mpm_get_stats(nebula_mpm* e, nebula_mpm_stats* s) {
+  return guarded([&] {
+    if (!s) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).stats(s);
+  });
+}
+int nebula_mpm_sync(nebula_mpm* e) {
+  return guarded([&] {
+    uint32_t f = E(e).syncAndCheck();
+    if (f & ~nebula::kErrTileOverflow) {
+      char buf[128];
+      std::snprintf(buf, sizeof(buf), "device error flags 0x%x (1: bounded wait expired, 2: non-finite particle state)", f);
+      throw Error(NEBULA_MPM_ERR_DEVICE, buf);
+    }
+  });
+}
+int nebula_mpm_profile_enable(nebula_mpm* e, int enable) {
+  return guarded([&] { E(e).profileEnable(enable != 0); });
+}
+int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_t launches[NEBULA_MPM_PHASES], int reset) {
+  return guarded([&] {
+    if (!ms || !launches) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).profileRead(ms, launches, reset != 0);
+  });
+}
+int nebula_mpm_export_bins(nebula_mpm* e, uint32_t* cnt, uint32_t* off, uint32_t* srt) {
+  return guarded([&] {
+    if (!cnt || !off || (!srt && E(e).liveCount())) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).exportBins(cnt, off, srt);
+  });
+}
+int nebula_mpm_export_grid(nebula_mpm* e, float dt, float* mom, float* mass) {
+  return guarded([&] {
+    if (!mom || !mass) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).exportGrid(dt, mom, mass);
+  });
+}
+
+void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint32_t out[3]) {
+  nebula::domainGridRes(domainSize, cellSize, out);
+}
+uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]) { return nebula::domainCubeRes(res); }
+uint32_t nebula_mpm_domain_hash_cells(const uint32_t res[3]) { return nebula::domainHashCells(res); }
+uint32_t nebula_mpm_domain_n_groups(uint32_t cells) { return (cells + 255u) / 256u; }
+
+}  // extern "C"

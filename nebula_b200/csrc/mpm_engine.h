@@ -1,0 +1,119 @@
+// mpm_engine.h -- nebula::MPMEngine, the C++ host engine behind include/nebula_mpm.h.
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/nebula_mpm.h"
+#include "mpm_device.cuh"
+#include "mpm_internal.h"
+
+namespace nebula {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int code, const std::string& msg);
+};
+void check(cudaError_t e, const char* what);
+extern thread_local std::string g_last_error;
+
+void domainGridRes(const float size[3], float h, uint32_t out[3]);
+uint32_t domainCubeRes(const uint32_t res[3]);
+uint32_t domainHashCells(const uint32_t res[3]);
+
+// Owning device allocation.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf();
+  void alloc(size_t n);
+  void ensure(size_t n);
+  void reset();
+};
+
+class MPMEngine {
+ public:
+  explicit MPMEngine(const nebula_mpm_config& cfg);
+  ~MPMEngine();
+
+  void setParams(const nebula_mpm_params& p);
+  const nebula_mpm_params& params() const { return params_; }
+  void setMaterials(const nebula_mpm_material* mats, uint32_t n);
+  void setParticleMaterialIds(const uint32_t* ids, uint32_t n);
+  void setColliders(const nebula_mpm_collider* c, uint32_t n);
+  void clearAnalyticColliders();
+  void setColliderSDF(const float* sdf, uint64_t n);
+  void setColliderSphere(float radius, float cx, float cy, float cz);
+  void clearCollider();
+  void setForces(const nebula_mpm_force* f, uint32_t n);
+  uint32_t appendParticles(const float* pos4, const float* vel4, uint32_t n);
+  void resetParticles();
+  void uploadState(const float* const f[8], uint32_t n);
+  void download(int field, float* host, uint64_t count);
+  void step(float dt, cudaStream_t s);
+  uint32_t liveCount() const { return live_; }
+  void stats(nebula_mpm_stats* s);
+  uint32_t syncAndCheck();
+  void exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt);
+  void exportGrid(float dt, float* mom, float* mass);
+  void profileEnable(bool on);
+  void profileRead(double* ms, uint64_t* launches, bool reset);
+
+ private:
+  // phase timing
+  void phaseBegin(int phase, cudaStream_t s);
+  void phaseEnd(int phase, cudaStream_t s, uint64_t launchesBefore);
+  cudaEvent_t takeEvent();
+  struct Timed {
+    int phase;
+    cudaEvent_t a, b;
+    uint64_t launches;
+  };
+  bool profile_ = false;
+  std::vector<cudaEvent_t> freeEvents_;
+  std::vector<Timed> timed_;
+  cudaEvent_t openEvent_ = nullptr;
+  double phaseMs_[NEBULA_MPM_PHASES] = {};
+  uint64_t phaseLaunches_[NEBULA_MPM_PHASES] = {};
+
+  void bindDevice() const;
+  void quiesce();
+  SubstepParams buildParams(float subDt) const;
+  StatePtrs statePtrs();
+  BinBuffers binBuffers();
+  void substepDense(const SubstepParams& P, cudaStream_t s);
+
+  nebula_mpm_config cfg_;
+  nebula_mpm_params params_{0.3f, 0.0f, 20, 0u, 1e5f, 0.577f, 0.0f, 0.0f};  // MPMEngine.h:72-80
+  int device_ = 0;
+  uint32_t gridRes_[3] = {1, 1, 1};
+  uint32_t cubeRes_ = 1;
+  uint32_t hashCells_ = 1;
+  uint32_t capacity_ = 0;
+  uint32_t live_ = 0;
+  cudaStream_t lastStream_ = nullptr;
+
+  DevBuf state_[8];
+  DevBuf gridMom_, gridMass_;
+  DevBuf cellCount_, cellStart_, cellEnd_, key_, rank_, sortedTmp_, sorted_, scanWs_;
+  DevBuf materials_, colliders_, forces_, sdf_, err_;
+  std::vector<Material> hostMaterials_;
+  uint32_t colliderCount_ = 0;
+  uint32_t forceCount_ = 0;
+  bool hasSdf_ = false;
+
+  uint64_t substeps_ = 0;
+  uint64_t launches_ = 0;
+  uint32_t activeBricks_ = 0;
+  uint32_t particleBricks_ = 0;
+  uint32_t overflow_ = 0;
+  uint32_t errorFlags_ = 0;
+};
+
+}  // namespace nebula

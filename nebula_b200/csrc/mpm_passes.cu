@@ -1,0 +1,187 @@
+// mpm_passes.cu -- single-pass kernels on the reference's dense grid layout.
+//
+// These run one reference dispatch each (binning, P2G, grid update + SDF
+// boundary, G2P) on gridMom (float4 x 2 hashCells: [0,NC) momentum/velocity,
+// [NC,2NC) pre-force velocity) and gridMass (float x NC), as the shaders do.
+// They back the single-pass C ABI and the dense engine path.
+#include "mpm_internal.h"
+#include "mpm_particle.cuh"
+#include "mpm_scan_kernel.cuh"
+
+namespace nebula {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline uint32_t blocksFor(uint64_t n, int t = kThreads) { return uint32_t((n + t - 1) / t); }
+
+// mpm_hash_count.comp:7-14 (+ the slot the sort would take)
+__global__ void __launch_bounds__(kThreads) k_bin_count(SubstepParams P, const float4* __restrict__ pos, uint32_t n, uint32_t* cellCount,
+                                                        uint32_t* key, uint32_t* rank) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = pos[i];
+  int cx, cy, cz;
+  cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
+  uint32_t c = mortonEncode(cx, cy, cz);
+  // warp-aggregated increment: lanes sharing a cell take consecutive slots
+  uint32_t peers = __match_any_sync(__activemask(), c);
+  int leader = __ffs(peers) - 1;
+  uint32_t lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (int(lane) == leader) base = atomicAdd(cellCount + c, uint32_t(__popc(peers)));
+  base = __shfl_sync(peers, base, leader);
+  key[i] = c;
+  rank[i] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// mpm_hash_sort.comp:7-15 with the slot taken at count time
+__global__ void __launch_bounds__(kThreads) k_bin_scatter(uint32_t n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank,
+                                                          const uint32_t* __restrict__ cellStart, uint32_t* sortedTmp, uint32_t* err) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t slot = cellStart[key[i]] + rank[i];
+  if (slot < n) sortedTmp[slot] = i;
+  else atomicOr(err, kErrBinRange);  // only after an expired scan wait
+}
+
+// In-cell canonical order (ascending particle index): each slot finds its
+// rank among the slots of its own cell.
+__global__ void __launch_bounds__(kThreads) k_bin_canon(uint32_t n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ cellStart,
+                                                        const uint32_t* __restrict__ cellCount, const uint32_t* __restrict__ sortedTmp,
+                                                        uint32_t* sorted, uint32_t* err) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t i = sortedTmp[s];
+  if (i >= n) {
+    atomicOr(err, kErrBinRange);
+    return;
+  }
+  uint32_t c = key[i];
+  uint32_t st = cellStart[c], cnt = cellCount[c];
+  if (st > n || cnt > n - st) {
+    atomicOr(err, kErrBinRange);
+    return;
+  }
+  uint32_t r = 0;
+  for (uint32_t j = st; j < st + cnt; ++j) r += sortedTmp[j] < i ? 1u : 0u;
+  sorted[st + r] = i;
+}
+
+// P2G: one thread per sorted slot, contributions added to the dense grid.
+__global__ void __launch_bounds__(kThreads) k_p2g_dense(SubstepParams P, StatePtrs st, const uint32_t* __restrict__ sorted, uint32_t n,
+                                                        float4* gridMom, float* gridMass) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t p = sorted[t];
+  if (p >= n) return;  // a caller-supplied order with an out-of-range index
+  PState s;
+  s.P = st.f[0][p]; s.v = st.f[1][p];
+  s.F0 = st.f[2][p]; s.F1 = st.f[3][p]; s.F2 = st.f[4][p];
+  s.B0 = st.f[5][p]; s.B1 = st.f[6][p]; s.B2 = st.f[7][p];
+  p2gParticle(P, s, P.dt, [&](int nx, int ny, int nz, float mx, float my, float mz, float m) {
+    uint32_t nid = mortonEncode(nx, ny, nz);
+    float* g = reinterpret_cast<float*>(gridMom + nid);
+    atomicAdd(g + 0, mx);
+    atomicAdd(g + 1, my);
+    atomicAdd(g + 2, mz);
+    atomicAdd(gridMass + nid, m);
+  });
+}
+
+// mpm_grid_update.comp + mpm_nanovdb_bc.comp, one thread per node.
+__global__ void __launch_bounds__(kThreads) k_grid_dense(SubstepParams P, float4* gridMom, const float* __restrict__ gridMass) {
+  uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= P.hashCells) return;
+  float mass = gridMass[gid];
+  if (mass < 1e-10f) return;
+  float4 mom = gridMom[gid];
+  int ix, iy, iz;
+  mortonDecode(gid, ix, iy, iz);
+  float3 v, vo;
+  gridNode(P, ix, iy, iz, mass, mom.x, mom.y, mom.z, v, vo);
+  gridMom[P.hashCells + gid] = make_float4(vo.x, vo.y, vo.z, 0.f);
+  gridMom[gid] = make_float4(v.x, v.y, v.z, 0.f);
+}
+
+struct DenseGrid {
+  const float4* mom;
+  const float* mass;
+  uint32_t nc;
+  __device__ __forceinline__ bool node(int x, int y, int z, float& m, float3& v, float3& vo) const {
+    uint32_t nid = mortonEncode(x, y, z);
+    m = __ldg(mass + nid);
+    if (m < 1e-10f) return false;
+    float4 a = __ldg(mom + nid);
+    float4 b = __ldg(mom + nc + nid);
+    v = make_float3(a.x, a.y, a.z);
+    vo = make_float3(b.x, b.y, b.z);
+    return true;
+  }
+};
+
+__global__ void __launch_bounds__(kThreads) k_g2p_dense(SubstepParams P, StatePtrs st, uint32_t n, const float4* __restrict__ gridMom,
+                                                        const float* __restrict__ gridMass, uint32_t* err) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  PState s;
+  s.P = st.f[0][p]; s.v = st.f[1][p];
+  s.F0 = st.f[2][p]; s.F1 = st.f[3][p]; s.F2 = st.f[4][p];
+  s.B0 = st.f[5][p]; s.B1 = st.f[6][p]; s.B2 = st.f[7][p];
+  DenseGrid g{gridMom, gridMass, P.hashCells};
+  g2pParticle(P, s, g, P.dt);
+  if (err && !(isfinite(s.P.x) && isfinite(s.P.y) && isfinite(s.P.z))) atomicOr(err, kErrNonFinite);
+  st.f[0][p] = s.P; st.f[1][p] = s.v;
+  st.f[2][p] = s.F0; st.f[3][p] = s.F1; st.f[4][p] = s.F2;
+  st.f[5][p] = s.B0; st.f[6][p] = s.B1; st.f[7][p] = s.B2;
+}
+
+}  // namespace
+
+size_t scanWorkspaceBytes(uint64_t n) { return (size_t(scanTiles(n)) + 2) * sizeof(unsigned long long); }
+
+cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, const BinBuffers& b, cudaStream_t s, uint64_t* launches) {
+  const uint64_t nc = P.hashCells;
+  cudaError_t e = cudaMemsetAsync(b.cellCount, 0, nc * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  if (n > 0) {
+    k_bin_count<<<blocksFor(n), kThreads, 0, s>>>(P, pos, n, b.cellCount, b.key, b.rank);
+    ++*launches;
+  }
+  const uint32_t tiles = scanTiles(nc);
+  e = cudaMemsetAsync(b.tileState, 0, (size_t(tiles) + 1) * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  k_scan_exclusive<<<tiles, kScanThreads, 0, s>>>(b.cellCount, b.cellStart, b.cellEnd, nc, b.tileState, b.tileCounter, b.err, nullptr);
+  ++*launches;
+  if (n > 0) {
+    k_bin_scatter<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.rank, b.cellStart, b.sortedTmp, b.err);
+    k_bin_canon<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
+    *launches += 2;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launchP2GDense(const SubstepParams& P, StatePtrs st, const uint32_t* sorted, uint32_t n, float4* gridMom, float* gridMass,
+                           cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_p2g_dense<<<blocksFor(n), kThreads, 0, s>>>(P, st, sorted, n, gridMom, gridMass);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchGridDense(const SubstepParams& P, float4* gridMom, const float* gridMass, cudaStream_t s, uint64_t* launches) {
+  k_grid_dense<<<blocksFor(P.hashCells), kThreads, 0, s>>>(P, gridMom, gridMass);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchG2PDense(const SubstepParams& P, StatePtrs st, uint32_t n, const float4* gridMom, const float* gridMass, uint32_t* err,
+                           cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_g2p_dense<<<blocksFor(n), kThreads, 0, s>>>(P, st, n, gridMom, gridMass, err);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+}  // namespace nebula

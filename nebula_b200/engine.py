@@ -1,0 +1,265 @@
+"""Python binding of the C++ ``nebula::MPMEngine`` (include/nebula_mpm.h).
+
+Method names follow the reference's ``MPMEngine`` (src/engine/MPMEngine.h:59-186)
+and ``EngineBase`` force API (src/engine/EngineBase.h:27-31), so code written
+against the reference reads the same:
+
+    eng = MPMEngine(MPMConfig(nx=20, ny=20, nz=20, domainSize=(1,1,1), cellSize=1/64))
+    eng.flip_ratio = -1.0
+    eng.addForce(gravity())
+    eng.step(dt)
+
+Everything runs in the CUDA library; this module only marshals arguments.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi
+from ._capi import call
+from .scenes import COLLIDER_DTYPE, FIELDS, FORCE_DTYPE, MATERIAL_DTYPE
+
+FIELD_INDEX = {f: i for i, f in enumerate(FIELDS)}
+
+
+@dataclass
+class MPMConfig:
+    """MPMConfig (src/engine/MPMEngine.h:22-55)."""
+    nx: int = 32
+    ny: int = 32
+    nz: int = 32
+    domainSize: tuple = (10.0, 10.0, 10.0)
+    cellSize: float = 10.0 / 64.0
+    maxParticles: int = 0
+    E: float = 1e4
+    nu: float = 0.3
+    rho0: float = 1000.0
+
+    def to_c(self) -> _capi.Config:
+        c = _capi.Config()
+        c.nx, c.ny, c.nz = self.nx, self.ny, self.nz
+        c.domainSize[:] = [float(v) for v in self.domainSize]
+        c.cellSize = self.cellSize
+        c.maxParticles = self.maxParticles
+        c.E, c.nu, c.rho0 = self.E, self.nu, self.rho0
+        return c
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    h = getattr(stream, "cuda_stream", None)  # torch.cuda.Stream
+    return C.c_void_p(h) if h else None
+
+
+_PARAM_NAMES = ("restitution", "wall_friction", "numSubsteps", "plasticModel", "q_max", "M_friction", "q_cohesion", "flip_ratio")
+
+
+class MPMEngine:
+    """One MPM scene on the GPU."""
+
+    def __init__(self, cfg: MPMConfig | None = None):
+        cfg = cfg or MPMConfig()
+        self.cfg = cfg
+        h = C.c_void_p()
+        call("nebula_mpm_create", C.byref(cfg.to_c()), C.byref(h))
+        self._h = h
+        self._forces = []
+
+    # ------------------------------------------------------------ lifetime
+    def cleanup(self):
+        if getattr(self, "_h", None) and self._h.value:
+            call("nebula_mpm_destroy", self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.cleanup()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.cleanup()
+
+    # ------------------------------------------------------------ public fields (MPMEngine.h:72-80)
+    def _params(self) -> _capi.Params:
+        p = _capi.Params()
+        call("nebula_mpm_get_params", self._h, C.byref(p))
+        return p
+
+    def __getattr__(self, name):
+        if name in _PARAM_NAMES:
+            return getattr(self._params(), name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in _PARAM_NAMES:
+            p = self._params()
+            setattr(p, name, value)
+            call("nebula_mpm_set_params", self._h, C.byref(p))
+        else:
+            object.__setattr__(self, name, value)
+
+    # ------------------------------------------------------------ tables
+    def setMaterials(self, mats):
+        a = np.ascontiguousarray(np.asarray(mats, dtype=MATERIAL_DTYPE).reshape(-1))
+        call("nebula_mpm_set_materials", self._h, _ptr(a), len(a))
+
+    def setParticleMaterialIds(self, ids):
+        a = np.ascontiguousarray(ids, dtype=np.uint32)
+        call("nebula_mpm_set_particle_material_ids", self._h, _ptr(a), len(a))
+
+    def setColliders(self, cols):
+        a = np.ascontiguousarray(np.asarray(cols, dtype=COLLIDER_DTYPE).reshape(-1))
+        call("nebula_mpm_set_colliders", self._h, _ptr(a), len(a))
+
+    def clearAnalyticColliders(self):
+        call("nebula_mpm_clear_analytic_colliders", self._h)
+
+    def setColliderSDF(self, morton_sdf):
+        a = np.ascontiguousarray(morton_sdf, dtype=np.float32)
+        call("nebula_mpm_set_collider_sdf", self._h, _ptr(a), a.size)
+
+    def setColliderSphere(self, radius, cx, cy, cz):
+        call("nebula_mpm_set_collider_sphere", self._h, radius, cx, cy, cz)
+
+    def clearCollider(self):
+        call("nebula_mpm_clear_collider", self._h)
+
+    def setForces(self, forces):
+        self._forces = list(forces)
+        a = np.zeros(max(1, len(self._forces)), FORCE_DTYPE)
+        for i, f in enumerate(self._forces):
+            a[i] = f
+        call("nebula_mpm_set_forces", self._h, _ptr(a), len(self._forces))
+
+    def addForce(self, f):
+        self.setForces(self._forces + [f])
+
+    def removeForce(self, index: int):
+        fs = list(self._forces)
+        del fs[index]
+        self.setForces(fs)
+
+    def clearForces(self):
+        self.setForces([])
+
+    # ------------------------------------------------------------ particles
+    def appendParticles(self, pos4, vel4) -> int:
+        p = np.ascontiguousarray(pos4, dtype=np.float32).reshape(-1, 4)
+        v = np.ascontiguousarray(vel4, dtype=np.float32).reshape(-1, 4)
+        if p.shape != v.shape:
+            raise ValueError("pos and vel must have the same shape")
+        k = C.c_uint32()
+        call("nebula_mpm_append_particles", self._h, _ptr(p), _ptr(v), p.shape[0], C.byref(k))
+        return k.value
+
+    def resetParticles(self):
+        call("nebula_mpm_reset_particles", self._h)
+
+    def upload_state(self, state: dict):
+        arrs = [np.ascontiguousarray(state[f], dtype=np.float32).reshape(-1, 4) for f in FIELDS]
+        n = arrs[0].shape[0]
+        ptrs = (C.c_void_p * 8)(*[a.ctypes.data for a in arrs])
+        call("nebula_mpm_upload_state", self._h, ptrs, n)
+
+    def liveParticleCount(self) -> int:
+        n = C.c_uint32()
+        call("nebula_mpm_live_count", self._h, C.byref(n))
+        return n.value
+
+    def download(self, field: str) -> np.ndarray:
+        n = self.liveParticleCount()
+        out = np.empty((n, 4), np.float32)
+        call("nebula_mpm_download", self._h, FIELD_INDEX[field], _ptr(out), out.size)
+        return out
+
+    def state(self) -> dict:
+        return {f: self.download(f) for f in FIELDS}
+
+    # ------------------------------------------------------------ stepping
+    def step(self, dt: float, stream=None):
+        """MPMEngine::step: numSubsteps substeps of dt/numSubsteps on `stream`."""
+        call("nebula_mpm_step", self._h, float(dt), _stream_handle(stream))
+
+    def run_substeps(self, sub_dt: float, count: int, stream=None):
+        """`count` substeps of length sub_dt (one step() call with numSubsteps=count)."""
+        old = self.numSubsteps
+        self.numSubsteps = int(count)
+        try:
+            self.step(sub_dt * count, stream)
+        finally:
+            self.numSubsteps = old
+
+    def sync(self):
+        call("nebula_mpm_sync", self._h)
+
+    def stats(self) -> dict:
+        s = _capi.Stats()
+        call("nebula_mpm_get_stats", self._h, C.byref(s))
+        return {k: (list(getattr(s, k)) if k == "grid_res" else getattr(s, k)) for k, _ in s._fields_}
+
+    # ------------------------------------------------------------ device timing
+    PHASES = ("bin", "p2g", "grid", "g2p", "g2p2g", "other")
+
+    def profile(self, enable: bool = True):
+        call("nebula_mpm_profile_enable", self._h, int(bool(enable)))
+
+    def profile_read(self, reset: bool = True) -> dict:
+        ms = np.zeros(6, np.float64)
+        ln = np.zeros(6, np.uint64)
+        call("nebula_mpm_profile_read", self._h, _ptr(ms), _ptr(ln), int(reset))
+        return {p: (float(ms[i]), int(ln[i])) for i, p in enumerate(self.PHASES)}
+
+    # ------------------------------------------------------------ reference-format exports
+    def export_bins(self):
+        st = self.stats()
+        nc, n = st["hash_cells"], st["live_particles"]
+        cnt = np.empty(nc, np.uint32)
+        off = np.empty(nc, np.uint32)
+        srt = np.empty(max(1, n), np.uint32)
+        call("nebula_mpm_export_bins", self._h, _ptr(cnt), _ptr(off), _ptr(srt))
+        return cnt, off, srt[:n]
+
+    def export_grid(self, dt: float):
+        nc = self.stats()["hash_cells"]
+        mom = np.empty((nc, 4), np.float32)
+        mass = np.empty(nc, np.float32)
+        call("nebula_mpm_export_grid", self._h, float(dt), _ptr(mom), _ptr(mass))
+        return mom, mass
+
+
+def engine_for_scene(scene, capacity: int | None = None) -> MPMEngine:
+    """An engine configured like `scene` (domain, materials, forces, colliders,
+    SDF, transfer mode) holding the scene's particle state."""
+    sp = scene.params
+    cfg = MPMConfig(nx=0, ny=0, nz=0, domainSize=tuple(sp.domain_size), cellSize=sp.cell_size,
+                    maxParticles=int(capacity or scene.n), E=1e4, nu=0.3, rho0=sp.rho0)
+    eng = MPMEngine(cfg)
+    eng.flip_ratio = sp.flip_ratio
+    eng.M_friction = sp.M_friction
+    eng.q_cohesion = sp.q_cohesion
+    eng.q_max = sp.q_max
+    eng.plasticModel = sp.plastic_model
+    if sp.materials:
+        eng.setMaterials(sp.materials_array()[: len(sp.materials)])
+    if sp.forces:
+        eng.setForces(list(sp.forces))
+    if sp.colliders:
+        eng.setColliders(sp.colliders_array()[: len(sp.colliders)])
+    if scene.sdf is not None:
+        eng.setColliderSDF(scene.sdf)
+    eng.upload_state(scene.state)
+    return eng

@@ -1,0 +1,394 @@
+"""Seeded synthetic MPM scenes and the per-substep parameter record.
+
+Every scene is generated from a counter-based SplitMix64 stream, so the oracle
+and the CUDA engine see bit-identical inputs.  Records mirror the reference's
+host structs:
+
+* ``MATERIAL_DTYPE`` -- ``MaterialParams`` (src/core/MaterialParams.h:16-38)
+* ``COLLIDER_DTYPE`` -- ``ColliderPrimitive`` (src/core/Collider.h:19-29)
+* ``FORCE_DTYPE``    -- ``ForceGPU`` (src/core/Force.h:27-32)
+
+``StepParams`` carries the scalar fields of ``MPMSimPC`` (src/core/MPMSimPC.h:14-77)
+that the substep reads, built like ``MPMEngine::buildPC`` (src/engine/MPMEngine.cpp:356-400).
+
+The workloads are synthetic stand-ins with the shapes and value ranges of the
+five measured configurations: an elastic block, a jelly/sand multimaterial
+scene, a 1M-particle Drucker-Prager slope over a terrain SDF, a 64-scene mix,
+and a differentiable elastic block.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MAT_ELASTIC, MAT_VON_MISES, MAT_DRUCKER_PRAGER, MAT_GRANULAR_POWDER, MAT_FLUID, MAT_VISCOPLASTIC_MUD = range(6)
+COLL_PLANE, COLL_SPHERE, COLL_BOX, COLL_CAPSULE = range(4)
+FORCE_GRAVITY, FORCE_CONSTANT_WIND = 0, 1
+
+MATERIAL_DTYPE = np.dtype([
+    ("mu", "<f4"), ("lambda", "<f4"), ("rho0", "<f4"), ("model", "<u4"),
+    ("M_friction", "<f4"), ("q_cohesion", "<f4"), ("q_max", "<f4"), ("bulkK", "<f4"),
+    ("fluidGamma", "<f4"), ("viscosity", "<f4"), ("hardening", "<f4"), ("xi", "<f4"),
+    ("pad", "<f4", (4,)),
+])
+COLLIDER_DTYPE = np.dtype([
+    ("type", "<u4"), ("pos", "<f4", (3,)), ("nrm", "<f4", (3,)), ("radius", "<f4"),
+    ("vel", "<f4", (3,)), ("restitution", "<f4"), ("friction", "<f4"), ("pad", "<f4", (3,)),
+])
+FORCE_DTYPE = np.dtype([("type", "<u2"), ("affectMask", "<u2"), ("data", "<f4", (7,))])
+assert MATERIAL_DTYPE.itemsize == 64 and COLLIDER_DTYPE.itemsize == 64 and FORCE_DTYPE.itemsize == 32
+
+FIELDS = ("P", "v", "F0", "F1", "F2", "B0", "B1", "B2")
+
+
+# ----------------------------------------------------------------------------- RNG
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, n: int, stream: int = 0) -> np.ndarray:
+    """n counter-based SplitMix64 outputs for (seed, stream): value i mixes
+    seed*2^32 + stream*2^48... (plus (i+1) golden-ratio increments)."""
+    with np.errstate(over="ignore"):
+        base = np.uint64((seed * 0x100000001B3 + stream * 0xD1B54A32D192ED03) & 0xFFFFFFFFFFFFFFFF)
+        z = base + (np.arange(1, n + 1, dtype=np.uint64) * _GOLDEN)
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform(seed: int, n: int, stream: int = 0, lo=0.0, hi=1.0) -> np.ndarray:
+    """float64 uniforms in [lo, hi) from the top 53 bits of SplitMix64."""
+    u = (splitmix64(seed, n, stream) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return lo + (hi - lo) * u
+
+
+# ----------------------------------------------------------------------------- domain
+def grid_res(domain_size, cell_size):
+    """domain::gridRes (src/core/Domain.h:14-17): max(1, ceil(size / h)) in float32."""
+    ds = np.asarray(domain_size, np.float32)
+    h = np.float32(max(np.float32(cell_size), np.float32(1e-6)))
+    r = np.ceil(ds / h)
+    return tuple(int(max(1, v)) for v in r)
+
+
+def morton_cube_res(res):
+    """domain::mortonCubeRes (src/core/Domain.h:25-30): next pow2 >= max axis."""
+    m = max(max(res), 1)
+    p = 1
+    while p < m:
+        p <<= 1
+    return p
+
+
+def hash_cells(res):
+    """domain::hashCells (src/core/Domain.h:34-37): cubeRes^3."""
+    c = morton_cube_res(res)
+    return c * c * c
+
+
+def n_groups(cells):
+    return (cells + 255) // 256
+
+
+def _expand(v):
+    v = v.astype(np.uint64)
+    v = (v | (v << np.uint64(16))) & np.uint64(0x030000FF)
+    v = (v | (v << np.uint64(8))) & np.uint64(0x0300F00F)
+    v = (v | (v << np.uint64(4))) & np.uint64(0x030C30C3)
+    v = (v | (v << np.uint64(2))) & np.uint64(0x09249249)
+    return v
+
+
+def morton_encode(x, y, z):
+    """Vectorised Morton code x | y<<1 | z<<2 (mpm_common.glsl:178-181)."""
+    x = np.asarray(x)
+    return (_expand(x) | (_expand(np.asarray(y)) << np.uint64(1)) | (_expand(np.asarray(z)) << np.uint64(2))).astype(np.uint32)
+
+
+def lame(E, nu):
+    """calcMu / calcLambda (src/core/MaterialParams.h:42-43), float32."""
+    E = np.float32(E)
+    nu = np.float32(nu)
+    mu = E / (np.float32(2.0) * (np.float32(1.0) + nu))
+    lam = E * nu / ((np.float32(1.0) + nu) * (np.float32(1.0) - np.float32(2.0) * nu))
+    return float(mu), float(lam)
+
+
+def material(model, E, nu, rho0, M_friction=0.0, q_cohesion=0.0, q_max=1e5, bulkK=0.0, viscosity=0.0):
+    m = np.zeros(1, MATERIAL_DTYPE)
+    mu, lam = lame(E, nu)
+    m["mu"], m["lambda"], m["rho0"], m["model"] = mu, lam, rho0, model
+    m["M_friction"], m["q_cohesion"], m["q_max"], m["bulkK"], m["viscosity"] = M_friction, q_cohesion, q_max, bulkK, viscosity
+    return m[0]
+
+
+def gravity(g=(0.0, -9.8, 0.0)):
+    """A GravityForce record with direction (0,1,0)-style packing: dir=g/|g|, strength=|g|."""
+    f = np.zeros(1, FORCE_DTYPE)
+    g = np.asarray(g, np.float64)
+    s = float(np.linalg.norm(g))
+    f["type"] = FORCE_GRAVITY
+    f["data"][0, :3] = g / s if s > 0 else 0.0
+    f["data"][0, 3] = s
+    return f[0]
+
+
+def sphere_collider(center, radius, vel=(0, 0, 0), restitution=0.3, friction=0.0):
+    c = np.zeros(1, COLLIDER_DTYPE)
+    c["type"] = COLL_SPHERE
+    c["pos"][0] = center
+    c["radius"] = radius
+    c["vel"][0] = vel
+    c["restitution"], c["friction"] = restitution, friction
+    return c[0]
+
+
+@dataclass
+class StepParams:
+    """Scalar parameters of one substep (the MPMSimPC fields the kernels read)."""
+    dt: float
+    cell_size: float
+    domain_size: tuple
+    world_min: tuple = (0.0, 0.0, 0.0)
+    flip_ratio: float = -1.0
+    materials: list = field(default_factory=list)
+    colliders: list = field(default_factory=list)
+    forces: list = field(default_factory=list)
+    mu_lame: float = 0.0
+    lambda_lame: float = 0.0
+    rho0: float = 1000.0
+    M_friction: float = 0.577
+    q_cohesion: float = 0.0
+    q_max: float = 1e5
+    plastic_model: int = 0
+
+    @property
+    def grid_res(self):
+        return grid_res(self.domain_size, self.cell_size)
+
+    @property
+    def cube_res(self):
+        return morton_cube_res(self.grid_res)
+
+    @property
+    def hash_cells(self):
+        return hash_cells(self.grid_res)
+
+    @property
+    def world_max(self):
+        return tuple(float(np.float32(a) + np.float32(b)) for a, b in zip(self.world_min, self.domain_size))
+
+    def materials_array(self):
+        a = np.zeros(max(1, len(self.materials)), MATERIAL_DTYPE)
+        for i, m in enumerate(self.materials):
+            a[i] = m
+        return a
+
+    def colliders_array(self):
+        a = np.zeros(max(1, len(self.colliders)), COLLIDER_DTYPE)
+        for i, c in enumerate(self.colliders):
+            a[i] = c
+        return a
+
+    def forces_array(self):
+        a = np.zeros(max(1, len(self.forces)), FORCE_DTYPE)
+        for i, f in enumerate(self.forces):
+            a[i] = f
+        return a
+
+
+@dataclass
+class Scene:
+    name: str
+    params: StepParams
+    state: dict
+    substeps: int
+    sdf: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.state["P"].shape[0]
+
+
+def make_state(pos, vp, vel=None, mat_ids=None) -> dict:
+    """Particle state in the reference layout (MPMEngine.cpp:46-53): 8 float4 per
+    particle; v.w carries the material id bits, F = I, B = 0, stress = 0."""
+    n = pos.shape[0]
+    st = {f: np.zeros((n, 4), np.float32) for f in FIELDS}
+    st["P"][:, :3] = pos
+    st["P"][:, 3] = vp
+    if vel is not None:
+        st["v"][:, :3] = vel
+    ids = np.zeros(n, np.uint32) if mat_ids is None else np.asarray(mat_ids, np.uint32)
+    st["v"][:, 3] = ids.view(np.float32)
+    st["F0"][:, 0] = 1.0
+    st["F1"][:, 1] = 1.0
+    st["F2"][:, 2] = 1.0
+    return st
+
+
+def jittered_lattice(seed, stream, counts, spacing, origin, jitter):
+    """Lattice of counts=(nx,ny,nz) points (x fastest, then z, then y), spacing
+    `spacing`, lower corner `origin`, each axis jittered by U(-jitter, +jitter)."""
+    nx, ny, nz = counts
+    iy, iz, ix = np.meshgrid(np.arange(ny), np.arange(nz), np.arange(nx), indexing="ij")
+    p = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.float64) * spacing
+    p += np.asarray(origin, np.float64)
+    n = p.shape[0]
+    j = uniform(seed, 3 * n, stream, -jitter, jitter).reshape(n, 3)
+    return (p + j).astype(np.float32)
+
+
+# ----------------------------------------------------------------------------- configs
+def elastic_block(seed=1, n_side=20, res=64, substeps=100, dt=1e-4, flip_ratio=-1.0):
+    """8,000-particle elastic block: 20^3 lattice, spacing 0.5h, jitter +/-0.25h,
+    centre (0.5, 0.7, 0.5) of the unit cube, 64^3 grid, E=1e4 nu=0.3 rho=1,
+    gravity -9.8 y, dt=1e-4, APIC."""
+    h = 1.0 / res
+    sp = 0.5 * h
+    half = sp * (n_side - 1) / 2.0
+    origin = (0.5 - half, 0.7 - half, 0.5 - half)
+    pos = jittered_lattice(seed, 0, (n_side, n_side, n_side), sp, origin, 0.25 * h)
+    vp = np.float32(sp) ** 3
+    params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=flip_ratio,
+                        materials=[material(MAT_ELASTIC, 1e4, 0.3, 1.0)], forces=[gravity()])
+    params.mu_lame, params.lambda_lame = lame(1e4, 0.3)
+    params.rho0 = 1.0
+    return Scene("elastic_block_8k_64", params, make_state(pos, vp), substeps)
+
+
+def multimaterial(seed=2, res=128, substeps=200, dt=5e-5):
+    """80,000 particles on 128^3: a 40,000-particle jelly cube (Hencky E=5e3,
+    rho 1000) dropped on a 40,000-particle Drucker-Prager sand slab (E=3.5e5,
+    friction 30 deg, rho 1600), nu=0.3, APIC, dt=5e-5."""
+    h = 1.0 / res
+    sp = 0.5 * h
+    # jelly: 35^3 lattice truncated to its first 40,000 points (top layer partial)
+    jel = jittered_lattice(seed, 0, (35, 35, 35), sp, (0.5 - 17 * sp, 0.35, 0.5 - 17 * sp), 0.25 * h)[:40000]
+    # sand slab: 100 x 4 x 100 points resting above the floor band
+    sand = jittered_lattice(seed, 1, (100, 4, 100), sp, (0.5 - 49.5 * sp, 3.0 * h, 0.5 - 49.5 * sp), 0.25 * h)
+    pos = np.concatenate([jel, sand])
+    ids = np.concatenate([np.zeros(40000, np.uint32), np.ones(40000, np.uint32)])
+    vp = np.float32(sp) ** 3
+    mats = [material(MAT_ELASTIC, 5e3, 0.3, 1000.0),
+            material(MAT_DRUCKER_PRAGER, 3.5e5, 0.3, 1600.0, M_friction=math.tan(math.radians(30.0)))]
+    params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
+                        materials=mats, forces=[gravity()])
+    params.mu_lame, params.lambda_lame = lame(5e3, 0.3)
+    return Scene("multimaterial_80k_128", params, make_state(pos, vp, mat_ids=ids), substeps)
+
+
+def terrain_height(seed, x, z):
+    """Synthetic terrain: 0.08 + sum of 8 seeded Gaussian ridges (height 0.05-0.2,
+    width 0.05-0.15, each along a seeded line) + one linear channel (depth 0.04)."""
+    u = uniform(seed, 8 * 5, 7).reshape(8, 5)
+    H = np.full(np.broadcast(x, z).shape, 0.08)
+    for i in range(8):
+        hgt = 0.05 + 0.15 * u[i, 0]
+        wid = 0.05 + 0.10 * u[i, 1]
+        cx, cz = u[i, 2], u[i, 3]
+        ang = math.pi * u[i, 4]
+        d = (x - cx) * math.sin(ang) - (z - cz) * math.cos(ang)
+        H = H + hgt * np.exp(-(d / wid) ** 2)
+    d = (x - 0.5) * math.sin(0.3) - (z - 0.5) * math.cos(0.3)
+    H = H - 0.04 * np.exp(-(d / 0.04) ** 2)
+    return H
+
+
+def terrain_sdf(seed, res, h):
+    """Dense Morton-ordered fp32 SDF (sdf[morton(ix,iy,iz)] = y - H(x,z) at cell centres),
+    the layout of MPMEngine::setColliderSDF (src/engine/MPMEngine.cpp:204-209)."""
+    c = (np.arange(res, dtype=np.float64) + 0.5) * h
+    X, Z = np.meshgrid(c, c, indexing="ij")           # [ix, iz]
+    H = terrain_height(seed, X, Z)                      # [ix, iz]
+    cube = morton_cube_res((res, res, res))
+    sdf = np.full(cube ** 3, 1e6, np.float32)
+    ix, iy, iz = np.meshgrid(np.arange(res), np.arange(res), np.arange(res), indexing="ij")
+    codes = morton_encode(ix.ravel(), iy.ravel(), iz.ravel())
+    vals = (c[iy.ravel()] - H[ix.ravel(), iz.ravel()]).astype(np.float32)
+    sdf[codes] = vals
+    return sdf, H
+
+
+def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, with_sdf=True):
+    """1,000,000 Drucker-Prager particles (friction 35 deg, E=1.4e5, nu=0.3,
+    rho 1600) as a jittered slab above a seeded terrain SDF on a 256^3 grid,
+    APIC, dt=2e-5."""
+    h = 1.0 / res
+    sp = 0.5 * h
+    nx, ny, nz = n_side
+    ox = 0.5 - sp * (nx - 1) / 2.0
+    oz = 0.5 - sp * (nz - 1) / 2.0
+    pos = jittered_lattice(seed, 0, (nx, ny, nz), sp, (ox, 0.0, oz), 0.25 * h)
+    sdf, H = (terrain_sdf(seed, res, h) if with_sdf else (None, None))
+    if H is not None:
+        # the slab starts 2h above the highest terrain point and falls onto it
+        pos[:, 1] += np.float32(H.max() + 2.0 * h)
+    else:
+        pos[:, 1] += np.float32(0.3)
+    vp = np.float32(sp) ** 3
+    mats = [material(MAT_DRUCKER_PRAGER, 1.4e5, 0.3, 1600.0, M_friction=math.tan(math.radians(35.0)))]
+    params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
+                        materials=mats, forces=[gravity()])
+    params.mu_lame, params.lambda_lame = lame(1.4e5, 0.3)
+    return Scene("slope_flow_1m_256", params, make_state(pos, vp), substeps, sdf=sdf)
+
+
+def batch_mix(seed=4, n_scenes=64, substeps=200, dt=1e-4, nmin=2000, nmax=200000):
+    """64 independent scenes: particle counts log-uniform in [2e3, 2e5], grids
+    64^3 / 96^3 / 128^3 (unit cube), a jittered box with initial velocity
+    U[-1,1]^3, ELASTIC or VON_MISES, and one sphere collider of radius 0.1
+    moving with a seeded velocity."""
+    scenes = []
+    u = uniform(seed, n_scenes * 8, 11).reshape(n_scenes, 8)
+    for s in range(n_scenes):
+        n_target = int(round(math.exp(math.log(nmin) + (math.log(nmax) - math.log(nmin)) * u[s, 0])))
+        res = (64, 96, 128)[min(2, int(u[s, 1] * 3))]
+        h = float(np.float32(1.0) / np.float32(res))
+        sp = 0.5 * h
+        side = max(2, int(round(n_target ** (1.0 / 3.0))))
+        nxz = side
+        ny = max(1, n_target // (nxz * nxz))
+        cnt = (nxz, ny, nxz)
+        n = nxz * ny * nxz
+        ox = 0.5 - sp * (nxz - 1) / 2.0
+        oy = 0.45
+        pos = jittered_lattice(seed * 1000 + s, 0, cnt, sp, (ox, oy, ox), 0.25 * h)
+        vel = uniform(seed * 1000 + s, 3, 1, -1.0, 1.0).astype(np.float32)
+        vels = np.broadcast_to(vel, (n, 3)).copy()
+        model = MAT_ELASTIC if u[s, 2] < 0.5 else MAT_VON_MISES
+        q_max = 50.0 + 450.0 * u[s, 3]
+        mats = [material(model, 1e4, 0.3, 1000.0, q_max=q_max)]
+        cvel = (uniform(seed * 1000 + s, 3, 2, -0.5, 0.5)).astype(np.float32)
+        col = sphere_collider((0.5, 0.25, 0.5), 0.1, vel=tuple(cvel))
+        params = StepParams(dt=dt, cell_size=h, domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
+                            materials=mats, forces=[gravity()], colliders=[col])
+        params.mu_lame, params.lambda_lame = lame(1e4, 0.3)
+        scenes.append(Scene("batch_%02d" % s, params, make_state(pos, np.float32(sp) ** 3, vel=vels), substeps))
+    return scenes
+
+
+def diff_block(seed=5, n=50000, res=64, substeps=200, dt=1e-4):
+    """50,000-particle elastic block for the adjoint: 37x37x37 lattice truncated to
+    50,000 points, per-particle E log-uniform in [5e3, 5e4], initial velocity
+    (0.3, 0, -0.2) + U(+/-0.05), APIC, dt=1e-4; target point seeded."""
+    h = 1.0 / res
+    sp = 0.5 * h
+    side = 37
+    pos = jittered_lattice(seed, 0, (side, side, side), sp, (0.5 - 18 * sp, 0.5, 0.5 - 18 * sp), 0.25 * h)[:n]
+    noise = uniform(seed, 3 * n, 1, -0.05, 0.05).reshape(n, 3)
+    vel = (np.array([0.3, 0.0, -0.2]) + noise).astype(np.float32)
+    E = np.exp(uniform(seed, n, 2, math.log(5e3), math.log(5e4))).astype(np.float32)
+    target = (np.array([0.5, 0.5, 0.5]) + uniform(seed, 3, 3, -0.05, 0.05)).astype(np.float32)
+    params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
+                        materials=[material(MAT_ELASTIC, 1e4, 0.3, 1000.0)], forces=[gravity()])
+    params.mu_lame, params.lambda_lame = lame(1e4, 0.3)
+    sc = Scene("diff_block_50k_64", params, make_state(pos, np.float32(sp) ** 3, vel=vel), substeps)
+    sc.extra = {"E": E, "nu": 0.3, "target": target, "checkpoint_every": 20}
+    return sc

@@ -1,0 +1,301 @@
+"""CPU oracle for the MPMEngine substep -- TEST INFRASTRUCTURE ONLY.
+
+This package is the parity checker for the CUDA path and the timed CPU
+baseline.  Only ``tests/``, ``bench.py`` (its ``cpu_baseline`` leg and the
+``--impl reference`` arm) and ``__graft_entry__.smoke()`` may import it; the
+product package ``nebula_b200`` never does.
+
+``mpm_oracle.cpp`` restates the reference's shaders (see its header for the
+file:line map) in C++ templated on precision; this module builds it with g++
+and drives it through ctypes.  Modes:
+
+* ``"ref32"`` -- float everywhere, the shaders' own precision and algorithm;
+* ``"mixed"`` -- float state, float64 SVD/stress inside the plastic return
+  maps (the CUDA path's precision policy);
+* ``"fp64"``  -- float64 everywhere (error statements, finite differences).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "mpm_oracle.cpp"
+LIB = HERE / "libmpm_oracle.so"
+
+MODES = {"ref32": 0, "mixed": 1, "fp64": 2}
+FIELDS = ("P", "v", "F0", "F1", "F2", "B0", "B1", "B2")
+
+
+class orc_params(C.Structure):
+    _fields_ = [
+        ("dt", C.c_float),
+        ("cellSize", C.c_float),
+        ("gridRes", C.c_uint32 * 3),
+        ("hashCells", C.c_uint32),
+        ("worldMin", C.c_float * 3),
+        ("worldMax", C.c_float * 3),
+        ("flip_ratio", C.c_float),
+        ("materialCount", C.c_uint32),
+        ("mu_lame", C.c_float),
+        ("lambda_lame", C.c_float),
+        ("rho0", C.c_float),
+        ("M_friction", C.c_float),
+        ("q_cohesion", C.c_float),
+        ("q_max", C.c_float),
+        ("plasticModel", C.c_uint32),
+        ("colliderCount", C.c_uint32),
+        ("forceCount", C.c_uint32),
+    ]
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle into ``oracle/libmpm_oracle.so`` (g++, OpenMP)."""
+    if LIB.exists() and not force and LIB.stat().st_mtime >= SRC.stat().st_mtime:
+        return LIB
+    tmp = LIB.with_suffix(".so.tmp%d" % os.getpid())
+    cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
+           "-o", str(tmp), str(SRC)]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp = C.c_void_p
+        L.orc_create.restype = vp
+        L.orc_create.argtypes = [C.c_int]
+        for name, args in [
+            ("orc_destroy", [vp]),
+            ("orc_set_params", [vp, C.POINTER(orc_params)]),
+            ("orc_set_tables", [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32]),
+            ("orc_set_sdf", [vp, vp]),
+            ("orc_set_state", [vp] + [vp] * 8 + [C.c_uint32]),
+            ("orc_get_state", [vp] + [vp] * 8),
+            ("orc_get_mat_ids", [vp, vp]),
+            ("orc_set_grid", [vp, vp, vp]),
+            ("orc_get_grid", [vp, vp, vp]),
+            ("orc_set_bins", [vp, vp, vp, vp]),
+            ("orc_get_bins", [vp, vp, vp, vp]),
+            ("orc_zero_grid", [vp]),
+            ("orc_bin", [vp]),
+            ("orc_p2g", [vp]),
+            ("orc_grid_update", [vp]),
+            ("orc_sdf_bc", [vp]),
+            ("orc_g2p", [vp]),
+            ("orc_substep", [vp]),
+            ("orc_run", [vp, C.c_uint32]),
+            ("orc_set_num_threads", [C.c_int]),
+            ("orc_morton_decode", [C.c_uint32, vp]),
+            ("orc_hencky", [vp, C.c_float, C.c_float, vp, C.c_int]),
+            ("orc_svd3", [vp, vp, vp, vp]),
+            ("orc_project", [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, vp]),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None
+        L.orc_num_threads.restype = C.c_int
+        L.orc_bspline2.restype = C.c_float
+        L.orc_bspline2.argtypes = [C.c_float]
+        L.orc_bspline2g.restype = C.c_float
+        L.orc_bspline2g.argtypes = [C.c_float]
+        L.orc_morton_encode.restype = C.c_uint32
+        L.orc_morton_encode.argtypes = [C.c_uint32] * 3
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def make_params(sp) -> orc_params:
+    """Build ``orc_params`` from a ``nebula_b200.scenes.StepParams``-like object."""
+    p = orc_params()
+    p.dt = sp.dt
+    p.cellSize = sp.cell_size
+    p.gridRes[:] = list(sp.grid_res)
+    p.hashCells = sp.hash_cells
+    p.worldMin[:] = list(sp.world_min)
+    p.worldMax[:] = list(sp.world_max)
+    p.flip_ratio = sp.flip_ratio
+    p.materialCount = len(sp.materials)
+    p.mu_lame = sp.mu_lame
+    p.lambda_lame = sp.lambda_lame
+    p.rho0 = sp.rho0
+    p.M_friction = sp.M_friction
+    p.q_cohesion = sp.q_cohesion
+    p.q_max = sp.q_max
+    p.plasticModel = sp.plastic_model
+    p.colliderCount = len(sp.colliders)
+    p.forceCount = len(sp.forces)
+    return p
+
+
+class Oracle:
+    """One simulated scene on the CPU oracle."""
+
+    def __init__(self, mode: str = "ref32"):
+        self._L = lib()
+        self._h = self._L.orc_create(MODES[mode])
+        self.mode = mode
+        self.n = 0
+        self.nc = 0
+        self._keep = []
+
+    def close(self):
+        if self._h:
+            self._L.orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- setup
+    def set_params(self, sp):
+        p = make_params(sp)
+        self._L.orc_set_params(self._h, C.byref(p))
+        self.nc = sp.hash_cells
+        mats = np.ascontiguousarray(sp.materials_array())
+        cols = np.ascontiguousarray(sp.colliders_array())
+        frc = np.ascontiguousarray(sp.forces_array())
+        self._keep = [mats, cols, frc]
+        self._L.orc_set_tables(self._h, _ptr(mats), len(sp.materials), _ptr(cols), len(sp.colliders),
+                               _ptr(frc), len(sp.forces))
+
+    def set_sdf(self, sdf):
+        if sdf is None:
+            self._L.orc_set_sdf(self._h, None)
+        else:
+            s = np.ascontiguousarray(sdf, dtype=np.float32)
+            assert s.size == self.nc
+            self._L.orc_set_sdf(self._h, _ptr(s))
+
+    def set_state(self, st: dict):
+        arrs = [np.ascontiguousarray(st[f], dtype=np.float32).reshape(-1, 4) for f in FIELDS]
+        n = arrs[0].shape[0]
+        self.n = n
+        self._L.orc_set_state(self._h, *[_ptr(a) for a in arrs], n)
+
+    def get_state(self) -> dict:
+        out = {f: np.empty((self.n, 4), np.float64) for f in FIELDS}
+        self._L.orc_get_state(self._h, *[_ptr(out[f]) for f in FIELDS])
+        ids = np.empty(self.n, np.uint32)
+        self._L.orc_get_mat_ids(self._h, _ptr(ids))
+        out["mat"] = ids
+        return out
+
+    def set_grid(self, mom, mass):
+        m = np.ascontiguousarray(mom, dtype=np.float32).reshape(-1)
+        s = np.ascontiguousarray(mass, dtype=np.float32).reshape(-1)
+        assert m.size == 8 * self.nc and s.size == self.nc
+        self._L.orc_set_grid(self._h, _ptr(m), _ptr(s))
+
+    def get_grid(self):
+        mom = np.empty((2 * self.nc, 4), np.float64)
+        mass = np.empty(self.nc, np.float64)
+        self._L.orc_get_grid(self._h, _ptr(mom), _ptr(mass))
+        return mom, mass
+
+    def set_bins(self, cnt, off, srt):
+        c = np.ascontiguousarray(cnt, dtype=np.uint32)
+        o = np.ascontiguousarray(off, dtype=np.uint32)
+        s = np.ascontiguousarray(srt, dtype=np.uint32)
+        self._L.orc_set_bins(self._h, _ptr(c), _ptr(o), _ptr(s))
+
+    def get_bins(self):
+        cnt = np.empty(self.nc, np.uint32)
+        off = np.empty(self.nc, np.uint32)
+        srt = np.empty(self.n, np.uint32)
+        self._L.orc_get_bins(self._h, _ptr(cnt), _ptr(off), _ptr(srt))
+        return cnt, off, srt
+
+    # ---------------------------------------------------------------- passes
+    def zero_grid(self):
+        self._L.orc_zero_grid(self._h)
+
+    def bin(self):
+        self._L.orc_bin(self._h)
+
+    def p2g(self):
+        self._L.orc_p2g(self._h)
+
+    def grid_update(self):
+        self._L.orc_grid_update(self._h)
+
+    def sdf_bc(self):
+        self._L.orc_sdf_bc(self._h)
+
+    def g2p(self):
+        self._L.orc_g2p(self._h)
+
+    def substep(self):
+        self._L.orc_substep(self._h)
+
+    def run(self, nsub: int):
+        self._L.orc_run(self._h, int(nsub))
+
+
+def set_num_threads(n: int):
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+def bspline2(d: float) -> float:
+    return float(lib().orc_bspline2(d))
+
+
+def bspline2g(d: float) -> float:
+    return float(lib().orc_bspline2g(d))
+
+
+def morton_encode(x: int, y: int, z: int) -> int:
+    return int(lib().orc_morton_encode(x, y, z))
+
+
+def morton_decode(c: int):
+    out = np.zeros(3, np.uint32)
+    lib().orc_morton_decode(c, _ptr(out))
+    return tuple(int(v) for v in out)
+
+
+def hencky(F_glsl: np.ndarray, mu: float, lam: float, fp64: bool = False) -> np.ndarray:
+    """Hencky Kirchhoff stress of a 3x3 F given in GLSL layout (F[c][r])."""
+    f = np.ascontiguousarray(F_glsl, dtype=np.float32).reshape(9)
+    t = np.empty(9, np.float32)
+    lib().orc_hencky(_ptr(f), mu, lam, _ptr(t), int(fp64))
+    return t.reshape(3, 3)
+
+
+def svd3(F_glsl: np.ndarray):
+    f = np.ascontiguousarray(F_glsl, dtype=np.float64).reshape(9)
+    U = np.empty(9)
+    V = np.empty(9)
+    s = np.empty(3)
+    lib().orc_svd3(_ptr(f), _ptr(U), _ptr(s), _ptr(V))
+    return U.reshape(3, 3), s, V.reshape(3, 3)
+
+
+def project(F_glsl: np.ndarray, model: int, mu, lam, M=0.0, qc=0.0, qmax=0.0) -> np.ndarray:
+    f = np.ascontiguousarray(F_glsl, dtype=np.float64).reshape(9)
+    out = np.empty(9)
+    lib().orc_project(_ptr(f), model, mu, lam, M, qc, qmax, _ptr(out))
+    return out.reshape(3, 3)
