@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--impl", default="nebula", choices=["nebula", "reference"])
     ap.add_argument("--workload", default="slope", choices=["slope", "elastic", "multimaterial"])
     ap.add_argument("--substeps", type=int, default=10, help="substeps per step() call")
+    ap.add_argument("--pipeline", default="fused", choices=["fused", "dense"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-substeps", type=int, default=0, help="oracle substeps timed for cpu_baseline (0 = auto)")
     return ap.parse_args()
@@ -210,7 +211,7 @@ def main():
     sp = sc.params
     n = sc.n
     S = args.substeps
-    eng = engine_for_scene(sc)
+    eng = engine_for_scene(sc, pipeline=args.pipeline)
     eng.numSubsteps = S
     stream = torch.cuda.current_stream()
     dt_frame = sp.dt * S
@@ -309,7 +310,7 @@ def main():
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": sc.name, "particles": n, "grid": list(sp.grid_res), "substeps_per_step": S, "dt": sp.dt,
-                   "transfer": "APIC" if sp.flip_ratio < -0.5 else ("FLIP" if flip else "PIC"), "parallelism": "replicas" if world > 1 else "single",
+                   "transfer": "APIC" if sp.flip_ratio < -0.5 else ("FLIP" if flip else "PIC"), "parallelism": "replicas" if world > 1 else "single", "pipeline": args.pipeline,
                    "l2": "inputs larger than L2 (128 MB particle state + 16.7M-cell grid, 126 MB L2)", "active_nodes": active},
         "roofline": roofline,
         "substep": {"ms": substep_ms, "canonical_bytes": canon, "canonical_frac": canon / (substep_ms * 1e-3) / 1e9 / hbm,

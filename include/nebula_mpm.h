@@ -187,6 +187,21 @@ int nebula_mpm_export_grid(nebula_mpm* e, float dt, float* mom, float* mass);
 int nebula_mpm_profile_enable(nebula_mpm* e, int enable);
 int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_t launches[NEBULA_MPM_PHASES], int reset);
 
+/* Substep pipeline (no counterpart in the reference, which always records its
+ * eleven dispatches): FUSED (default) keeps particles in 4x4x4-cell brick
+ * order and runs grid update, fused G2P+P2G, brick scan and permutation per
+ * substep on the bricks particles touch; DENSE runs one kernel per reference
+ * dispatch over the whole Morton grid.  Both compute the same substep. */
+#define NEBULA_MPM_PIPELINE_DENSE 0
+#define NEBULA_MPM_PIPELINE_FUSED 1
+int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
+/* The engine's own brick binning of the current positions (FUSED pipeline):
+ * *numBricks listed bricks (brick id = cell Morton code >> 6) with the first
+ * sorted slot of each (brickStarts has *numBricks + 1 entries, the last = live
+ * count), and the original particle index in each sorted slot.  brickIds and
+ * brickStarts hold hashCells/64 (+1) entries, sortedPids live entries.  Host arrays. */
+int nebula_mpm_export_brick_bins(nebula_mpm* e, uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids);
+
 /* Domain helpers (src/core/Domain.h:14-39). */
 void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint32_t out[3]);
 uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]);

@@ -11,6 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libnebula_mpm.so"
 
 OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_DEVICE, ERR_UNSUPPORTED = range(6)
+PIPELINE_DENSE, PIPELINE_FUSED = 0, 1
 
 
 class NebulaError(RuntimeError):
@@ -74,6 +75,8 @@ _SIGS = {
     "nebula_mpm_sync": (C.c_int, [C.c_void_p]),
     "nebula_mpm_export_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_set_pipeline": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "nebula_mpm_export_grid": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]),
     "nebula_mpm_domain_grid_res": (None, [C.c_float * 3, C.c_float, C.c_uint32 * 3]),

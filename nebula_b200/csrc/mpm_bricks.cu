@@ -1,0 +1,696 @@
+// mpm_bricks.cu -- brick-sparse fused substep kernels (sm_100a).
+//
+// Same per-particle and per-node math as the single-pass kernels
+// (mpm_particle.cuh, restating mpm_p2g.comp, mpm_grid_update.comp,
+// mpm_nanovdb_bc.comp and mpm_g2p.comp), organised for HBM:
+//   * particles live in brick order, read once and written once per substep;
+//   * G2P reads a brick's 6^3 node neighbourhood staged in shared memory;
+//   * P2G accumulates into an 8^3 shared tile and flushes each non-zero node
+//     with one vector reduction to global memory;
+//   * only bricks some particle stencil touched are updated or cleared.
+#include "mpm_bricks.cuh"
+#include "mpm_particle.cuh"
+#include "mpm_scan.cuh"
+
+namespace nebula {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint32_t kBrickScanSpinLimit = 1u << 22;
+constexpr unsigned long long kStFlagAgg = 1ull << 48;
+constexpr unsigned long long kStFlagPre = 2ull << 48;
+constexpr unsigned long long kStValue = (1ull << 48) - 1;
+
+inline uint32_t blocksFor(uint64_t n, int t = kThreads) { return uint32_t((n + t - 1) / t); }
+
+__device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
+
+// Lanes in `mask` holding the same key take consecutive slots of counter[key].
+__device__ __forceinline__ uint32_t warpAggInc(uint32_t mask, uint32_t* counter, uint32_t key) {
+  const uint32_t peers = __match_any_sync(mask, key);
+  const int leader = __ffs(peers) - 1;
+  const uint32_t lane = laneId();
+  uint32_t base = 0;
+  if (int(lane) == leader) base = atomicAdd(counter + key, uint32_t(__popc(peers)));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+// Mark every brick holding a node of the 3x3x3 stencil around cell (cx,cy,cz).
+__device__ __forceinline__ void markStencilBricks(const SubstepParams& P, int cx, int cy, int cz, uint32_t* flag) {
+  const int cr = int(P.cubeRes) - 1;
+  const int x0 = max(cx - 1, 0) >> 2, x1 = min(cx + 1, cr) >> 2;
+  const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, cr) >> 2;
+  const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, cr) >> 2;
+  for (int bz = z0; bz <= z1; ++bz)
+    for (int by = y0; by <= y1; ++by)
+      for (int bx = x0; bx <= x1; ++bx) flag[mortonEncode(bx, by, bz)] = 1u;
+}
+
+// ------------------------------------------------------------------ binning count (standalone)
+__global__ void __launch_bounds__(kThreads) k_brick_count(SubstepParams P, const float4* __restrict__ pos, uint32_t n, BrickBuffers B) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < n;
+  const uint32_t mask = __ballot_sync(0xffffffffu, act);
+  if (!act) return;
+  const float4 p = pos[i];
+  int cx, cy, cz;
+  cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
+  const uint32_t b = mortonEncode(cx, cy, cz) >> 6;
+  B.binKey[i] = b;
+  B.binRank[i] = warpAggInc(mask, B.brickCount, b);
+  markStencilBricks(P, cx, cy, cz, B.brickFlag);
+}
+
+// ------------------------------------------------------------------ compaction scan
+__device__ __forceinline__ unsigned long long ldv64(const unsigned long long* p) { return *reinterpret_cast<const volatile unsigned long long*>(p); }
+
+// One chain of the decoupled look-back: returns the exclusive prefix of `tile`.
+__device__ uint32_t lookBack(unsigned long long* st, uint32_t tile, uint32_t aggregate, unsigned long long tag, uint32_t* err) {
+  if (tile == 0) {
+    atomicExch(st, tag | kStFlagPre | aggregate);
+    return 0;
+  }
+  atomicExch(st + tile, tag | kStFlagAgg | aggregate);
+  uint32_t prefix = 0;
+  int64_t j = int64_t(tile) - 1;
+  uint32_t spins = 0;
+  while (j >= 0) {
+    const unsigned long long s = ldv64(st + j);
+    const bool mine = (s & ~((1ull << 50) - 1)) == tag;
+    const unsigned long long flag = s & (3ull << 48);
+    if (!mine || flag == 0) {
+      if (++spins > kBrickScanSpinLimit) {
+        atomicOr(err, kErrScanTimeout);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    prefix += uint32_t(s & kStValue);
+    if (flag == kStFlagPre) break;
+    --j;
+  }
+  atomicExch(st + tile, tag | kStFlagPre | uint32_t(prefix + aggregate));
+  return prefix;
+}
+
+__global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B, unsigned long long launchBase, uint32_t epoch, uint32_t* err) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[3][kBrickScanThreads / 32];
+  __shared__ uint32_t s_prefix[3];
+  if (threadIdx.x == 0) s_tile = uint32_t(atomicAdd(B.scanTile, 1ull) - launchBase);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const unsigned long long tag = (unsigned long long)(epoch & 0x3fffu) << 50;
+  const uint32_t b0 = tile * kBrickScanTile + threadIdx.x * kBrickScanItems;
+  uint32_t cnt[kBrickScanItems];
+  uint32_t flg = 0;  // bit k: grid-active
+  uint32_t sc = 0, sp = 0, sg = 0;
+#pragma unroll
+  for (int k = 0; k < kBrickScanItems; ++k) {
+    const uint32_t b = b0 + k;
+    cnt[k] = 0;
+    if (b < B.nb) {
+      cnt[k] = B.brickCount[b];
+      const uint32_t f = B.brickFlag[b];
+      B.brickCount[b] = 0;
+      B.brickFlag[b] = 0;
+      if (f) flg |= 1u << k;
+    }
+    sc += cnt[k];
+    sp += cnt[k] ? 1u : 0u;
+  }
+  sg = __popc(flg);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t ic = sc, ip = sp, ig = sg;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t yc = __shfl_up_sync(0xffffffffu, ic, o), yp = __shfl_up_sync(0xffffffffu, ip, o), yg = __shfl_up_sync(0xffffffffu, ig, o);
+    if (lane >= o) {
+      ic += yc;
+      ip += yp;
+      ig += yg;
+    }
+  }
+  if (lane == 31) {
+    s_warp[0][warp] = ic;
+    s_warp[1][warp] = ip;
+    s_warp[2][warp] = ig;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int W = kBrickScanThreads / 32;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uint32_t w = lane < W ? s_warp[c][lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      if (lane < W) s_warp[c][lane] = w;
+    }
+  }
+  __syncthreads();
+  constexpr int WL = kBrickScanThreads / 32 - 1;
+  // chains run in three different warps
+  if (threadIdx.x == 0 || threadIdx.x == 32 || threadIdx.x == 64) {
+    const int c = threadIdx.x >> 5;
+    const uint32_t agg = s_warp[c][WL];
+    const uint32_t pre = lookBack(B.scanState + size_t(c) * B.tiles, tile, agg, tag, err);
+    s_prefix[c] = pre;
+    if (tile == B.tiles - 1) {
+      const uint32_t total = pre + agg;
+      if (c == 0) {
+        B.counters[kCntTotal] = total;
+      } else if (c == 1) {
+        B.counters[kCntNumPB] = total;
+      } else {
+        B.counters[kCntNumGB] = total;
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t rc = s_prefix[0] + (warp > 0 ? s_warp[0][warp - 1] : 0u) + ic - sc;
+  uint32_t rp = s_prefix[1] + (warp > 0 ? s_warp[1][warp - 1] : 0u) + ip - sp;
+  uint32_t rg = s_prefix[2] + (warp > 0 ? s_warp[2][warp - 1] : 0u) + ig - sg;
+#pragma unroll
+  for (int k = 0; k < kBrickScanItems; ++k) {
+    const uint32_t b = b0 + k;
+    if (b < B.nb) {
+      B.brickStart[b] = rc;
+      if (cnt[k]) {
+        B.pbBrick[rp] = b;
+        B.pbStart[rp] = rc;
+        ++rp;
+      }
+      if (flg & (1u << k)) {
+        B.gbBrick[rg] = b;
+        ++rg;
+      }
+    }
+    rc += cnt[k];
+  }
+  if (tile == B.tiles - 1 && threadIdx.x == 0) {
+    // the last tile's look-back finished, so all three totals are final
+    const uint32_t npb = s_prefix[1] + s_warp[1][WL];
+    B.pbStart[npb] = s_prefix[0] + s_warp[0][WL];
+    B.counters[kCntQueueP2G] = 0;
+    B.counters[kCntQueueFused] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint32_t n, uint32_t* err) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t slot = B.brickStart[B.binKey[t]] + B.binRank[t];
+  if (slot < n) B.perm[slot] = t;
+  else atomicOr(err, kErrBinRange);
+}
+
+// ------------------------------------------------------------------ shared-memory P2G
+// A CTA handles one particle brick at a time, in chunks of kChunk particles.
+// Each particle's P2G inputs go to a shared row, counting-sorted by the cell
+// its stencil is centred on (6^3 cells around the brick).  A warp then takes
+// whole cells: lanes 0..26 own the cell's 27 stencil nodes and accumulate the
+// contributions of all the cell's particles in registers, then add them with
+// plain stores into the warp's private 8^3 tile (lanes own distinct nodes, one
+// cell per warp at a time, so nothing races).  The brick ends with one sum over
+// the private tiles and one vector reduction per non-zero node.
+constexpr int kChunk = kThreads;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRow = 23;        // floats per input row (22 used; odd stride keeps writes conflict-free)
+constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
+constexpr int kTileNodes = 512; // 8^3
+
+struct P2GSmem {
+  float rows[kChunk * kRow];
+  float tiles[kWarps * 4 * kTileNodes];
+  uint32_t cellCount[kCellSlots];
+  uint32_t cellStart[kCellSlots];
+  uint16_t order[kChunk];
+  uint16_t cells[kCellSlots];
+  uint32_t numCells;
+  uint32_t item;
+};
+
+template <bool FLIP>
+struct G2P2GSmem {
+  P2GSmem p2g;
+  float4 v[216];
+  float4 vo[FLIP ? 216 : 1];
+};
+
+// Inputs of one particle's P2G: x, m, m v, m (4/h^2) B (APIC), dt Vp tau.
+__device__ __forceinline__ void p2gRow(const SubstepParams& P, const PState& s, float dtStress, float* row) {
+  const float m = fetchRho0(P, __float_as_uint(s.v.w)) * s.P.w;
+  row[0] = s.P.x; row[1] = s.P.y; row[2] = s.P.z;
+  row[3] = m;
+  row[4] = m * s.v.x; row[5] = m * s.v.y; row[6] = m * s.v.z;
+  if (P.flip_ratio < -0.5f) {
+    const float k = m * (4.0f / (P.cellSize * P.cellSize));
+    row[7] = k * s.B0.x; row[8] = k * s.B0.y; row[9] = k * s.B0.z;
+    row[10] = k * s.B1.x; row[11] = k * s.B1.y; row[12] = k * s.B1.z;
+    row[13] = k * s.B2.x; row[14] = k * s.B2.y; row[15] = k * s.B2.z;
+  } else {
+#pragma unroll
+    for (int i = 7; i < 16; ++i) row[i] = 0.f;
+  }
+  const float sdt = dtStress * s.P.w;
+  // symmetric stress: xx yy zz xy xz yz
+  row[16] = sdt * s.F0.w; row[17] = sdt * s.F1.w; row[18] = sdt * s.F2.w;
+  row[19] = sdt * s.B0.w; row[20] = sdt * s.B1.w; row[21] = sdt * s.B2.w;
+}
+
+// Contribution of the particle in `row` to the node centred at xi.
+__device__ __forceinline__ void p2gNodeTerm(const float* __restrict__ row, const float xi[3], float invH, float acc[4]) {
+  float wa[3], ga[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float d = (row[a] - xi[a]) * invH;
+    wa[a] = bspline2(d);
+    ga[a] = bspline2g(d);
+  }
+  const float w = wa[0] * wa[1] * wa[2];
+  if (w < 1e-12f) return;
+  const float dw0 = ga[0] * wa[1] * wa[2] * invH, dw1 = wa[0] * ga[1] * wa[2] * invH, dw2 = wa[0] * wa[1] * ga[2] * invH;
+  const float r0 = xi[0] - row[0], r1 = xi[1] - row[1], r2 = xi[2] - row[2];
+  const float* Q = row + 7;
+  const float* T = row + 16;
+  const float td0 = T[0] * dw0 + T[3] * dw1 + T[4] * dw2;
+  const float td1 = T[3] * dw0 + T[1] * dw1 + T[5] * dw2;
+  const float td2 = T[4] * dw0 + T[5] * dw1 + T[2] * dw2;
+  acc[0] += w * (row[4] + (Q[0] * r0 + Q[3] * r1 + Q[6] * r2)) - td0;
+  acc[1] += w * (row[5] + (Q[1] * r0 + Q[4] * r1 + Q[7] * r2)) - td1;
+  acc[2] += w * (row[6] + (Q[2] * r0 + Q[5] * r1 + Q[8] * r2)) - td2;
+  acc[3] += w * row[3];
+}
+
+// Direct scatter of one row to global memory (stencils outside the brick's tile).
+__device__ __forceinline__ void p2gRowGlobal(const SubstepParams& P, const float* row, int cx, int cy, int cz, float4* acc) {
+  const float invH = 1.0f / P.cellSize;
+  const int cr = int(P.cubeRes);
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx, ny = cy + dy, nz = cz + dz;
+        if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
+        const float xi[3] = {nodeCentre(P, 0, nx), nodeCentre(P, 1, ny), nodeCentre(P, 2, nz)};
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
+        p2gNodeTerm(row, xi, invH, a);
+        if (a[3] != 0.f || a[0] != 0.f || a[1] != 0.f || a[2] != 0.f) redAddV4(acc + mortonEncode(nx, ny, nz), a[0], a[1], a[2], a[3]);
+      }
+}
+
+__device__ __forceinline__ void p2gZeroTiles(P2GSmem& sm) {
+  for (int q = threadIdx.x; q < kWarps * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
+  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.cellCount[q] = 0u;
+}
+
+// Called by every thread once the chunk's rows are written and each thread
+// holding an in-tile particle has its cell key (< 216) and rank; ends synced.
+// Tile origin (node) = (bx, by, bz) * 4 - 2; stencil-centre cells start at + 1.
+__device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, int key, uint32_t rank, int tx, int ty, int tz) {
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // exclusive scan of the 216 cell counts + list of non-empty cells
+    const int lane = threadIdx.x;
+    uint32_t c[7], sum = 0, ne = 0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const int q = lane * 7 + k;
+      c[k] = q < kCellSlots ? sm.cellCount[q] : 0u;
+      sum += c[k];
+      ne += c[k] ? 1u : 0u;
+    }
+    uint32_t is = sum, in = ne;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o), yn = __shfl_up_sync(0xffffffffu, in, o);
+      if (lane >= o) {
+        is += ys;
+        in += yn;
+      }
+    }
+    uint32_t run = is - sum, pos = in - ne;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const int q = lane * 7 + k;
+      if (q < kCellSlots) {
+        sm.cellStart[q] = run;
+        if (c[k]) sm.cells[pos++] = uint16_t(q);
+      }
+      run += c[k];
+    }
+    if (lane == 31) sm.numCells = in;
+  }
+  __syncthreads();
+  if (key >= 0) sm.order[sm.cellStart[key] + rank] = uint16_t(threadIdx.x);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
+  const float invH = 1.0f / P.cellSize;
+  const int cr = int(P.cubeRes);
+  float* tile = sm.tiles + warp * 4 * kTileNodes;
+  const uint32_t numCells = sm.numCells;
+  for (uint32_t ci = warp; ci < numCells; ci += kWarps) {
+    const int q = sm.cells[ci];
+    const int rx = q % 6, ry = (q / 6) % 6, rz = q / 36;
+    if (lane >= 27) continue;
+    const int lx = rx + dx, ly = ry + dy, lz = rz + dz;  // tile-local node
+    const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
+    if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
+    const float xi[3] = {nodeCentre(P, 0, nx), nodeCentre(P, 1, ny), nodeCentre(P, 2, nz)};
+    float a[4] = {0.f, 0.f, 0.f, 0.f};
+    const uint32_t st = sm.cellStart[q], en = st + sm.cellCount[q];
+    for (uint32_t j = st; j < en; ++j) p2gNodeTerm(sm.rows + sm.order[j] * kRow, xi, invH, a);
+    const int t = (lz * 8 + ly) * 8 + lx;
+    tile[t] += a[3];
+    tile[kTileNodes + t] += a[0];
+    tile[2 * kTileNodes + t] += a[1];
+    tile[3 * kTileNodes + t] += a[2];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.cellCount[q] = 0u;
+  __syncthreads();
+}
+
+// Sum the private tiles and add every non-zero node to the global grid.
+__device__ __forceinline__ void p2gFlush(const SubstepParams& P, P2GSmem& sm, int tx, int ty, int tz, float4* acc) {
+  const int cr = int(P.cubeRes);
+  for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
+    float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const float* t = sm.tiles + w * 4 * kTileNodes;
+      m += t[q];
+      mx += t[kTileNodes + q];
+      my += t[2 * kTileNodes + q];
+      mz += t[3 * kTileNodes + q];
+    }
+    if (m == 0.f && mx == 0.f && my == 0.f && mz == 0.f) continue;
+    const int nx = tx + (q & 7), ny = ty + ((q >> 3) & 7), nz = tz + (q >> 6);
+    if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
+    redAddV4(acc + mortonEncode(nx, ny, nz), mx, my, mz, m);
+  }
+}
+
+// G2P node source: the brick's 6^3 staged neighbourhood, global memory outside it.
+template <bool FLIP>
+struct StagedGrid {
+  const float4* sv;
+  const float4* svo;
+  const float4* gvel;
+  const float4* gvold;
+  int ox, oy, oz;
+  __device__ __forceinline__ bool node(int x, int y, int z, float& m, float3& v, float3& vo) const {
+    const int lx = x - ox, ly = y - oy, lz = z - oz;
+    float4 a, b = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((unsigned)lx < 6u && (unsigned)ly < 6u && (unsigned)lz < 6u) {
+      const int q = (lz * 6 + ly) * 6 + lx;
+      a = sv[q];
+      if (FLIP) b = svo[q];
+    } else {
+      const uint32_t c = mortonEncode(x, y, z);
+      a = gvel[c];
+      if (FLIP) b = gvold[c];
+    }
+    m = a.w;
+    if (m < 1e-10f) return false;
+    v = make_float3(a.x, a.y, a.z);
+    vo = make_float3(b.x, b.y, b.z);
+    return true;
+  }
+};
+
+// The slot of a particle's stencil centre among the brick's 216 cell slots, or -1.
+__device__ __forceinline__ int cellSlot(int cx, int cy, int cz, int ox, int oy, int oz) {
+  const int rx = cx - ox, ry = cy - oy, rz = cz - oz;
+  if ((unsigned)rx < 6u && (unsigned)ry < 6u && (unsigned)rz < 6u) return (rz * 6 + ry) * 6 + rx;
+  return -1;
+}
+
+// ------------------------------------------------------------------ P2G over particle bricks (standalone)
+__global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P, StatePtrs cur, uint32_t n, BrickBuffers B, GridBuffers G,
+                                                         float dtStress) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
+  const uint32_t numPB = B.counters[kCntNumPB];
+  for (;;) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(B.counters + kCntQueueP2G, 1u);
+    p2gZeroTiles(sm);
+    __syncthreads();
+    const uint32_t i = sm.item;
+    if (i >= numPB) break;
+    const uint32_t b = B.pbBrick[i], end = min(B.pbStart[i + 1], n), start = min(B.pbStart[i], end);
+    int bx, by, bz;
+    mortonDecode(b, bx, by, bz);
+    const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
+    for (uint32_t base = start; base < end; base += kChunk) {
+      const uint32_t t = base + threadIdx.x;
+      int key = -1;
+      uint32_t rank = 0;
+      if (t < end) {
+        const uint32_t s = B.perm[t];
+        if (s < n) {
+          const PState st = loadState(cur.f, s);
+          float* row = sm.rows + threadIdx.x * kRow;
+          p2gRow(P, st, dtStress, row);
+          int cx, cy, cz;
+          cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
+          key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
+          if (key >= 0) rank = atomicAdd(&sm.cellCount[key], 1u);
+          else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+        }
+      }
+      p2gChunk(P, sm, key, rank, tx, ty, tz);
+    }
+    p2gFlush(P, sm, tx, ty, tz, G.acc);
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ sparse grid update
+__global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, BrickBuffers B, GridBuffers G) {
+  const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
+  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t code = (B.gbBrick[g >> 6] << 6) | uint32_t(g & 63u);
+    if (code >= P.hashCells) continue;
+    const float4 a = G.acc[code];
+    G.acc[code] = make_float4(0.f, 0.f, 0.f, 0.f);
+    int ix, iy, iz;
+    mortonDecode(code, ix, iy, iz);
+    float3 v, vo;
+    const bool ok = gridNode(P, ix, iy, iz, a.w, a.x, a.y, a.z, v, vo);
+    G.vel[code] = ok ? make_float4(v.x, v.y, v.z, a.w) : make_float4(0.f, 0.f, 0.f, a.w);
+    if (G.vold) G.vold[code] = ok ? make_float4(vo.x, vo.y, vo.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridBuffers G) {
+  const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
+  for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t code = (B.gbBrick[g >> 6] << 6) | uint32_t(g & 63u);
+    G.acc[code] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// ------------------------------------------------------------------ fused G2P -> update -> P2G
+template <bool FLIP>
+__global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
+                                                    uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G, float dtStress,
+                                                    uint32_t* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  G2P2GSmem<FLIP>& S = *reinterpret_cast<G2P2GSmem<FLIP>*>(smem_raw);
+  P2GSmem& sm = S.p2g;
+  const uint32_t numPB = B.counters[kCntNumPB];
+  for (;;) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(B.counters + kCntQueueFused, 1u);
+    p2gZeroTiles(sm);
+    __syncthreads();
+    const uint32_t i = sm.item;
+    if (i >= numPB) break;
+    const uint32_t b = B.pbBrick[i], end = min(B.pbStart[i + 1], n), start = min(B.pbStart[i], end);
+    int bx, by, bz;
+    mortonDecode(b, bx, by, bz);
+    // stage the 6^3 nodes [4b-1, 4b+4]^3 (nodes outside [0, gridRes) read as empty)
+    const int sx = 4 * bx - 1, sy = 4 * by - 1, sz = 4 * bz - 1;
+    for (int q = threadIdx.x; q < 216; q += blockDim.x) {
+      const int x = sx + q % 6, y = sy + (q / 6) % 6, z = sz + q / 36;
+      const bool valid = x >= 0 && y >= 0 && z >= 0 && x < P.gridRes[0] && y < P.gridRes[1] && z < P.gridRes[2];
+      const uint32_t c = valid ? mortonEncode(x, y, z) : 0u;
+      S.v[q] = valid ? G.vel[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (FLIP) S.vo[q] = valid ? G.vold[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
+    const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
+    for (uint32_t base = start; base < end; base += kChunk) {
+      const uint32_t t = base + threadIdx.x;
+      const bool act = t < end;
+      const uint32_t mask = __ballot_sync(0xffffffffu, act);
+      int key = -1;
+      uint32_t rank = 0;
+      if (act) {
+        const uint32_t s = B.perm[t];
+        const bool valid = s < n;
+        PState st;
+        int cx = 0, cy = 0, cz = 0;
+        uint32_t nb = 0;
+        if (valid) {
+          st = loadState(cur.f, s);
+          const uint32_t pid = pidCur[s];
+          g2pParticle(P, st, grid, P.dt);
+          storeState(nxt.f, t, st);
+          pidNxt[t] = pid;
+          if (!(isfinite(st.P.x) && isfinite(st.P.y) && isfinite(st.P.z))) atomicOr(err, kErrNonFinite);
+          cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
+          nb = mortonEncode(cx, cy, cz) >> 6;
+        } else {
+          atomicOr(err, kErrBinRange);  // a slot that maps nowhere: only after an expired scan wait
+        }
+        // every active lane reaches this one call site
+        const uint32_t r = warpAggInc(mask, B.brickCount, nb);
+        B.binKey[t] = nb;
+        B.binRank[t] = r;
+        if (valid) {
+          markStencilBricks(P, cx, cy, cz, B.brickFlag);
+          float* row = sm.rows + threadIdx.x * kRow;
+          p2gRow(P, st, dtStress, row);
+          key = cellSlot(cx, cy, cz, sx, sy, sz);
+          if (key >= 0) {
+            rank = atomicAdd(&sm.cellCount[key], 1u);
+          } else {
+            p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+            atomicAdd(B.counters + kCntOverflow, 1u);
+          }
+        }
+      }
+      p2gChunk(P, sm, key, rank, tx, ty, tz);
+    }
+    p2gFlush(P, sm, tx, ty, tz, G.acc);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_unpermute(StatePtrs in, const uint32_t* __restrict__ pid, StatePtrs out, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t d = pid[i];
+  if (d >= n) return;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) out.f[k][d] = in.f[k][i];
+}
+
+__global__ void __launch_bounds__(kThreads) k_sorted_pid(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ pid, uint32_t* out,
+                                                         uint32_t n) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t s = perm[t];
+  out[t] = s < n ? pid[s] : 0xffffffffu;
+}
+
+__global__ void __launch_bounds__(kThreads) k_iota(uint32_t* pid, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pid[i] = i;
+}
+
+template <class K> int persistentBlocks(K kernel, int numSMs, size_t smem = 0) {
+  int perSM = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, smem) != cudaSuccess || perSM < 1) perSM = 1;
+  return perSM * numSMs;
+}
+
+}  // namespace
+
+cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
+                             uint64_t* launches) {
+  (void)err;
+  if (n == 0) return cudaSuccess;
+  k_brick_count<<<blocksFor(n), kThreads, 0, s>>>(P, pos, n, b);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t epoch, uint32_t* err, cudaStream_t s, uint64_t* launches) {
+  k_brick_scan<<<b.tiles, kBrickScanThreads, 0, s>>>(b, (unsigned long long)epoch * b.tiles, epoch, err);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_perm_scatter<<<blocksFor(n), kThreads, 0, s>>>(b, n, err);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+template <class K> int setupBigSmem(K kernel, size_t smem, int numSMs) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  return persistentBlocks(kernel, numSMs, smem);
+}
+
+cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
+                            int numSMs, cudaStream_t s, uint64_t* launches) {
+  static int blocks = 0;
+  const size_t smem = sizeof(P2GSmem);
+  if (!blocks) blocks = setupBigSmem(k_p2g_bricks, smem, numSMs);
+  k_p2g_bricks<<<blocks, kThreads, smem, s>>>(P, cur, n, b, g, dtStress);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches) {
+  static int blocks = 0;
+  if (!blocks) blocks = persistentBlocks(k_grid_bricks, numSMs);
+  k_grid_bricks<<<blocks, kThreads, 0, s>>>(P, b, g);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches) {
+  k_clear_bricks<<<numSMs * 4, kThreads, 0, s>>>(b, g);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches) {
+  if (P.flip_ratio > 0.01f) {
+    static int blocks = 0;
+    const size_t smem = sizeof(G2P2GSmem<true>);
+    if (!blocks) blocks = setupBigSmem(k_g2p2g<true>, smem, numSMs);
+    k_g2p2g<true><<<blocks, kThreads, smem, s>>>(P, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+  } else {
+    static int blocks = 0;
+    const size_t smem = sizeof(G2P2GSmem<false>);
+    if (!blocks) blocks = setupBigSmem(k_g2p2g<false>, smem, numSMs);
+    k_g2p2g<false><<<blocks, kThreads, smem, s>>>(P, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+  }
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchUnpermute(StatePtrs in, const uint32_t* pid, StatePtrs out, uint32_t n, cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_unpermute<<<blocksFor(n), kThreads, 0, s>>>(in, pid, out, n);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchSortedPid(const uint32_t* perm, const uint32_t* pid, uint32_t* out, uint32_t n, cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_sorted_pid<<<blocksFor(n), kThreads, 0, s>>>(perm, pid, out, n);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchIota(uint32_t* pid, uint32_t n, cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_iota<<<blocksFor(n), kThreads, 0, s>>>(pid, n);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+}  // namespace nebula

@@ -1,0 +1,73 @@
+// mpm_bricks.cuh -- buffers and launchers of the brick-sparse fused substep.
+//
+// The grid is split into bricks of 4x4x4 cells; a brick is 64 consecutive
+// Morton codes, so brick id = cell Morton code >> 6.  Per substep:
+//   grid     sparse grid update over the bricks the last P2G touched
+//   g2p2g    per particle brick: G2P from the staged grid, particle update,
+//            P2G of the updated particle into a shared tile, binning count
+//   scan     brick counts / marks -> particle-brick list, grid-brick list,
+//            brick starts (single pass, decoupled look-back, compaction)
+//   perm     (brick, rank) -> sorted slot of every particle
+// Particles are physically reordered by brick every substep (ping-pong state
+// buffers plus the original particle id).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_internal.h"
+
+namespace nebula {
+
+constexpr int kBrickScanThreads = 256;
+constexpr int kBrickScanItems = 8;
+constexpr int kBrickScanTile = kBrickScanThreads * kBrickScanItems;
+
+// counters[] slots
+enum : int { kCntNumPB = 0, kCntNumGB = 1, kCntTotal = 2, kCntQueueP2G = 3, kCntQueueFused = 4, kCntOverflow = 5, kCntSlots = 8 };
+
+struct BrickBuffers {
+  uint32_t nb;                // number of bricks (>= 1)
+  uint32_t tiles;             // scan tiles over nb
+  uint32_t* brickCount;       // [nb] particles per brick (zeroed by the scan)
+  uint32_t* brickFlag;        // [nb] grid-active marks (zeroed by the scan)
+  uint32_t* brickStart;       // [nb] first sorted slot of each brick
+  uint32_t* pbBrick;          // [nb] particle-brick list
+  uint32_t* pbStart;          // [nb + 1] first slot of each listed brick; pbStart[numPB] = total
+  uint32_t* gbBrick;          // [nb] grid-brick list
+  uint32_t* counters;         // [kCntSlots]
+  unsigned long long* scanState;  // [3 * tiles] status words (epoch-tagged)
+  unsigned long long* scanTile;   // monotone tile counter
+  uint32_t* binKey;           // [cap] brick of each particle (by buffer index)
+  uint32_t* binRank;          // [cap] rank inside its brick
+  uint32_t* perm;             // [cap] sorted slot -> buffer index
+};
+
+struct GridBuffers {
+  float4* acc;   // [ncPad] (mom.xyz, mass) accumulated by P2G
+  float4* vel;   // [ncPad] (v.xyz, mass) after the grid update
+  float4* vold;  // [ncPad] pre-force velocity (FLIP), may be null
+};
+
+// Standalone binning of the particles in buffer order: counts + stencil marks.
+cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
+                             uint64_t* launches);
+// Compaction scan; epoch must differ from the previous launch's (mod 2^14).
+cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t epoch, uint32_t* err, cudaStream_t s, uint64_t* launches);
+cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches);
+// P2G of the particles of every listed brick (no binning, no marks).
+cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
+                            int numSMs, cudaStream_t s, uint64_t* launches);
+// Sparse grid update over the listed grid bricks; clears acc as it reads.
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
+// Zero acc over the listed grid bricks (discarding a pending P2G).
+cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
+// The fused G2P -> particle update -> P2G + binning count.
+cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches);
+// out[pid[i]] = in[i] for the 8 fields (original particle order).
+cudaError_t launchUnpermute(StatePtrs in, const uint32_t* pid, StatePtrs out, uint32_t n, cudaStream_t s, uint64_t* launches);
+cudaError_t launchIota(uint32_t* pid, uint32_t n, cudaStream_t s, uint64_t* launches);
+// out[t] = pid[perm[t]]: original particle ids in brick order.
+cudaError_t launchSortedPid(const uint32_t* perm, const uint32_t* pid, uint32_t* out, uint32_t n, cudaStream_t s, uint64_t* launches);
+
+}  // namespace nebula

@@ -103,6 +103,11 @@ __device__ __forceinline__ void cellCoords(const SubstepParams& P, float x, floa
   cz = int(uint32_t(lz));
 }
 
+// One vector reduction of 4 floats into global memory (sm_90+).
+__device__ __forceinline__ void redAddV4(float4* addr, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
 // ------------------------------------------------------------------ B-spline
 __device__ __forceinline__ float gsign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
 __device__ __forceinline__ double gsign(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }

@@ -82,26 +82,42 @@ MPMEngine::MPMEngine(const nebula_mpm_config& cfg) : cfg_(cfg) {
   capacity_ = cfg.maxParticles > 0 ? cfg.maxParticles : uint32_t(lattice);
   if (lattice > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "nx*ny*nz exceeds maxParticles");
 
-  for (int k = 0; k < 8; ++k) state_[k].alloc(size_t(std::max(capacity_, 1u)) * sizeof(float4));
-  const size_t nc = hashCells_;
-  gridMom_.alloc(nc * 2 * sizeof(float4));
-  gridMass_.alloc(nc * sizeof(float));
-  cellCount_.alloc(nc * sizeof(uint32_t));
-  cellStart_.alloc(nc * sizeof(uint32_t));
-  cellEnd_.alloc(nc * sizeof(uint32_t));
-  const size_t pc = size_t(std::max(capacity_, 1u)) * sizeof(uint32_t);
-  key_.alloc(pc);
-  rank_.alloc(pc);
-  sortedTmp_.alloc(pc);
-  sorted_.alloc(pc);
-  scanWs_.alloc(scanWorkspaceBytes(nc));
+  const size_t capN = size_t(std::max(capacity_, 1u));
+  for (int k = 0; k < 8; ++k) {
+    state_[k].alloc(capN * sizeof(float4));
+    stateB_[k].alloc(capN * sizeof(float4));
+  }
+  for (auto& p : pid_) p.alloc(capN * sizeof(uint32_t));
   materials_.alloc(kMaxMaterials * sizeof(Material));
   colliders_.alloc(kMaxColliders * sizeof(Collider));
   forces_.alloc(kMaxForces * sizeof(Force));
   err_.alloc(sizeof(uint32_t));
   check(cudaMemset(err_.ptr, 0, sizeof(uint32_t)), "cudaMemset");
-  check(cudaMemset(gridMom_.ptr, 0, gridMom_.bytes), "cudaMemset");
-  check(cudaMemset(gridMass_.ptr, 0, gridMass_.bytes), "cudaMemset");
+  check(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, device_), "cudaDeviceGetAttribute");
+
+  // brick-sparse grid: dense arrays over hashCells (padded to one brick), touched per brick
+  ncPad_ = std::max(hashCells_, 64u);
+  nb_ = ncPad_ / 64u;
+  tiles_ = (nb_ + kBrickScanTile - 1) / kBrickScanTile;
+  gridAcc_.alloc(size_t(ncPad_) * sizeof(float4));
+  gridVel_.alloc(size_t(ncPad_) * sizeof(float4));
+  check(cudaMemset(gridAcc_.ptr, 0, gridAcc_.bytes), "cudaMemset");
+  check(cudaMemset(gridVel_.ptr, 0, gridVel_.bytes), "cudaMemset");
+  for (DevBuf* b : {&bCount_, &bFlag_, &bStart_, &pbBrick_, &gbBrick_}) {
+    b->alloc(size_t(nb_) * sizeof(uint32_t));
+    check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
+  }
+  pbStart_.alloc(size_t(nb_ + 1) * sizeof(uint32_t));
+  counters_.alloc(kCntSlots * sizeof(uint32_t));
+  scanState_.alloc(size_t(3) * tiles_ * sizeof(unsigned long long));
+  scanTile_.alloc(sizeof(unsigned long long));
+  for (DevBuf* b : {&pbStart_, &counters_, &scanState_, &scanTile_}) check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
+  for (DevBuf* b : {&binKey_, &binRank_, &perm_}) {
+    b->alloc(capN * sizeof(uint32_t));
+    check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
+  }
+  uint64_t l = 0;
+  check(launchIota(static_cast<uint32_t*>(pid_[0].ptr), capacity_, nullptr, &l), "iota");
 
   // default material: presetJelly(E, nu, rho0) with model ELASTIC and the
   // public DP/VM defaults (MPMEngine.cpp:67-78)
@@ -214,11 +230,31 @@ void MPMEngine::setParams(const nebula_mpm_params& p) {
   params_ = p;
 }
 
+void MPMEngine::setPipeline(int p) {
+  if (p != NEBULA_MPM_PIPELINE_DENSE && p != NEBULA_MPM_PIPELINE_FUSED) throw Error(NEBULA_MPM_ERR_INVALID, "unknown pipeline");
+  if (p == pipeline_) return;
+  bindDevice();
+  prepareHostAccess(true);
+  pipeline_ = p;
+}
+
+// Before the host reads or writes particle arrays: a write needs the particles
+// back in their original order and any pending P2G discarded; both need the
+// engine's stream drained.
+void MPMEngine::prepareHostAccess(bool modifiesParticles) {
+  bindDevice();
+  if (modifiesParticles) {
+    normalizeOrder(lastStream_);
+    discardPending(lastStream_);
+  }
+  quiesce();
+}
+
 void MPMEngine::setMaterials(const nebula_mpm_material* mats, uint32_t n) {
   if (n == 0) return;  // MPMEngine.cpp:240
   if (n > uint32_t(kMaxMaterials)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 16 materials");
   if (!mats) throw Error(NEBULA_MPM_ERR_INVALID, "null materials");
-  quiesce();
+  prepareHostAccess(true);  // rho0 enters P2G
   hostMaterials_.assign(reinterpret_cast<const Material*>(mats), reinterpret_cast<const Material*>(mats) + n);
   check(cudaMemcpy(materials_.ptr, mats, n * sizeof(Material), cudaMemcpyHostToDevice), "upload materials");
 }
@@ -226,20 +262,20 @@ void MPMEngine::setMaterials(const nebula_mpm_material* mats, uint32_t n) {
 void MPMEngine::setParticleMaterialIds(const uint32_t* ids, uint32_t n) {
   if (n > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "more ids than particle capacity");
   if (n && !ids) throw Error(NEBULA_MPM_ERR_INVALID, "null ids");
-  quiesce();
+  prepareHostAccess(true);
   std::vector<float4> v(n);
   for (uint32_t i = 0; i < n; ++i) {
     float w;
     std::memcpy(&w, ids + i, 4);
     v[i] = make_float4(0.f, 0.f, 0.f, w);
   }
-  if (n) check(cudaMemcpy(state_[1].ptr, v.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "upload ids");
+  if (n) check(cudaMemcpy(statePtrs(cur_).f[1], v.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "upload ids");
 }
 
 void MPMEngine::setColliders(const nebula_mpm_collider* c, uint32_t n) {
   if (n > uint32_t(kMaxColliders)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 64 colliders");
   if (n && !c) throw Error(NEBULA_MPM_ERR_INVALID, "null colliders");
-  quiesce();
+  prepareHostAccess(false);
   colliderCount_ = n;
   if (n) check(cudaMemcpy(colliders_.ptr, c, n * sizeof(Collider), cudaMemcpyHostToDevice), "upload colliders");
 }
@@ -248,7 +284,7 @@ void MPMEngine::clearAnalyticColliders() { colliderCount_ = 0; }
 
 void MPMEngine::setColliderSDF(const float* sdf, uint64_t n) {
   if (!sdf || n != hashCells_) throw Error(NEBULA_MPM_ERR_INVALID, "SDF must hold hashCells floats");
-  quiesce();
+  prepareHostAccess(false);
   sdf_.ensure(size_t(hashCells_) * sizeof(float));
   check(cudaMemcpy(sdf_.ptr, sdf, size_t(hashCells_) * sizeof(float), cudaMemcpyHostToDevice), "upload sdf");
   hasSdf_ = true;
@@ -276,7 +312,7 @@ void MPMEngine::setForces(const nebula_mpm_force* f, uint32_t n) {
   for (uint32_t i = 0; i < n; ++i)
     if (f[i].type != FORCE_GRAVITY && f[i].type != FORCE_CONSTANT_WIND)
       throw Error(NEBULA_MPM_ERR_UNSUPPORTED, "only GRAVITY and CONSTANT_WIND forces act on the MPM grid in this build");
-  quiesce();
+  prepareHostAccess(false);
   forceCount_ = n;
   if (n) check(cudaMemcpy(forces_.ptr, f, n * sizeof(Force), cudaMemcpyHostToDevice), "upload forces");
 }
@@ -285,13 +321,12 @@ uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32
   const uint32_t nNew = std::min(n, capacity_ - live_);  // MPMEngine.cpp:212-214
   if (nNew == 0) return 0;
   if (!pos4 || !vel4) throw Error(NEBULA_MPM_ERR_INVALID, "null particle arrays");
-  quiesce();
+  prepareHostAccess(true);
   std::vector<float4> F0(nNew, make_float4(1, 0, 0, 0)), F1(nNew, make_float4(0, 1, 0, 0)), F2(nNew, make_float4(0, 0, 1, 0)),
       Z(nNew, make_float4(0, 0, 0, 0));
-  const size_t off = size_t(live_) * sizeof(float4), bytes = size_t(nNew) * sizeof(float4);
-  auto up = [&](int k, const void* src) {
-    check(cudaMemcpy(static_cast<char*>(state_[k].ptr) + off, src, bytes, cudaMemcpyHostToDevice), "append");
-  };
+  StatePtrs st = statePtrs(cur_);
+  const size_t bytes = size_t(nNew) * sizeof(float4);
+  auto up = [&](int k, const void* src) { check(cudaMemcpy(st.f[k] + live_, src, bytes, cudaMemcpyHostToDevice), "append"); };
   up(0, pos4);
   up(1, vel4);
   up(2, F0.data());
@@ -305,7 +340,7 @@ uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32
 }
 
 void MPMEngine::resetParticles() {
-  quiesce();
+  prepareHostAccess(true);
   live_ = 0;
 }
 
@@ -313,9 +348,10 @@ void MPMEngine::uploadState(const float* const f[8], uint32_t n) {
   if (n > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "more particles than capacity");
   for (int k = 0; k < 8; ++k)
     if (n && !f[k]) throw Error(NEBULA_MPM_ERR_INVALID, "null field");
-  quiesce();
+  prepareHostAccess(true);
+  StatePtrs st = statePtrs(cur_);
   for (int k = 0; k < 8; ++k)
-    if (n) check(cudaMemcpy(state_[k].ptr, f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice), "upload state");
+    if (n) check(cudaMemcpy(st.f[k], f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice), "upload state");
   live_ = n;
 }
 
@@ -323,8 +359,16 @@ void MPMEngine::download(int field, float* host, uint64_t count) {
   if (field < 0 || field > 7) throw Error(NEBULA_MPM_ERR_INVALID, "field index out of range");
   if (count != uint64_t(live_) * 4) throw Error(NEBULA_MPM_ERR_INVALID, "count must be 4 * live particles");
   if (count && !host) throw Error(NEBULA_MPM_ERR_INVALID, "null host buffer");
+  bindDevice();
+  const float4* src = statePtrs(cur_).f[field];
+  if (permuted_ && live_) {
+    // original order into the idle buffer (free between substeps)
+    StatePtrs tmp = statePtrs(cur_ ^ 1);
+    check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, lastStream_, &launches_), "unpermute");
+    src = tmp.f[field];
+  }
   quiesce();
-  if (count) check(cudaMemcpy(host, state_[field].ptr, count * sizeof(float), cudaMemcpyDeviceToHost), "download");
+  if (count) check(cudaMemcpy(host, src, count * sizeof(float), cudaMemcpyDeviceToHost), "download");
 }
 
 SubstepParams MPMEngine::buildParams(float subDt) const {
@@ -356,13 +400,70 @@ SubstepParams MPMEngine::buildParams(float subDt) const {
   return P;
 }
 
-StatePtrs MPMEngine::statePtrs() {
+StatePtrs MPMEngine::statePtrs(int buf) {
   StatePtrs s;
-  for (int k = 0; k < 8; ++k) s.f[k] = static_cast<float4*>(state_[k].ptr);
+  for (int k = 0; k < 8; ++k) s.f[k] = static_cast<float4*>(buf == 0 ? state_[k].ptr : stateB_[k].ptr);
   return s;
+}
+StatePtrs MPMEngine::statePtrs() { return statePtrs(cur_); }
+
+BrickBuffers MPMEngine::brickBuffers() {
+  BrickBuffers b;
+  b.nb = nb_;
+  b.tiles = tiles_;
+  b.brickCount = static_cast<uint32_t*>(bCount_.ptr);
+  b.brickFlag = static_cast<uint32_t*>(bFlag_.ptr);
+  b.brickStart = static_cast<uint32_t*>(bStart_.ptr);
+  b.pbBrick = static_cast<uint32_t*>(pbBrick_.ptr);
+  b.pbStart = static_cast<uint32_t*>(pbStart_.ptr);
+  b.gbBrick = static_cast<uint32_t*>(gbBrick_.ptr);
+  b.counters = static_cast<uint32_t*>(counters_.ptr);
+  b.scanState = static_cast<unsigned long long*>(scanState_.ptr);
+  b.scanTile = static_cast<unsigned long long*>(scanTile_.ptr);
+  b.binKey = static_cast<uint32_t*>(binKey_.ptr);
+  b.binRank = static_cast<uint32_t*>(binRank_.ptr);
+  b.perm = static_cast<uint32_t*>(perm_.ptr);
+  return b;
+}
+
+GridBuffers MPMEngine::gridBuffers() {
+  GridBuffers g;
+  g.acc = static_cast<float4*>(gridAcc_.ptr);
+  g.vel = static_cast<float4*>(gridVel_.ptr);
+  g.vold = nullptr;
+  if (params_.flip_ratio > 0.01f) {
+    if (!gridVold_.ptr) {
+      gridVold_.alloc(size_t(ncPad_) * sizeof(float4));
+      check(cudaMemset(gridVold_.ptr, 0, gridVold_.bytes), "cudaMemset");
+    }
+    g.vold = static_cast<float4*>(gridVold_.ptr);
+  }
+  return g;
+}
+
+// Buffers of the dense pipeline (and of the reference-format binning export),
+// allocated on first use.
+void MPMEngine::ensureDense() {
+  if (denseReady_) return;
+  const size_t nc = hashCells_;
+  const size_t pc = size_t(std::max(capacity_, 1u)) * sizeof(uint32_t);
+  gridMom_.alloc(nc * 2 * sizeof(float4));
+  gridMass_.alloc(nc * sizeof(float));
+  check(cudaMemset(gridMom_.ptr, 0, gridMom_.bytes), "cudaMemset");
+  check(cudaMemset(gridMass_.ptr, 0, gridMass_.bytes), "cudaMemset");
+  cellCount_.alloc(nc * sizeof(uint32_t));
+  cellStart_.alloc(nc * sizeof(uint32_t));
+  cellEnd_.alloc(nc * sizeof(uint32_t));
+  key_.alloc(pc);
+  rank_.alloc(pc);
+  sortedTmp_.alloc(pc);
+  sorted_.alloc(pc);
+  scanWs_.alloc(scanWorkspaceBytes(nc));
+  denseReady_ = true;
 }
 
 BinBuffers MPMEngine::binBuffers() {
+  ensureDense();
   BinBuffers b;
   b.cellCount = static_cast<uint32_t*>(cellCount_.ptr);
   b.cellStart = static_cast<uint32_t*>(cellStart_.ptr);
@@ -377,19 +478,87 @@ BinBuffers MPMEngine::binBuffers() {
   return b;
 }
 
-// One substep in the reference's pass order (MPMEngine.cpp:419-472): zero the
-// grid, bin, P2G, grid update (+ SDF boundary fused per node), G2P.
+// Put the particles back in original order (buffer index == particle index).
+void MPMEngine::normalizeOrder(cudaStream_t s) {
+  if (!permuted_) return;
+  StatePtrs src = statePtrs(cur_), dst = statePtrs(cur_ ^ 1);
+  check(launchUnpermute(src, static_cast<const uint32_t*>(pid_[cur_].ptr), dst, live_, s, &launches_), "unpermute");
+  cur_ ^= 1;
+  check(launchIota(static_cast<uint32_t*>(pid_[cur_].ptr), capacity_, s, &launches_), "iota");
+  permuted_ = false;
+  // the pending bins index the old order
+  discardPending(s);
+}
+
+void MPMEngine::discardPending(cudaStream_t s) {
+  if (!pending_) return;
+  check(launchClearBricks(brickBuffers(), gridBuffers(), numSMs_, s, &launches_), "clear bricks");
+  pending_ = false;
+}
+
+bool MPMEngine::pendingMatches(float subDt) const {
+  return pending_ && pendingDt_ == subDt && pendingApic_ == (params_.flip_ratio < -0.5f);
+}
+
+// Bin the current particles (buffer order), then P2G them into the brick grid.
+void MPMEngine::buildPending(const SubstepParams& P, cudaStream_t s) {
+  BrickBuffers B = brickBuffers();
+  GridBuffers G = gridBuffers();
+  uint32_t* err = static_cast<uint32_t*>(err_.ptr);
+  uint64_t l0 = launches_;
+  phaseBegin(kPhaseBin, s);
+  check(launchBrickCount(P, statePtrs(cur_).f[0], live_, B, err, s, &launches_), "brick count");
+  check(launchBrickScan(B, scanEpoch_++, err, s, &launches_), "brick scan");
+  check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
+  phaseEnd(kPhaseBin, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseP2G, s);
+  check(launchP2GBricks(P, statePtrs(cur_), live_, B, G, P.dt, numSMs_, s, &launches_), "p2g bricks");
+  phaseEnd(kPhaseP2G, s, l0);
+  pending_ = true;
+  pendingDt_ = P.dt;
+  pendingApic_ = P.flip_ratio < -0.5f;
+}
+
+// One substep on the pending grid: grid update, fused G2P + P2G (+ binning
+// count), brick scan, permutation.  Leaves the next substep's grid pending.
+void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
+  BrickBuffers B = brickBuffers();
+  GridBuffers G = gridBuffers();
+  uint32_t* err = static_cast<uint32_t*>(err_.ptr);
+  uint64_t l0 = launches_;
+  phaseBegin(kPhaseGrid, s);
+  check(launchGridBricks(P, B, G, numSMs_, s, &launches_), "grid bricks");
+  phaseEnd(kPhaseGrid, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseFused, s);
+  check(launchG2P2G(P, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
+                    static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, P.dt, err, numSMs_, s, &launches_),
+        "g2p2g");
+  phaseEnd(kPhaseFused, s, l0);
+  l0 = launches_;
+  phaseBegin(kPhaseBin, s);
+  check(launchBrickScan(B, scanEpoch_++, err, s, &launches_), "brick scan");
+  check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
+  phaseEnd(kPhaseBin, s, l0);
+  cur_ ^= 1;
+  permuted_ = true;
+  ++substeps_;
+}
+
+// One substep in the reference's pass order (MPMEngine.cpp:419-472): bin,
+// zero the grid, P2G, grid update (+ SDF boundary fused per node), G2P.
 void MPMEngine::substepDense(const SubstepParams& P, cudaStream_t s) {
   BinBuffers b = binBuffers();
-  StatePtrs st = statePtrs();
+  StatePtrs st = statePtrs(cur_);
   uint64_t l0 = launches_;
   phaseBegin(kPhaseBin, s);
   check(launchBin(P, st.f[0], live_, b, s, &launches_), "bin");
   phaseEnd(kPhaseBin, s, l0);
-  l0 = launches_;
-  phaseBegin(kPhaseP2G, s);
   check(cudaMemsetAsync(gridMom_.ptr, 0, gridMom_.bytes, s), "zero grid");
   check(cudaMemsetAsync(gridMass_.ptr, 0, gridMass_.bytes, s), "zero grid");
+  l0 = launches_;
+  phaseBegin(kPhaseP2G, s);
   check(launchP2GDense(P, st, b.sorted, live_, static_cast<float4*>(gridMom_.ptr), static_cast<float*>(gridMass_.ptr), s, &launches_), "p2g");
   phaseEnd(kPhaseP2G, s, l0);
   l0 = launches_;
@@ -407,32 +576,91 @@ void MPMEngine::substepDense(const SubstepParams& P, cudaStream_t s) {
 void MPMEngine::step(float dt, cudaStream_t s) {
   bindDevice();
   if (!(dt >= 0.f) || !std::isfinite(dt)) throw Error(NEBULA_MPM_ERR_INVALID, "dt must be finite and >= 0");
-  lastStream_ = s;
+  if (s != lastStream_) {
+    // work queued on the previous stream must finish first
+    quiesce();
+    lastStream_ = s;
+  }
   const int n = std::max(1, params_.numSubsteps);
   const float subDt = dt / float(n);  // MPMEngine.cpp:413
   const SubstepParams P = buildParams(subDt);
-  for (int k = 0; k < params_.numSubsteps; ++k) substepDense(P, s);
+  if (params_.numSubsteps <= 0 || live_ == 0) return;
+  if (pipeline_ == NEBULA_MPM_PIPELINE_DENSE) {
+    normalizeOrder(s);
+    discardPending(s);
+    for (int k = 0; k < params_.numSubsteps; ++k) substepDense(P, s);
+    return;
+  }
+  if (!pendingMatches(subDt)) {
+    discardPending(s);
+    buildPending(P, s);
+  }
+  for (int k = 0; k < params_.numSubsteps; ++k) substepFused(P, s);
 }
 
 void MPMEngine::exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt) {
   bindDevice();
   const SubstepParams P = buildParams(0.f);
   BinBuffers b = binBuffers();
-  check(launchBin(P, static_cast<const float4*>(state_[0].ptr), live_, b, lastStream_, &launches_), "bin");
+  const float4* pos = statePtrs(cur_).f[0];
+  if (permuted_ && live_) {
+    StatePtrs tmp = statePtrs(cur_ ^ 1);
+    check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, lastStream_, &launches_), "unpermute");
+    pos = tmp.f[0];
+  }
+  check(launchBin(P, pos, live_, b, lastStream_, &launches_), "bin");
   quiesce();
   check(cudaMemcpy(cnt, b.cellCount, size_t(hashCells_) * 4, cudaMemcpyDeviceToHost), "download bins");
   check(cudaMemcpy(off, b.cellEnd, size_t(hashCells_) * 4, cudaMemcpyDeviceToHost), "download bins");
   if (live_) check(cudaMemcpy(srt, b.sorted, size_t(live_) * 4, cudaMemcpyDeviceToHost), "download bins");
 }
 
+void MPMEngine::exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids) {
+  bindDevice();
+  if (pipeline_ != NEBULA_MPM_PIPELINE_FUSED) throw Error(NEBULA_MPM_ERR_INVALID, "brick bins exist in the FUSED pipeline only");
+  cudaStream_t s = lastStream_;
+  // binning does not depend on dt; a grid built here is rebuilt by a step with dt != 0
+  if (!pending_) buildPending(buildParams(0.f), s);
+  uint32_t* tmp = static_cast<uint32_t*>(binKey_.ptr);  // free between substeps
+  check(launchSortedPid(static_cast<const uint32_t*>(perm_.ptr), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, s, &launches_),
+        "sorted pid");
+  quiesce();
+  uint32_t cnt[kCntSlots];
+  check(cudaMemcpy(cnt, counters_.ptr, sizeof(cnt), cudaMemcpyDeviceToHost), "download counters");
+  *numBricks = cnt[kCntNumPB];
+  if (cnt[kCntNumPB] > nb_) throw Error(NEBULA_MPM_ERR_DEVICE, "brick count exceeds the brick grid");
+  check(cudaMemcpy(brickIds, pbBrick_.ptr, size_t(cnt[kCntNumPB]) * 4, cudaMemcpyDeviceToHost), "download bricks");
+  check(cudaMemcpy(brickStarts, pbStart_.ptr, size_t(cnt[kCntNumPB] + 1) * 4, cudaMemcpyDeviceToHost), "download bricks");
+  if (live_) check(cudaMemcpy(sortedPids, tmp, size_t(live_) * 4, cudaMemcpyDeviceToHost), "download bricks");
+  // binKey is rebuilt by the next binning; the pending grid stays valid
+}
+
 void MPMEngine::exportGrid(float dt, float* mom, float* mass) {
   bindDevice();
   const SubstepParams P = buildParams(dt);
   cudaStream_t s = lastStream_;
+  std::vector<float4> acc(hashCells_);
+  if (pipeline_ == NEBULA_MPM_PIPELINE_FUSED) {
+    if (!pendingMatches(dt)) {
+      discardPending(s);
+      buildPending(P, s);
+    }
+    quiesce();
+    check(cudaMemcpy(acc.data(), gridAcc_.ptr, size_t(hashCells_) * sizeof(float4), cudaMemcpyDeviceToHost), "download grid");
+    for (uint32_t i = 0; i < hashCells_; ++i) {
+      mom[4 * size_t(i)] = acc[i].x;
+      mom[4 * size_t(i) + 1] = acc[i].y;
+      mom[4 * size_t(i) + 2] = acc[i].z;
+      mom[4 * size_t(i) + 3] = 0.f;
+      mass[i] = acc[i].w;
+    }
+    return;
+  }
+  normalizeOrder(s);
+  BinBuffers b = binBuffers();
+  StatePtrs st = statePtrs(cur_);
   check(cudaMemsetAsync(gridMom_.ptr, 0, gridMom_.bytes, s), "zero grid");
   check(cudaMemsetAsync(gridMass_.ptr, 0, gridMass_.bytes, s), "zero grid");
-  BinBuffers b = binBuffers();
-  StatePtrs st = statePtrs();
   check(launchBin(P, st.f[0], live_, b, s, &launches_), "bin");
   check(launchP2GDense(P, st, b.sorted, live_, static_cast<float4*>(gridMom_.ptr), static_cast<float*>(gridMass_.ptr), s, &launches_), "p2g");
   quiesce();
@@ -450,6 +678,14 @@ uint32_t MPMEngine::syncAndCheck() {
 
 void MPMEngine::stats(nebula_mpm_stats* s) {
   std::memset(s, 0, sizeof(*s));
+  if (pipeline_ == NEBULA_MPM_PIPELINE_FUSED && counters_.ptr) {
+    quiesce();
+    uint32_t cnt[kCntSlots];
+    check(cudaMemcpy(cnt, counters_.ptr, sizeof(cnt), cudaMemcpyDeviceToHost), "download counters");
+    particleBricks_ = cnt[kCntNumPB];
+    activeBricks_ = cnt[kCntNumGB];
+    overflow_ = cnt[kCntOverflow];
+  }
   s->substeps = substeps_;
   s->live_particles = live_;
   s->active_bricks = activeBricks_;
@@ -600,6 +836,15 @@ int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_
   return guarded([&] {
     if (!ms || !launches) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
     E(e).profileRead(ms, launches, reset != 0);
+  });
+}
+int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline) {
+  return guarded([&] { E(e).setPipeline(pipeline); });
+}
+int nebula_mpm_export_brick_bins(nebula_mpm* e, uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids) {
+  return guarded([&] {
+    if (!numBricks || !brickIds || !brickStarts || (!sortedPids && E(e).liveCount())) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).exportBrickBins(numBricks, brickIds, brickStarts, sortedPids);
   });
 }
 int nebula_mpm_export_bins(nebula_mpm* e, uint32_t* cnt, uint32_t* off, uint32_t* srt) {

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/nebula_mpm.h"
+#include "mpm_bricks.cuh"
 #include "mpm_device.cuh"
 #include "mpm_internal.h"
 
@@ -64,6 +65,9 @@ class MPMEngine {
   void exportGrid(float dt, float* mom, float* mass);
   void profileEnable(bool on);
   void profileRead(double* ms, uint64_t* launches, bool reset);
+  void setPipeline(int p);
+  int pipeline() const { return pipeline_; }
+  void exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids);
 
  private:
   // phase timing
@@ -88,6 +92,17 @@ class MPMEngine {
   StatePtrs statePtrs();
   BinBuffers binBuffers();
   void substepDense(const SubstepParams& P, cudaStream_t s);
+  // brick-sparse fused pipeline
+  StatePtrs statePtrs(int buf);
+  BrickBuffers brickBuffers();
+  GridBuffers gridBuffers();
+  void ensureDense();
+  void normalizeOrder(cudaStream_t s);
+  void discardPending(cudaStream_t s);
+  void buildPending(const SubstepParams& P, cudaStream_t s);
+  void substepFused(const SubstepParams& P, cudaStream_t s);
+  void prepareHostAccess(bool modifiesParticles);
+  bool pendingMatches(float subDt) const;
 
   nebula_mpm_config cfg_;
   nebula_mpm_params params_{0.3f, 0.0f, 20, 0u, 1e5f, 0.577f, 0.0f, 0.0f};  // MPMEngine.h:72-80
@@ -100,6 +115,21 @@ class MPMEngine {
   cudaStream_t lastStream_ = nullptr;
 
   DevBuf state_[8];
+  DevBuf stateB_[8];
+  DevBuf pid_[2];
+  int cur_ = 0;
+  bool permuted_ = false;
+  int pipeline_ = NEBULA_MPM_PIPELINE_FUSED;
+  int numSMs_ = 148;
+  // brick-sparse grid + binning
+  uint32_t ncPad_ = 64, nb_ = 1, tiles_ = 1;
+  DevBuf gridAcc_, gridVel_, gridVold_;
+  DevBuf bCount_, bFlag_, bStart_, pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_;
+  uint32_t scanEpoch_ = 0;
+  bool pending_ = false;
+  float pendingDt_ = 0.f;
+  bool pendingApic_ = false;
+  bool denseReady_ = false;
   DevBuf gridMom_, gridMass_;
   DevBuf cellCount_, cellStart_, cellEnd_, key_, rank_, sortedTmp_, sorted_, scanWs_;
   DevBuf materials_, colliders_, forces_, sdf_, err_;

@@ -82,10 +82,7 @@ __global__ void __launch_bounds__(kThreads) k_p2g_dense(SubstepParams P, StatePt
   s.B0 = st.f[5][p]; s.B1 = st.f[6][p]; s.B2 = st.f[7][p];
   p2gParticle(P, s, P.dt, [&](int nx, int ny, int nz, float mx, float my, float mz, float m) {
     uint32_t nid = mortonEncode(nx, ny, nz);
-    float* g = reinterpret_cast<float*>(gridMom + nid);
-    atomicAdd(g + 0, mx);
-    atomicAdd(g + 1, my);
-    atomicAdd(g + 2, mz);
+    redAddV4(gridMom + nid, mx, my, mz, 0.f);
     atomicAdd(gridMass + nid, m);
   });
 }

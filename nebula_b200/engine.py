@@ -211,6 +211,23 @@ class MPMEngine:
         call("nebula_mpm_get_stats", self._h, C.byref(s))
         return {k: (list(getattr(s, k)) if k == "grid_res" else getattr(s, k)) for k, _ in s._fields_}
 
+    # ------------------------------------------------------------ pipeline
+    def set_pipeline(self, name: str):
+        """"fused" (default: brick-sparse, fused G2P+P2G) or "dense" (one kernel per reference dispatch)."""
+        call("nebula_mpm_set_pipeline", self._h, {"dense": _capi.PIPELINE_DENSE, "fused": _capi.PIPELINE_FUSED}[name])
+
+    def export_brick_bins(self):
+        """The engine's brick binning: (brick ids, start slots, original particle id per slot)."""
+        st = self.stats()
+        nb = max(1, st["hash_cells"] // 64)
+        n = st["live_particles"]
+        ids = np.empty(nb, np.uint32)
+        starts = np.empty(nb + 1, np.uint32)
+        pids = np.empty(max(1, n), np.uint32)
+        k = C.c_uint32()
+        call("nebula_mpm_export_brick_bins", self._h, C.byref(k), _ptr(ids), _ptr(starts), _ptr(pids))
+        return ids[: k.value].copy(), starts[: k.value + 1].copy(), pids[:n].copy()
+
     # ------------------------------------------------------------ device timing
     PHASES = ("bin", "p2g", "grid", "g2p", "g2p2g", "other")
 
@@ -241,13 +258,15 @@ class MPMEngine:
         return mom, mass
 
 
-def engine_for_scene(scene, capacity: int | None = None) -> MPMEngine:
+def engine_for_scene(scene, capacity: int | None = None, pipeline: str = "fused") -> MPMEngine:
     """An engine configured like `scene` (domain, materials, forces, colliders,
     SDF, transfer mode) holding the scene's particle state."""
     sp = scene.params
     cfg = MPMConfig(nx=0, ny=0, nz=0, domainSize=tuple(sp.domain_size), cellSize=sp.cell_size,
                     maxParticles=int(capacity or scene.n), E=1e4, nu=0.3, rho0=sp.rho0)
     eng = MPMEngine(cfg)
+    if pipeline != "fused":
+        eng.set_pipeline(pipeline)
     eng.flip_ratio = sp.flip_ratio
     eng.M_friction = sp.M_friction
     eng.q_cohesion = sp.q_cohesion

@@ -263,6 +263,28 @@ def elastic_block(seed=1, n_side=20, res=64, substeps=100, dt=1e-4, flip_ratio=-
     return Scene("elastic_block_8k_64", params, make_state(pos, vp), substeps)
 
 
+def shear_block(model=MAT_ELASTIC, seed=1, gamma=20.0, substeps=100, dt=1e-4, flip_ratio=-1.0):
+    """Parity variant of the elastic block: same 8,000-particle geometry on 64^3,
+    rho 1000 instead of 1 (with rho = 1 and E = 1e4 the wave CFL number is
+    c dt / h = 0.74 and the reference algorithm blows up within ~40 substeps in
+    float32 and float64 alike), and an initial shear velocity v_x = gamma (y - 0.7)
+    so that F develops distinct singular values.  model: ELASTIC (E=1e4),
+    VON_MISES (E=1e4, q_max=200) or DRUCKER_PRAGER (E=3.5e5, rho 1600, 30 deg)."""
+    sc = elastic_block(seed=seed, substeps=substeps, dt=dt, flip_ratio=flip_ratio)
+    if model == MAT_DRUCKER_PRAGER:
+        m = material(model, 3.5e5, 0.3, 1600.0, M_friction=math.tan(math.radians(30.0)))
+    elif model == MAT_VON_MISES:
+        m = material(model, 1e4, 0.3, 1000.0, q_max=200.0)
+    else:
+        m = material(MAT_ELASTIC, 1e4, 0.3, 1000.0)
+    sc.params.materials = [m]
+    sc.params.rho0 = float(m["rho0"])
+    P = sc.state["P"]
+    sc.state["v"][:, 0] = (gamma * (P[:, 1].astype(np.float64) - 0.7)).astype(np.float32)
+    sc.name = "shear_block_%s_8k_64" % ("elastic", "vonmises", "druckerprager")[min(model, 2)]
+    return sc
+
+
 def multimaterial(seed=2, res=128, substeps=200, dt=5e-5):
     """80,000 particles on 128^3: a 40,000-particle jelly cube (Hencky E=5e3,
     rho 1000) dropped on a 40,000-particle Drucker-Prager sand slab (E=3.5e5,

@@ -1,0 +1,191 @@
+"""The brick-sparse fused pipeline (default engine path) on the GPU.
+
+Checks the engine's own brick binning against the oracle's cell binning, the
+fused pipeline against the dense one and the oracle, and the host paths that
+invalidate a pending P2G (dt changes, uploads, appends, parameter changes).
+"""
+import numpy as np
+import pytest
+
+from nebula_b200 import scenes as S
+from nebula_b200.engine import engine_for_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def oracle_run(sc, n, mode="ref32"):
+    from oracle import Oracle
+    o = Oracle(mode)
+    o.set_params(sc.params)
+    o.set_sdf(sc.sdf)
+    o.set_state(sc.state)
+    o.run(n)
+    return o.get_state()
+
+
+def Fm(st):
+    return np.concatenate([st["F0"][:, :3], st["F1"][:, :3], st["F2"][:, :3]], axis=1)
+
+
+@pytest.mark.parametrize("make", [S.elastic_block, S.multimaterial, lambda: S.slope_flow(with_sdf=False)],
+                         ids=["elastic_8k_64", "multimaterial_80k_128", "slope_1m_256"])
+def test_brick_bins_match_oracle_cells(make):
+    """Every listed brick holds exactly the particles whose cell Morton code >> 6
+    is that brick; bricks are listed in ascending order."""
+    sc = make()
+    eng = engine_for_scene(sc)
+    ids, starts, pids = eng.export_brick_bins()
+    from oracle import Oracle
+    o = Oracle("ref32")
+    o.set_params(sc.params)
+    o.set_state(sc.state)
+    o.bin()
+    cnt, off, srt = o.get_bins()
+    cell_of = np.empty(sc.n, np.uint32)
+    nz = np.nonzero(cnt)[0]
+    for c in nz:
+        cell_of[srt[off[c] - cnt[c]:off[c]]] = c
+    brick_of = cell_of >> 6
+    assert np.all(np.diff(ids.astype(np.int64)) > 0)
+    assert starts[0] == 0 and starts[-1] == sc.n
+    assert np.array_equal(np.sort(pids), np.arange(sc.n, dtype=np.uint32))
+    seg = np.repeat(ids, np.diff(starts))
+    assert np.array_equal(seg, brick_of[pids])
+
+
+def test_brick_bins_after_substeps():
+    """Binning produced inside the fused kernel after 30 substeps."""
+    sc = S.shear_block()
+    eng = engine_for_scene(sc)
+    eng.run_substeps(sc.params.dt, 30)
+    st = eng.state()
+    ids, starts, pids = eng.export_brick_bins()
+    h = sc.params.cell_size
+    g = np.clip(np.floor(st["P"][:, :3].astype(np.float32) / np.float32(h)), 0, 63).astype(np.int64)
+    brick = S.morton_encode(g[:, 0], g[:, 1], g[:, 2]) >> 6
+    assert np.array_equal(np.repeat(ids, np.diff(starts)), brick[pids])
+
+
+@pytest.mark.parametrize("make,n", [(S.shear_block, 100), (S.multimaterial, 60)], ids=["elastic_shear", "multimaterial"])
+def test_fused_matches_dense(make, n):
+    sc = make()
+    a = engine_for_scene(sc, pipeline="fused")
+    b = engine_for_scene(sc, pipeline="dense")
+    a.run_substeps(sc.params.dt, n)
+    b.run_substeps(sc.params.dt, n)
+    sa, sb = a.state(), b.state()
+    ex, ev = rel_l2(sa["P"][:, :3], sb["P"][:, :3]), rel_l2(sa["v"][:, :3], sb["v"][:, :3])
+    print("fused vs dense after %d substeps: x %.2e v %.2e" % (n, ex, ev))
+    assert ex < 1e-5 and ev < 1e-3
+
+
+def test_fused_elastic_shear_vs_oracle_in_chunks():
+    """100 substeps as 7 step() calls of different dt lengths (pending grid
+    rebuilt whenever the substep length changes)."""
+    sc = S.shear_block()
+    eng = engine_for_scene(sc)
+    dt = sc.params.dt
+    for k in (10, 20, 5, 25, 15, 10, 15):
+        eng.run_substeps(dt, k)
+    gs = eng.state()
+    rs = oracle_run(sc, 100)
+    ex, eF = rel_l2(gs["P"][:, :3], rs["P"][:, :3]), rel_l2(Fm(gs), Fm(rs))
+    print("chunked fused: x %.2e F %.2e" % (ex, eF))
+    assert ex <= 1e-4 and eF <= 1e-4
+
+
+def test_fused_dt_change_rebuilds_pending_grid():
+    sc = S.shear_block()
+    eng = engine_for_scene(sc)
+    dt = sc.params.dt
+    eng.run_substeps(dt, 10)
+    eng.run_substeps(dt / 2, 10)  # different substep length
+    gs = eng.state()
+    from oracle import Oracle
+    o = Oracle("ref32")
+    o.set_params(sc.params)
+    o.set_state(sc.state)
+    o.run(10)
+    sp2 = sc.params
+    sp2.dt = dt / 2
+    o.set_params(sp2)
+    o.run(10)
+    rs = o.get_state()
+    assert rel_l2(gs["P"][:, :3], rs["P"][:, :3]) < 1e-5
+    assert rel_l2(Fm(gs), Fm(rs)) < 1e-5
+
+
+def test_fused_host_edits_between_steps():
+    """Upload / append / material ids between steps see particles in original order."""
+    sc = S.shear_block()
+    eng = engine_for_scene(sc, capacity=sc.n + 100)
+    eng.run_substeps(sc.params.dt, 10)
+    st = eng.state()
+    # original order after reordering: particle 0 is still particle 0
+    rs = oracle_run(sc, 10)
+    assert rel_l2(st["P"][:, :3], rs["P"][:, :3]) < 1e-6
+    # append 100 particles and keep stepping
+    pos = np.tile(np.array([[0.3, 0.3, 0.3, 1e-6]], np.float32), (100, 1))
+    pos[:, 0] += np.linspace(0, 0.05, 100, dtype=np.float32)
+    vel = np.zeros((100, 4), np.float32)
+    assert eng.appendParticles(pos, vel) == 100
+    eng.run_substeps(sc.params.dt, 10)
+    st2 = eng.state()
+    assert st2["P"].shape[0] == sc.n + 100
+    assert np.all(np.isfinite(st2["P"]))
+    # the appended particles fell under gravity only
+    assert np.all(st2["v"][sc.n:, 1] < 0)
+    # re-upload the original scene: result equals a fresh run
+    eng.upload_state(sc.state)
+    eng.run_substeps(sc.params.dt, 10)
+    st3 = eng.state()
+    assert rel_l2(st3["P"][:, :3], rs["P"][:, :3]) < 1e-6
+
+
+def test_fused_flip_and_pic_vs_oracle():
+    for flip in (0.0, 0.95):
+        sc = S.shear_block(flip_ratio=flip)
+        eng = engine_for_scene(sc)
+        eng.run_substeps(sc.params.dt, 60)
+        gs = eng.state()
+        rs = oracle_run(sc, 60)
+        ex, ev = rel_l2(gs["P"][:, :3], rs["P"][:, :3]), rel_l2(gs["v"][:, :3], rs["v"][:, :3])
+        print("flip %.2f: x %.2e v %.2e" % (flip, ex, ev))
+        assert ex < 1e-5 and ev < 1e-4
+
+
+def test_fused_fast_particle_leaves_tile():
+    """A FLIP particle crossing several cells per substep scatters outside its
+    block tile (global-reduction path) and still matches the oracle."""
+    sp = S.StepParams(dt=5e-3, cell_size=1.0 / 16, domain_size=(1.0, 1.0, 1.0), flip_ratio=1.0,
+                      materials=[S.material(S.MAT_ELASTIC, 1e3, 0.3, 1000.0)], forces=[])
+    pos = np.array([[0.3, 0.5, 0.5], [0.5, 0.5, 0.5]], np.float32)
+    st = S.make_state(pos, np.float32(1e-4), vel=np.array([[40.0, 0.0, 0.0], [0.0, 0.0, 0.0]], np.float32))
+    sc = S.Scene("fast", sp, st, 8)
+    eng = engine_for_scene(sc)
+    eng.run_substeps(sp.dt, 4)
+    gs = eng.state()
+    assert eng.stats()["overflow_particles"] > 0
+    rs = oracle_run(sc, 4)
+    assert rel_l2(gs["P"][:, :3], rs["P"][:, :3]) < 1e-6
+    assert rel_l2(gs["v"][:, :3], rs["v"][:, :3]) < 1e-5
+
+
+def test_fused_export_grid_after_step_is_p2g_of_state():
+    """The grid left pending by the fused kernel equals a fresh P2G of the
+    updated particles."""
+    sc = S.shear_block()
+    eng = engine_for_scene(sc)
+    eng.run_substeps(sc.params.dt, 12)
+    mom, mass = eng.export_grid(sc.params.dt)  # pending grid from the fused scatter
+    st = eng.state()
+    sc2 = S.Scene("x", sc.params, st, 0)
+    fresh = engine_for_scene(sc2)
+    fmom, fmass = fresh.export_grid(sc.params.dt)  # standalone P2G
+    assert rel_l2(mom[:, :3], fmom[:, :3]) < 1e-5 and rel_l2(mass, fmass) < 1e-5
