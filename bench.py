@@ -296,10 +296,13 @@ def main():
     per_launch_ms = dom_ms / calls
     alg = algorithmic_bytes(dom, n, active, sp.hash_cells, flip, sdf)
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
+    # dram__bytes_read.sum + dram__bytes_write.sum of one launch, from the committed ncu summary
     traffic = None
-    tf = ROOT / "profiles" / ("traffic_%s_%s.json" % (dom, sc.name))
+    tf = ROOT / "profiles" / ("%s_%s.txt" % (dom, sc.name.replace("slope_flow", "slope")))
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        for ln in tf.read_text().splitlines():
+            if ln.startswith("dram_bytes_per_launch"):
+                traffic = float(ln.split("=")[1])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "kernel": dom, "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms, "peak_source": src + " (hbm_gbs)"}
     substep_ms = ms / (args.steps * S)

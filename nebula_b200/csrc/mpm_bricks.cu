@@ -95,13 +95,18 @@ __device__ uint32_t lookBack(unsigned long long* st, uint32_t tile, uint32_t agg
   return prefix;
 }
 
-__global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B, unsigned long long launchBase, uint32_t epoch, uint32_t* err) {
-  __shared__ uint32_t s_tile;
+// Tickets from the monotone counter number every tile of every launch: tile =
+// ticket % tiles, launch = ticket / tiles.  Launches are stream-ordered, so one
+// launch's tickets are contiguous, and no host-side value changes between
+// launches (the kernel can be replayed from a CUDA graph).
+__global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B, uint32_t* err) {
+  __shared__ unsigned long long s_ticket;
   __shared__ uint32_t s_warp[3][kBrickScanThreads / 32];
   __shared__ uint32_t s_prefix[3];
-  if (threadIdx.x == 0) s_tile = uint32_t(atomicAdd(B.scanTile, 1ull) - launchBase);
+  if (threadIdx.x == 0) s_ticket = atomicAdd(B.scanTile, 1ull);
   __syncthreads();
-  const uint32_t tile = s_tile;
+  const uint32_t tile = uint32_t(s_ticket % B.tiles);
+  const uint32_t epoch = uint32_t(s_ticket / B.tiles);
   const unsigned long long tag = (unsigned long long)(epoch & 0x3fffu) << 50;
   const uint32_t b0 = tile * kBrickScanTile + threadIdx.x * kBrickScanItems;
   uint32_t cnt[kBrickScanItems];
@@ -220,12 +225,12 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 // the private tiles and one vector reduction per non-zero node.
 constexpr int kChunk = kThreads;
 constexpr int kWarps = kThreads / 32;
-constexpr int kRow = 23;        // floats per input row (22 used; odd stride keeps writes conflict-free)
+constexpr int kRow = 10;        // float4 per input row: 3 axes x 3 offsets of (A0, A1, A2, W), then (m, -, -, -)
 constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
 
 struct P2GSmem {
-  float rows[kChunk * kRow];
+  float4 rows[kChunk * kRow];
   float tiles[kWarps * 4 * kTileNodes];
   uint32_t cellCount[kCellSlots];
   uint32_t cellStart[kCellSlots];
@@ -242,63 +247,75 @@ struct G2P2GSmem {
   float4 vo[FLIP ? 216 : 1];
 };
 
-// Inputs of one particle's P2G: x, m, m v, m (4/h^2) B (APIC), dt Vp tau.
-__device__ __forceinline__ void p2gRow(const SubstepParams& P, const PState& s, float dtStress, float* row) {
+// P2G inputs of one particle in separable form.  The quadratic B-spline weight
+// of node (dx,dy,dz) is W_x[dx] W_y[dy] W_z[dz], so the particle's momentum
+// term  w (m v + m (4/h^2) B r) - dt Vp tau grad w  equals
+//   W_y W_z A_x[dx] + W_x W_z A_y[dy] + W_x W_y A_z[dz]
+// with, per axis c and offset d (r_c = x_i,c - x_p,c, G = N'/h):
+//   A_c[d] = [c == x] m v W_c + (m 4/h^2 B)[:, c] W_c r_c - (dt Vp tau)[:, c] G_c
+// and the mass term is m W_x W_y W_z.  row[3c + d] = (A_c[d], W_c[d]); row[9].x = m.
+__device__ __forceinline__ void p2gRow(const SubstepParams& P, const PState& s, float dtStress, int cx, int cy, int cz, float4* row) {
+  const float invH = 1.0f / P.cellSize;
   const float m = fetchRho0(P, __float_as_uint(s.v.w)) * s.P.w;
-  row[0] = s.P.x; row[1] = s.P.y; row[2] = s.P.z;
-  row[3] = m;
-  row[4] = m * s.v.x; row[5] = m * s.v.y; row[6] = m * s.v.z;
+  const float av[3] = {m * s.v.x, m * s.v.y, m * s.v.z};
+  float Q[3][3];  // GLSL [col][row]
   if (P.flip_ratio < -0.5f) {
     const float k = m * (4.0f / (P.cellSize * P.cellSize));
-    row[7] = k * s.B0.x; row[8] = k * s.B0.y; row[9] = k * s.B0.z;
-    row[10] = k * s.B1.x; row[11] = k * s.B1.y; row[12] = k * s.B1.z;
-    row[13] = k * s.B2.x; row[14] = k * s.B2.y; row[15] = k * s.B2.z;
+    Q[0][0] = k * s.B0.x; Q[0][1] = k * s.B0.y; Q[0][2] = k * s.B0.z;
+    Q[1][0] = k * s.B1.x; Q[1][1] = k * s.B1.y; Q[1][2] = k * s.B1.z;
+    Q[2][0] = k * s.B2.x; Q[2][1] = k * s.B2.y; Q[2][2] = k * s.B2.z;
   } else {
 #pragma unroll
-    for (int i = 7; i < 16; ++i) row[i] = 0.f;
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) Q[c][q] = 0.f;
   }
   const float sdt = dtStress * s.P.w;
-  // symmetric stress: xx yy zz xy xz yz
-  row[16] = sdt * s.F0.w; row[17] = sdt * s.F1.w; row[18] = sdt * s.F2.w;
-  row[19] = sdt * s.B0.w; row[20] = sdt * s.B1.w; row[21] = sdt * s.B2.w;
+  const float T[3][3] = {{sdt * s.F0.w, sdt * s.B0.w, sdt * s.B1.w},
+                         {sdt * s.B0.w, sdt * s.F1.w, sdt * s.B2.w},
+                         {sdt * s.B1.w, sdt * s.B2.w, sdt * s.F2.w}};
+  const float xp[3] = {s.P.x, s.P.y, s.P.z};
+  const int cc[3] = {cx, cy, cz};
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float xi = nodeCentre(P, c, cc[c] - 1 + d);
+      const float dd = (xp[c] - xi) * invH;
+      const float W = bspline2(dd);
+      const float Gc = bspline2g(dd) * invH;
+      const float Rw = W * (xi - xp[c]);
+      float A[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) A[q] = (c == 0 ? av[q] * W : 0.f) + Q[c][q] * Rw - T[c][q] * Gc;
+      row[3 * c + d] = make_float4(A[0], A[1], A[2], W);
+    }
+  row[9] = make_float4(m, 0.f, 0.f, 0.f);
 }
 
-// Contribution of the particle in `row` to the node centred at xi.
-__device__ __forceinline__ void p2gNodeTerm(const float* __restrict__ row, const float xi[3], float invH, float acc[4]) {
-  float wa[3], ga[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float d = (row[a] - xi[a]) * invH;
-    wa[a] = bspline2(d);
-    ga[a] = bspline2g(d);
-  }
-  const float w = wa[0] * wa[1] * wa[2];
+// Contribution of `row` to its stencil node (dx, dy, dz), skipped below w = 1e-12.
+__device__ __forceinline__ void p2gNodeTerm(const float4* __restrict__ row, int dx, int dy, int dz, float acc[4]) {
+  const float4 X = row[dx], Y = row[3 + dy], Z = row[6 + dz];
+  const float wyz = Y.w * Z.w;
+  const float w = X.w * wyz;
   if (w < 1e-12f) return;
-  const float dw0 = ga[0] * wa[1] * wa[2] * invH, dw1 = wa[0] * ga[1] * wa[2] * invH, dw2 = wa[0] * wa[1] * ga[2] * invH;
-  const float r0 = xi[0] - row[0], r1 = xi[1] - row[1], r2 = xi[2] - row[2];
-  const float* Q = row + 7;
-  const float* T = row + 16;
-  const float td0 = T[0] * dw0 + T[3] * dw1 + T[4] * dw2;
-  const float td1 = T[3] * dw0 + T[1] * dw1 + T[5] * dw2;
-  const float td2 = T[4] * dw0 + T[5] * dw1 + T[2] * dw2;
-  acc[0] += w * (row[4] + (Q[0] * r0 + Q[3] * r1 + Q[6] * r2)) - td0;
-  acc[1] += w * (row[5] + (Q[1] * r0 + Q[4] * r1 + Q[7] * r2)) - td1;
-  acc[2] += w * (row[6] + (Q[2] * r0 + Q[5] * r1 + Q[8] * r2)) - td2;
-  acc[3] += w * row[3];
+  const float wxz = X.w * Z.w, wxy = X.w * Y.w;
+  acc[0] += wyz * X.x + wxz * Y.x + wxy * Z.x;
+  acc[1] += wyz * X.y + wxz * Y.y + wxy * Z.y;
+  acc[2] += wyz * X.z + wxz * Y.z + wxy * Z.z;
+  acc[3] += w * row[9].x;
 }
 
 // Direct scatter of one row to global memory (stencils outside the brick's tile).
-__device__ __forceinline__ void p2gRowGlobal(const SubstepParams& P, const float* row, int cx, int cy, int cz, float4* acc) {
-  const float invH = 1.0f / P.cellSize;
+__device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* row, int cx, int cy, int cz, float4* acc) {
   const int cr = int(P.cubeRes);
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int nx = cx + dx, ny = cy + dy, nz = cz + dz;
+  for (int dz = 0; dz < 3; ++dz)
+    for (int dy = 0; dy < 3; ++dy)
+      for (int dx = 0; dx < 3; ++dx) {
+        const int nx = cx + dx - 1, ny = cy + dy - 1, nz = cz + dz - 1;
         if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
-        const float xi[3] = {nodeCentre(P, 0, nx), nodeCentre(P, 1, ny), nodeCentre(P, 2, nz)};
         float a[4] = {0.f, 0.f, 0.f, 0.f};
-        p2gNodeTerm(row, xi, invH, a);
+        p2gNodeTerm(row, dx, dy, dz, a);
         if (a[3] != 0.f || a[0] != 0.f || a[1] != 0.f || a[2] != 0.f) redAddV4(acc + mortonEncode(nx, ny, nz), a[0], a[1], a[2], a[3]);
       }
 }
@@ -350,7 +367,6 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, in
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
-  const float invH = 1.0f / P.cellSize;
   const int cr = int(P.cubeRes);
   float* tile = sm.tiles + warp * 4 * kTileNodes;
   const uint32_t numCells = sm.numCells;
@@ -361,10 +377,9 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, in
     const int lx = rx + dx, ly = ry + dy, lz = rz + dz;  // tile-local node
     const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
     if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
-    const float xi[3] = {nodeCentre(P, 0, nx), nodeCentre(P, 1, ny), nodeCentre(P, 2, nz)};
     float a[4] = {0.f, 0.f, 0.f, 0.f};
     const uint32_t st = sm.cellStart[q], en = st + sm.cellCount[q];
-    for (uint32_t j = st; j < en; ++j) p2gNodeTerm(sm.rows + sm.order[j] * kRow, xi, invH, a);
+    for (uint32_t j = st; j < en; ++j) p2gNodeTerm(sm.rows + sm.order[j] * kRow, dx, dy, dz, a);
     const int t = (lz * 8 + ly) * 8 + lx;
     tile[t] += a[3];
     tile[kTileNodes + t] += a[0];
@@ -424,6 +439,14 @@ struct StagedGrid {
   }
 };
 
+// Generic gather for particles whose stencil leaves the staged block (outside
+// the grid interior); kept out of line to keep the hot loop small.
+template <bool FLIP>
+__device__ __forceinline__ void gatherFallback(const SubstepParams& P, const PState& st, const StagedGrid<FLIP>& grid, float vpic[3], float vpo[3],
+                                            float Gv[3][3], float Bn[3][3]) {
+  g2pGather(P, st, grid, vpic, vpo, Gv, Bn);
+}
+
 // The slot of a particle's stencil centre among the brick's 216 cell slots, or -1.
 __device__ __forceinline__ int cellSlot(int cx, int cy, int cz, int ox, int oy, int oz) {
   const int rx = cx - ox, ry = cy - oy, rz = cz - oz;
@@ -455,10 +478,10 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P, StateP
         const uint32_t s = B.perm[t];
         if (s < n) {
           const PState st = loadState(cur.f, s);
-          float* row = sm.rows + threadIdx.x * kRow;
-          p2gRow(P, st, dtStress, row);
           int cx, cy, cz;
           cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
+          float4* row = sm.rows + threadIdx.x * kRow;
+          p2gRow(P, st, dtStress, cx, cy, cz, row);
           key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
           if (key >= 0) rank = atomicAdd(&sm.cellCount[key], 1u);
           else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
@@ -520,8 +543,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtr
       const int x = sx + q % 6, y = sy + (q / 6) % 6, z = sz + q / 36;
       const bool valid = x >= 0 && y >= 0 && z >= 0 && x < P.gridRes[0] && y < P.gridRes[1] && z < P.gridRes[2];
       const uint32_t c = valid ? mortonEncode(x, y, z) : 0u;
-      S.v[q] = valid ? G.vel[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-      if (FLIP) S.vo[q] = valid ? G.vold[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 v = valid ? G.vel[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const bool live = v.w >= 1e-10f;  // the nodes the shader gathers from
+      if (!live) v = make_float4(0.f, 0.f, 0.f, v.w);
+      S.v[q] = v;
+      if (FLIP) S.vo[q] = live ? G.vold[c] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
     const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
@@ -541,7 +567,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtr
         if (valid) {
           st = loadState(cur.f, s);
           const uint32_t pid = pidCur[s];
-          g2pParticle(P, st, grid, P.dt);
+          float vpic[3], vpo[3], Gv[3][3], Bn[3][3];
+          if (!g2pGatherStaged<FLIP>(P, st, S.v, S.vo, sx, sy, sz, vpic, vpo, Gv, Bn)) gatherFallback<FLIP>(P, st, grid, vpic, vpo, Gv, Bn);
+          g2pUpdate(P, st, P.dt, vpic, vpo, Gv, Bn);
           storeState(nxt.f, t, st);
           pidNxt[t] = pid;
           if (!(isfinite(st.P.x) && isfinite(st.P.y) && isfinite(st.P.z))) atomicOr(err, kErrNonFinite);
@@ -556,8 +584,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtr
         B.binRank[t] = r;
         if (valid) {
           markStencilBricks(P, cx, cy, cz, B.brickFlag);
-          float* row = sm.rows + threadIdx.x * kRow;
-          p2gRow(P, st, dtStress, row);
+          float4* row = sm.rows + threadIdx.x * kRow;
+          p2gRow(P, st, dtStress, cx, cy, cz, row);
           key = cellSlot(cx, cy, cz, sx, sy, sz);
           if (key >= 0) {
             rank = atomicAdd(&sm.cellCount[key], 1u);
@@ -613,8 +641,8 @@ cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t
   return cudaGetLastError();
 }
 
-cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t epoch, uint32_t* err, cudaStream_t s, uint64_t* launches) {
-  k_brick_scan<<<b.tiles, kBrickScanThreads, 0, s>>>(b, (unsigned long long)epoch * b.tiles, epoch, err);
+cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches) {
+  k_brick_scan<<<b.tiles, kBrickScanThreads, 0, s>>>(b, err);
   ++*launches;
   return cudaGetLastError();
 }

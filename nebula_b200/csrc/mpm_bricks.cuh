@@ -51,8 +51,8 @@ struct GridBuffers {
 // Standalone binning of the particles in buffer order: counts + stencil marks.
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches);
-// Compaction scan; epoch must differ from the previous launch's (mod 2^14).
-cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t epoch, uint32_t* err, cudaStream_t s, uint64_t* launches);
+// Compaction scan (tile numbering and status epochs come from a device ticket).
+cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches);
 cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches);
 // P2G of the particles of every listed brick (no binning, no marks).
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,

@@ -176,43 +176,45 @@ template <class T> __device__ __forceinline__ T dexp(T x);
 template <> __device__ __forceinline__ float dexp<float>(float x) { return expf(x); }
 template <> __device__ __forceinline__ double dexp<double>(double x) { return exp(x); }
 
+// One Jacobi rotation zeroing A[P][Q] (P < Q), as mpm_common.glsl:224-244; the
+// pivot pair is a template argument so every index is static.
+template <class T, int P0, int P1>
+__device__ __forceinline__ void jacobiRotate(m3<T>& A, m3<T>& V) {
+  constexpr int R = 3 - P0 - P1;
+  const T apq = A.m[P0][P1];
+  const T app = A.m[P0][P0], aqq = A.m[P1][P1];
+  const T tau = (aqq - app) / (T(2) * apq);
+  const T t = gsign(tau) / (fabs(tau) + dsqrt<T>(T(1) + tau * tau));
+  const T c = T(1) / dsqrt<T>(T(1) + t * t);
+  const T s = t * c;
+  A.m[P0][P0] = app - t * apq;
+  A.m[P1][P1] = aqq + t * apq;
+  A.m[P0][P1] = T(0);
+  A.m[P1][P0] = T(0);
+  const T arp = A.m[R][P0], arq = A.m[R][P1];
+  A.m[R][P0] = c * arp - s * arq;
+  A.m[P0][R] = A.m[R][P0];
+  A.m[R][P1] = s * arp + c * arq;
+  A.m[P1][R] = A.m[R][P1];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const T vrp = V.m[q][P0], vrq = V.m[q][P1];
+    V.m[q][P0] = c * vrp - s * vrq;
+    V.m[q][P1] = s * vrp + c * vrq;
+  }
+}
+
 // jacobiEigen3 (mpm_common.glsl:213-247): cyclic-max Jacobi, <= 20 rotations,
 // stop when every off-diagonal of A is below 1e-8.
 template <class T> __device__ __forceinline__ void jacobiEigen3(m3<T> A, T D[3], m3<T>& V) {
   V = m3ident<T>();
 #pragma unroll 1
   for (int iter = 0; iter < 20; iter++) {
-    T a01 = A.m[0][1], a02 = A.m[0][2], a12 = A.m[1][2];
-    T b01 = fabs(a01), b02 = fabs(a02), b12 = fabs(a12);
+    const T b01 = fabs(A.m[0][1]), b02 = fabs(A.m[0][2]), b12 = fabs(A.m[1][2]);
     if (fmax(b01, fmax(b02, b12)) < T(1e-8)) break;
-    int p0, p1;
-    T apq;
-    if (b01 >= fmax(b02, b12)) { p0 = 0; p1 = 1; apq = a01; }
-    else if (b02 >= b12) { p0 = 0; p1 = 2; apq = a02; }
-    else { p0 = 1; p1 = 2; apq = a12; }
-    const int r = 3 - p0 - p1;  // the untouched index
-    T app = A.m[p0][p0], aqq = A.m[p1][p1];
-    T tau = (aqq - app) / (T(2) * apq);
-    T t = gsign(tau) / (fabs(tau) + dsqrt<T>(T(1) + tau * tau));
-    T c = T(1) / dsqrt<T>(T(1) + t * t);
-    T s = t * c;
-    A.m[p0][p0] = app - t * apq;
-    A.m[p1][p1] = aqq + t * apq;
-    A.m[p0][p1] = T(0);
-    A.m[p1][p0] = T(0);
-    {
-      T arp = A.m[r][p0], arq = A.m[r][p1];
-      A.m[r][p0] = c * arp - s * arq;
-      A.m[p0][r] = A.m[r][p0];
-      A.m[r][p1] = s * arp + c * arq;
-      A.m[p1][r] = A.m[r][p1];
-    }
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      T vrp = V.m[q][p0], vrq = V.m[q][p1];
-      V.m[q][p0] = c * vrp - s * vrq;
-      V.m[q][p1] = s * vrp + c * vrq;
-    }
+    if (b01 >= fmax(b02, b12)) jacobiRotate<T, 0, 1>(A, V);
+    else if (b02 >= b12) jacobiRotate<T, 0, 2>(A, V);
+    else jacobiRotate<T, 1, 2>(A, V);
   }
   D[0] = A.m[0][0];
   D[1] = A.m[1][1];

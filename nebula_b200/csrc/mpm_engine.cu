@@ -508,7 +508,7 @@ void MPMEngine::buildPending(const SubstepParams& P, cudaStream_t s) {
   uint64_t l0 = launches_;
   phaseBegin(kPhaseBin, s);
   check(launchBrickCount(P, statePtrs(cur_).f[0], live_, B, err, s, &launches_), "brick count");
-  check(launchBrickScan(B, scanEpoch_++, err, s, &launches_), "brick scan");
+  check(launchBrickScan(B, err, s, &launches_), "brick scan");
   check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
   phaseEnd(kPhaseBin, s, l0);
   l0 = launches_;
@@ -538,7 +538,7 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   phaseEnd(kPhaseFused, s, l0);
   l0 = launches_;
   phaseBegin(kPhaseBin, s);
-  check(launchBrickScan(B, scanEpoch_++, err, s, &launches_), "brick scan");
+  check(launchBrickScan(B, err, s, &launches_), "brick scan");
   check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
   phaseEnd(kPhaseBin, s, l0);
   cur_ ^= 1;

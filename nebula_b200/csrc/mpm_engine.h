@@ -125,7 +125,6 @@ class MPMEngine {
   uint32_t ncPad_ = 64, nb_ = 1, tiles_ = 1;
   DevBuf gridAcc_, gridVel_, gridVold_;
   DevBuf bCount_, bFlag_, bStart_, pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_;
-  uint32_t scanEpoch_ = 0;
   bool pending_ = false;
   float pendingDt_ = 0.f;
   bool pendingApic_ = false;

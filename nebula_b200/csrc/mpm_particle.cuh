@@ -171,19 +171,19 @@ __device__ __forceinline__ bool gridNode(const SubstepParams& P, int ix, int iy,
 }
 
 // ---------------------------------------------------------------- G2P
-// grid.node(nx, ny, nz, mass, vel, vold) returns false for nodes to skip and
-// fills mass / velocity / pre-force velocity otherwise.
-// Returns a bit set: 1 = J-reset fired, 2 = SDF push-out fired.
+// Gather of mpm_g2p.comp:87-118 through a node accessor: vpic, vpic_old,
+// grad v (G) and the APIC B (both GLSL [col][row]).
 template <class Grid>
-__device__ __forceinline__ uint32_t g2pParticle(const SubstepParams& P, PState& s, const Grid& grid, float dt) {
+__device__ __forceinline__ void g2pGather(const SubstepParams& P, const PState& s, const Grid& grid, float vpic[3], float vpo[3], float G[3][3],
+                                          float Bn[3][3]) {
   const float h = P.cellSize;
   const float xp[3] = {s.P.x, s.P.y, s.P.z};
   int base[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) base[a] = int(floorf(__fdiv_rn(xp[a] - P.worldMin[a], h))) - 1;
   const bool flip = P.flip_ratio > 0.01f;
-  float vpic[3] = {0.f, 0.f, 0.f}, vpo[3] = {0.f, 0.f, 0.f};
-  float G[3][3], Bn[3][3];  // GLSL [col][row]
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vpic[i] = vpo[i] = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -231,7 +231,87 @@ __device__ __forceinline__ uint32_t g2pParticle(const SubstepParams& P, PState& 
           vpo[2] += w * vo.z;
         }
       }
+}
 
+// The same gather from a brick's staged 6^3 node block (origin sx,sy,sz) whose
+// velocities are zero where the node is outside [0, gridRes) or lighter than
+// 1e-10 -- exactly the nodes the shader skips.  The B-spline weights are
+// products of 1D factors, so sums run along x first for each (dy, dz) and are
+// then scaled by the y/z factors.  Returns false when the particle's stencil
+// is not inside the block (the caller then uses g2pGather).
+template <bool FLIP>
+__device__ __forceinline__ bool g2pGatherStaged(const SubstepParams& P, const PState& s, const float4* __restrict__ sv, const float4* __restrict__ svo,
+                                                int sx, int sy, int sz, float vpic[3], float vpo[3], float G[3][3], float Bn[3][3]) {
+  const float h = P.cellSize, invH = 1.0f / P.cellSize;
+  const float xp[3] = {s.P.x, s.P.y, s.P.z};
+  int base[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) base[a] = int(floorf(__fdiv_rn(xp[a] - P.worldMin[a], h))) - 1;
+  const int lx = base[0] - sx, ly = base[1] - sy, lz = base[2] - sz;
+  if ((unsigned)lx > 3u || (unsigned)ly > 3u || (unsigned)lz > 3u) return false;
+  float W[3][3], Gd[3][3], R[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float xi = nodeCentre(P, a, base[a] + k);
+      const float d = (xp[a] - xi) * invH;
+      W[a][k] = bspline2(d);
+      Gd[a][k] = bspline2g(d) * invH;
+      R[a][k] = xi - xp[a];
+    }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vpic[i] = vpo[i] = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) { G[a][b] = 0.f; Bn[a][b] = 0.f; }
+#pragma unroll
+  for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy) {
+      float Sw[3] = {0.f, 0.f, 0.f}, Sr[3] = {0.f, 0.f, 0.f}, Sg[3] = {0.f, 0.f, 0.f}, So[3] = {0.f, 0.f, 0.f};
+      const int q0 = ((lz + dz) * 6 + (ly + dy)) * 6 + lx;
+#pragma unroll
+      for (int dx = 0; dx < 3; ++dx) {
+        const float4 a = sv[q0 + dx];
+        const float wx = W[0][dx], wr = W[0][dx] * R[0][dx], gx = Gd[0][dx];
+        Sw[0] += wx * a.x; Sw[1] += wx * a.y; Sw[2] += wx * a.z;
+        Sr[0] += wr * a.x; Sr[1] += wr * a.y; Sr[2] += wr * a.z;
+        Sg[0] += gx * a.x; Sg[1] += gx * a.y; Sg[2] += gx * a.z;
+        if (FLIP) {
+          const float4 o = svo[q0 + dx];
+          So[0] += wx * o.x; So[1] += wx * o.y; So[2] += wx * o.z;
+        }
+      }
+      const float wyz = W[1][dy] * W[2][dz];
+      const float byy = W[1][dy] * R[1][dy] * W[2][dz];
+      const float bzz = wyz * R[2][dz];
+      const float gyy = Gd[1][dy] * W[2][dz];
+      const float gzz = W[1][dy] * Gd[2][dz];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        vpic[i] += wyz * Sw[i];
+        Bn[0][i] += wyz * Sr[i];
+        Bn[1][i] += byy * Sw[i];
+        Bn[2][i] += bzz * Sw[i];
+        G[0][i] += wyz * Sg[i];
+        G[1][i] += gyy * Sw[i];
+        G[2][i] += gzz * Sw[i];
+        if (FLIP) vpo[i] += wyz * So[i];
+      }
+    }
+  return true;
+}
+
+// Everything of mpm_g2p.comp after the gather (lines 120-271): material,
+// F update, return map, stress, J reset, transfer, advection, SDF push-out,
+// world clamp, write-back.  Returns event bits (1 J reset, 2 SDF push-out).
+__device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s, float dt, const float vpic[3], const float vpo[3],
+                                              const float G[3][3], float Bn[3][3]) {
+  const float h = P.cellSize;
+  const float xp[3] = {s.P.x, s.P.y, s.P.z};
+  const bool flip = P.flip_ratio > 0.01f;
   const MatSample mat = fetchMaterial(P, __float_as_uint(s.v.w));
   // F_new = (I + dt grad v) F
   m3<float> F, A;
@@ -351,6 +431,14 @@ __device__ __forceinline__ uint32_t g2pParticle(const SubstepParams& P, PState& 
   s.B1 = make_float4(Bn[1][0], Bn[1][1], Bn[1][2], tau.m[0][2]);
   s.B2 = make_float4(Bn[2][0], Bn[2][1], Bn[2][2], tau.m[1][2]);
   return events;
+}
+
+// grid.node(nx, ny, nz, mass, vel, vold) returns false for nodes to skip.
+template <class Grid>
+__device__ __forceinline__ uint32_t g2pParticle(const SubstepParams& P, PState& s, const Grid& grid, float dt) {
+  float vpic[3], vpo[3], G[3][3], Bn[3][3];
+  g2pGather(P, s, grid, vpic, vpo, G, Bn);
+  return g2pUpdate(P, s, dt, vpic, vpo, G, Bn);
 }
 
 }  // namespace nebula

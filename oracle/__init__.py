@@ -25,6 +25,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SRC = HERE / "mpm_oracle.cpp"
+SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp")
 LIB = HERE / "libmpm_oracle.so"
 
 MODES = {"ref32": 0, "mixed": 1, "fp64": 2}
@@ -55,11 +56,11 @@ class orc_params(C.Structure):
 
 def build(force: bool = False) -> Path:
     """Compile the oracle into ``oracle/libmpm_oracle.so`` (g++, OpenMP)."""
-    if LIB.exists() and not force and LIB.stat().st_mtime >= SRC.stat().st_mtime:
+    if LIB.exists() and not force and all(LIB.stat().st_mtime >= s.stat().st_mtime for s in SRCS):
         return LIB
     tmp = LIB.with_suffix(".so.tmp%d" % os.getpid())
     cmd = ["g++", "-O2", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-fPIC", "-shared",
-           "-o", str(tmp), str(SRC)]
+           "-o", str(tmp)] + [str(s) for s in SRCS]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
@@ -106,6 +107,14 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = None
+        L.adj_grad.restype = C.c_int
+        L.adj_grad.argtypes = [vp, vp, C.c_size_t] + [vp] * 7 + [C.c_int, C.c_int] + [vp] * 6
+        L.adj_loss.restype = C.c_int
+        L.adj_loss.argtypes = [vp, vp, C.c_size_t] + [vp] * 7 + [C.c_int, vp, vp]
+        L.adj_hencky.restype = None
+        L.adj_hencky.argtypes = [vp, C.c_double, C.c_double, vp]
+        L.adj_hencky_vjp.restype = None
+        L.adj_hencky_vjp.argtypes = [vp, C.c_double, C.c_double, vp, vp, vp, vp]
         L.orc_num_threads.restype = C.c_int
         L.orc_bspline2.restype = C.c_float
         L.orc_bspline2.argtypes = [C.c_float]
@@ -299,3 +308,56 @@ def project(F_glsl: np.ndarray, model: int, mu, lam, M=0.0, qc=0.0, qmax=0.0) ->
     out = np.empty(9)
     lib().orc_project(_ptr(f), model, mu, lam, M, qc, qmax, _ptr(out))
     return out.reshape(3, 3)
+
+
+# ----------------------------------------------------------------------------- adjoint (float64)
+EVENT_NAMES = {1: "grid speed cap", 2: "J reset", 4: "world clamp", 8: "particle left the grid interior"}
+
+
+def _adj_args(params, res, x0, v0, Vp, rho, mu, lam, target):
+    prm = np.array([params["dt"], params["h"], *params["g"]], np.float64)
+    r = np.array(res, np.int32)
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (x0, v0, Vp, rho, mu, lam, target)]
+    return prm, r, arrs
+
+
+def adjoint_grad(params, res, x0, v0, Vp, rho, mu, lam, target, nsub, every=20):
+    """Reverse-mode gradient of |COM(x_T) - target|^2 w.r.t. v0 and per-particle
+    (mu, lambda), float64, with checkpoints every `every` substeps."""
+    prm, r, arrs = _adj_args(params, res, x0, v0, Vp, rho, mu, lam, target)
+    n = arrs[2].size
+    loss = np.zeros(1)
+    gv = np.zeros(3 * n)
+    gmu = np.zeros(n)
+    glam = np.zeros(n)
+    xT = np.zeros(3 * n)
+    ev = np.zeros(1, np.uint32)
+    lib().adj_grad(_ptr(prm), _ptr(r), n, *[_ptr(a) for a in arrs], int(nsub), int(every), _ptr(loss), _ptr(gv), _ptr(gmu),
+                   _ptr(glam), _ptr(xT), _ptr(ev))
+    return {"loss": float(loss[0]), "gv0": gv.reshape(n, 3), "gmu": gmu, "glam": glam, "xT": xT.reshape(n, 3), "events": int(ev[0])}
+
+
+def adjoint_loss(params, res, x0, v0, Vp, rho, mu, lam, target, nsub):
+    prm, r, arrs = _adj_args(params, res, x0, v0, Vp, rho, mu, lam, target)
+    n = arrs[2].size
+    loss = np.zeros(1)
+    ev = np.zeros(1, np.uint32)
+    lib().adj_loss(_ptr(prm), _ptr(r), n, *[_ptr(a) for a in arrs], int(nsub), _ptr(loss), _ptr(ev))
+    return float(loss[0]), int(ev[0])
+
+
+def hencky_ref64(F, mu, lam):
+    f = np.ascontiguousarray(F, np.float64).reshape(9)
+    t = np.zeros(9)
+    lib().adj_hencky(_ptr(f), mu, lam, _ptr(t))
+    return t.reshape(3, 3)
+
+
+def hencky_ref64_vjp(F, mu, lam, tbar):
+    f = np.ascontiguousarray(F, np.float64).reshape(9)
+    tb = np.ascontiguousarray(tbar, np.float64).reshape(9)
+    fb = np.zeros(9)
+    mb = np.zeros(1)
+    lb = np.zeros(1)
+    lib().adj_hencky_vjp(_ptr(f), mu, lam, _ptr(tb), _ptr(fb), _ptr(mb), _ptr(lb))
+    return fb.reshape(3, 3), float(mb[0]), float(lb[0])
