@@ -241,6 +241,21 @@ typedef struct nebula_mpm_particles {
 size_t nebula_mpm_bin_workspace_size(uint32_t hashCells, uint32_t particleCount);
 int nebula_mpm_bin(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSorted,
                    void* dWorkspace, size_t workspaceBytes, void* stream);
+/* Same outputs as nebula_mpm_bin, for callers that cannot provide or allocate a
+ * workspace: the scratch is a fixed file-scope device array inside the library
+ * (hashCells <= nebula_mpm_bin_noalloc_max_cells() = 2^21, i.e. 128^3, and
+ * particleCount <= nebula_mpm_bin_noalloc_max_particles() = 2^18; larger
+ * sizes return NEBULA_MPM_ERR_INVALID).  No device memory is allocated.  The
+ * first call on each device (with that device current) looks up the array's
+ * address; make it before any stream capture.  Every call clears what it
+ * needs on the stream.  Calls on one device share the scratch, so calls that
+ * can overlap in time must be ordered by the caller.  This entry point has no
+ * counterpart in the reference: its binning (mpm_hash_count.comp,
+ * hash_scan_*.comp, mpm_hash_sort.comp) runs on engine-owned buffers only. */
+size_t nebula_mpm_bin_noalloc_max_cells(void);
+size_t nebula_mpm_bin_noalloc_max_particles(void);
+int nebula_mpm_bin_noalloc(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSorted,
+                           void* stream);
 /* mpm_zero_grid.comp + mpm_p2g.comp: writes gridMom[0, hashCells) (w = 0) and
  * gridMass; clears gridMom[hashCells, 2 hashCells). */
 int nebula_mpm_p2g(const nebula_mpm_pass* pass, const nebula_mpm_particles* parts, const uint32_t* dCellCount, const uint32_t* dCellOffset,
