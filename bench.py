@@ -20,6 +20,7 @@ import json
 import os
 import subprocess
 import sys
+import threading
 import time
 from pathlib import Path
 
@@ -35,7 +36,7 @@ UNIT = "particle-substeps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nebula", choices=["nebula", "reference"])
     ap.add_argument("--workload", default="slope", choices=["slope", "elastic", "multimaterial"])
@@ -65,17 +66,58 @@ def peaks():
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    """SM clock and throttle-reason sampling during the timed region.
+
+    Polls NVML every 5 ms from a thread on the device the bench runs on
+    (matched by UUID); falls back to ``nvidia-smi -lms 200`` when NVML is not
+    importable.  Read-only: no clock or power setting is touched."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.sm, self.smax, self.reasons = [], [], set()
         self.path = Path("/tmp/nebula_clocks_%d_%d.csv" % (os.getpid(), index))
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            nv = None
+        if nv is not None:
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown, "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown, "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.stop_flag = threading.Event()
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        self.smax.append(float(smax))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.reasons.update(k for k, b in bits.items() if r & b)
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
@@ -83,33 +125,38 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            src = "nvml"
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        try:
-            self.path.unlink()
-        except OSError:
-            pass
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.sm.append(float(parts[1]))
+                    self.smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(self.NAMES, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        self.reasons.add(nm)
+            try:
+                self.path.unlink()
+            except OSError:
+                pass
+            src = "nvidia-smi"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no NVML or nvidia-smi"]}
+        sm = self.sm
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(self.smax) if self.smax else None,
+                "sm_min_mhz": min(sm) if sm else None, "reasons": sorted(self.reasons), "samples": len(sm), "source": src}
 
 
 # ----------------------------------------------------------------------------- algorithmic bytes
