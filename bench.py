@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--pipeline", default="fused", choices=["fused", "dense"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-substeps", type=int, default=0, help="oracle substeps timed for cpu_baseline (0 = auto)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement on the 64-scene mix")
+    ap.add_argument("--batch-steps", type=int, default=5, help="timed steps of the batched / plain comparison")
     return ap.parse_args()
 
 
@@ -228,6 +230,76 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- batched vs plain
+def measure_batch(steps: int, warmup: int, substeps: int) -> dict:
+    """The 64-scene mix advanced by the batched engine (one set of launches
+    per substep, replayed from a CUDA graph) and by 64 single-scene engines
+    stepped one after another, on the same stream, with each scene's moving
+    sphere re-uploaded as a collider track before every step in both forms."""
+    import torch
+
+    from nebula_b200 import scenes as S
+    from nebula_b200.batch import batch_for_scenes
+    from nebula_b200.engine import engine_for_scene
+
+    scenes = S.batch_mix()
+    n = sum(sc.n for sc in scenes)
+    dt = scenes[0].params.dt
+    frames = warmup + steps
+    tracks = [[S.collider_track(sc, substeps, k * substeps) for k in range(frames)] for sc in scenes]
+    stream = torch.cuda.Stream()
+
+    def timed(step_fn):
+        for k in range(warmup):
+            step_fn(k)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(warmup, frames):
+            step_fn(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    b, ids = batch_for_scenes(scenes)
+
+    def batch_step(k):
+        for i, s in enumerate(ids):
+            b.set_collider_track(s, tracks[i][k])
+        b.step(dt * substeps, substeps, stream)
+
+    st0 = b.stats()
+    ms_b = timed(batch_step)
+    b.sync()
+    st1 = b.stats()
+    launches_b = int(st1["kernel_launches"] - st0["kernel_launches"])
+    b.cleanup()
+
+    engines = [engine_for_scene(sc) for sc in scenes]
+    for e in engines:
+        e.numSubsteps = substeps
+
+    def plain_step(k):
+        for i, e in enumerate(engines):
+            e.setColliderTrack(tracks[i][k])
+            e.step(dt * substeps, stream)
+
+    l0 = sum(e.stats()["kernel_launches"] for e in engines)
+    ms_p = timed(plain_step)
+    for e in engines:
+        e.sync()
+    launches_p = int(sum(e.stats()["kernel_launches"] for e in engines) - l0)
+    for e in engines:
+        e.cleanup()
+    ps = float(n) * substeps * steps
+    return {"workload": "batch_mix_64", "scenes": len(scenes), "particles": n, "substeps_per_step": substeps, "steps": steps,
+            "warmup": warmup, "dt": dt, "value": ps / (ms_b * 1e-3), "ms_per_step": ms_b / steps, "plain_value": ps / (ms_p * 1e-3),
+            "plain_ms_per_step": ms_p / steps, "speedup": ms_p / ms_b, "unit": UNIT, "gpu_launches": launches_b,
+            "plain_gpu_launches": launches_p,
+            "note": "batched: one grid update + one fused G2P/P2G + scan + permutation per substep over all scenes, graph "
+                    "replay; plain: the same kernels per scene, 64 engines in sequence"}
+
+
 # ----------------------------------------------------------------------------- nebula arm
 def main():
     args = parse()
@@ -388,9 +460,11 @@ def main():
         cdt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": n * k / cdt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
                                 "sample": "%d substeps of %s (after one untimed), CPU oracle ref32 mode, OpenMP" % (k, sc.name)}
+    eng.cleanup()
+    if not args.no_batch:
+        line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.cleanup()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

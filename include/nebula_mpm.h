@@ -202,6 +202,79 @@ int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
  * brickStarts hold hashCells/64 (+1) entries, sortedPids live entries.  Host arrays. */
 int nebula_mpm_export_brick_bins(nebula_mpm* e, uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids);
 
+/* ---------------------------------------------------------------- batched scenes
+ * No counterpart in the reference (one MPMEngine holds one scene).  A batch
+ * holds many independent scenes, each with the engine's parameter surface,
+ * and advances all of them with one set of launches per substep: scenes share
+ * one brick space and one particle array, and a step of K substeps is
+ * replayed from a CUDA graph captured on first use (when `stream` is not
+ * NULL).  Scenes are added before the first step; the layout is fixed after
+ * it.  Substep k of a step uses collider set min(k, trackLen-1) of each
+ * scene's collider track, which is how a host moves a collider every
+ * substep (the reference re-uploads ColliderSet between dispatches). */
+typedef struct nebula_mpm_batch nebula_mpm_batch;
+typedef struct nebula_mpm_batch_config {
+  uint32_t maxScenes;     /* scene table capacity (<= 65536) */
+  uint32_t maxParticles;  /* particle capacity over all scenes */
+} nebula_mpm_batch_config;
+typedef struct nebula_mpm_scene_info {
+  uint32_t grid_res[3];
+  uint32_t cube_res;
+  uint32_t hash_cells;
+  uint32_t particles;
+  uint32_t first_brick;   /* the scene's bricks in the shared brick space */
+  uint32_t bricks;
+} nebula_mpm_scene_info;
+typedef struct nebula_mpm_batch_stats {
+  uint64_t substeps;
+  uint32_t scenes;
+  uint32_t live_particles;
+  uint32_t total_bricks;
+  uint32_t active_bricks;     /* grid bricks touched by the last P2G, all scenes */
+  uint32_t particle_bricks;   /* bricks holding particles at the last binning */
+  uint32_t overflow_particles;
+  uint64_t kernel_launches;   /* kernels launched, graph replays included */
+  uint64_t graph_launches;
+  uint32_t error_flags;
+} nebula_mpm_batch_stats;
+
+int nebula_mpm_batch_create(const nebula_mpm_batch_config* cfg, nebula_mpm_batch** out);
+int nebula_mpm_batch_destroy(nebula_mpm_batch* b);
+/* Adds a scene with domain, cell size, E, nu, rho0 from `cfg` (nx, ny, nz and
+ * maxParticles are ignored) and n particles pos4=(x,Vp), vel4=(v, id bits),
+ * F=I, B=0 (MPMEngine::appendParticles semantics).  *scene receives its index. */
+int nebula_mpm_batch_add_scene(nebula_mpm_batch* b, const nebula_mpm_config* cfg, const float* pos4, const float* vel4, uint32_t n,
+                               uint32_t* scene);
+/* Per-scene forms of the engine setters above (numSubsteps is ignored: the
+ * batch step takes its own count). */
+int nebula_mpm_batch_set_params(nebula_mpm_batch* b, uint32_t scene, const nebula_mpm_params* p);
+int nebula_mpm_batch_get_params(const nebula_mpm_batch* b, uint32_t scene, nebula_mpm_params* p);
+int nebula_mpm_batch_set_materials(nebula_mpm_batch* b, uint32_t scene, const nebula_mpm_material* mats, uint32_t n);
+int nebula_mpm_batch_set_particle_material_ids(nebula_mpm_batch* b, uint32_t scene, const uint32_t* ids, uint32_t n);
+int nebula_mpm_batch_set_colliders(nebula_mpm_batch* b, uint32_t scene, const nebula_mpm_collider* c, uint32_t n);
+/* substeps consecutive sets of perSubstep colliders (perSubstep <= 64). */
+int nebula_mpm_batch_set_collider_track(nebula_mpm_batch* b, uint32_t scene, const nebula_mpm_collider* c, uint32_t perSubstep,
+                                        uint32_t substeps);
+int nebula_mpm_batch_set_collider_sdf(nebula_mpm_batch* b, uint32_t scene, const float* morton_sdf, uint64_t n);
+int nebula_mpm_batch_clear_collider_sdf(nebula_mpm_batch* b, uint32_t scene);
+int nebula_mpm_batch_set_forces(nebula_mpm_batch* b, uint32_t scene, const nebula_mpm_force* f, uint32_t n);
+/* Replace the scene's full state (n must equal its particle count). */
+int nebula_mpm_batch_upload_state(nebula_mpm_batch* b, uint32_t scene, const float* const fields[8], uint32_t n);
+/* Field `field` of the scene's particles in their original order (count = 4 * particles). */
+int nebula_mpm_batch_download(nebula_mpm_batch* b, uint32_t scene, int field, float* host, uint64_t count);
+/* `substeps` substeps of dt/substeps for every scene, stream-ordered. */
+int nebula_mpm_batch_step(nebula_mpm_batch* b, float dt, uint32_t substeps, void* stream);
+/* Graph capture and replay of steps (default on); off launches eagerly. */
+int nebula_mpm_batch_set_graphs(nebula_mpm_batch* b, int enable);
+int nebula_mpm_batch_sync(nebula_mpm_batch* b);
+int nebula_mpm_batch_get_stats(nebula_mpm_batch* b, nebula_mpm_batch_stats* s);
+int nebula_mpm_batch_scene_info(const nebula_mpm_batch* b, uint32_t scene, nebula_mpm_scene_info* info);
+
+/* Collider track of the single-scene engine: substep k of each later step
+ * uses collider set min(k, substeps-1) (same semantics as the batch call);
+ * nebula_mpm_set_colliders resets it to one set. */
+int nebula_mpm_set_collider_track(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t perSubstep, uint32_t substeps);
+
 /* Domain helpers (src/core/Domain.h:14-39). */
 void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint32_t out[3]);
 uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]);

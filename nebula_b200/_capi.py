@@ -48,6 +48,21 @@ class Particles(C.Structure):
     _fields_ = [("f", C.c_void_p * 8)]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("maxScenes", C.c_uint32), ("maxParticles", C.c_uint32)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("grid_res", C.c_uint32 * 3), ("cube_res", C.c_uint32), ("hash_cells", C.c_uint32), ("particles", C.c_uint32),
+                ("first_brick", C.c_uint32), ("bricks", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("substeps", C.c_uint64), ("scenes", C.c_uint32), ("live_particles", C.c_uint32), ("total_bricks", C.c_uint32),
+                ("active_bricks", C.c_uint32), ("particle_bricks", C.c_uint32), ("overflow_particles", C.c_uint32),
+                ("kernel_launches", C.c_uint64), ("graph_launches", C.c_uint64), ("error_flags", C.c_uint32)]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -79,6 +94,26 @@ _SIGS = {
     "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "nebula_mpm_export_grid": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_set_collider_track": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "nebula_mpm_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(C.c_void_p)]),
+    "nebula_mpm_batch_destroy": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_batch_add_scene": (C.c_int, [C.c_void_p, C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "nebula_mpm_batch_set_params": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Params)]),
+    "nebula_mpm_batch_get_params": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(Params)]),
+    "nebula_mpm_batch_set_materials": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "nebula_mpm_batch_set_particle_material_ids": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "nebula_mpm_batch_set_colliders": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "nebula_mpm_batch_set_collider_track": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]),
+    "nebula_mpm_batch_set_collider_sdf": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_batch_clear_collider_sdf": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "nebula_mpm_batch_set_forces": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "nebula_mpm_batch_upload_state": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p * 8, C.c_uint32]),
+    "nebula_mpm_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_batch_step": (C.c_int, [C.c_void_p, C.c_float, C.c_uint32, C.c_void_p]),
+    "nebula_mpm_batch_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_batch_sync": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
+    "nebula_mpm_batch_scene_info": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(SceneInfo)]),
     "nebula_mpm_domain_grid_res": (None, [C.c_float * 3, C.c_float, C.c_uint32 * 3]),
     "nebula_mpm_domain_cube_res": (C.c_uint32, [C.c_uint32 * 3]),
     "nebula_mpm_domain_hash_cells": (C.c_uint32, [C.c_uint32 * 3]),

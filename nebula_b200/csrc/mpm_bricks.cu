@@ -47,19 +47,56 @@ __device__ __forceinline__ void markStencilBricks(const SubstepParams& P, int cx
       for (int bx = x0; bx <= x1; ++bx) flag[mortonEncode(bx, by, bz)] = 1u;
 }
 
+// ------------------------------------------------------------------ batch scenes
+// The scene s with base[s] <= x < base[s+1] (base non-decreasing, x < base[count]).
+__device__ __forceinline__ uint32_t findScene(const uint32_t* __restrict__ base, uint32_t count, uint32_t x) {
+  uint32_t lo = 0, hi = count;
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+static_assert(sizeof(SubstepParams) % 4 == 0, "SubstepParams is copied as 32-bit words");
+constexpr int kParamWords = int(sizeof(SubstepParams) / 4);
+
+// Word copy of one scene's parameters by threads t = 0..nthreads-1.
+__device__ __forceinline__ void copyParams(SubstepParams* dst, const SubstepParams* src, int t, int nthreads) {
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  for (int q = t; q < kParamWords; q += nthreads) d[q] = a[q];
+}
+
+__device__ __forceinline__ GridBuffers offsetGrid(const GridBuffers& G, uint32_t brickBase) {
+  const size_t c = size_t(brickBase) << 6;
+  return GridBuffers{G.acc + c, G.vel + c, G.vold ? G.vold + c : nullptr};
+}
+
 // ------------------------------------------------------------------ binning count (standalone)
-__global__ void __launch_bounds__(kThreads) k_brick_count(SubstepParams P, const float4* __restrict__ pos, uint32_t n, BrickBuffers B) {
+template <bool BATCH>
+__global__ void __launch_bounds__(kThreads) k_brick_count(SubstepParams P0, SceneTable T, const float4* __restrict__ pos, uint32_t n,
+                                                          BrickBuffers B) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < n;
   const uint32_t mask = __ballot_sync(0xffffffffu, act);
   if (!act) return;
   const float4 p = pos[i];
-  int cx, cy, cz;
-  cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
-  const uint32_t b = mortonEncode(cx, cy, cz) >> 6;
-  B.binKey[i] = b;
-  B.binRank[i] = warpAggInc(mask, B.brickCount, b);
-  markStencilBricks(P, cx, cy, cz, B.brickFlag);
+  auto body = [&](const SubstepParams& P, uint32_t base) {
+    int cx, cy, cz;
+    cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
+    const uint32_t b = base + (mortonEncode(cx, cy, cz) >> 6);
+    B.binKey[i] = b;
+    B.binRank[i] = warpAggInc(mask, B.brickCount, b);
+    markStencilBricks(P, cx, cy, cz, B.brickFlag + base);
+  };
+  if constexpr (BATCH) {
+    const uint32_t sc = findScene(T.partBase, T.count, i);
+    body(T.params[sc], T.brickBase[sc]);
+  } else {
+    body(P0, 0u);
+  }
 }
 
 // ------------------------------------------------------------------ compaction scan
@@ -455,8 +492,37 @@ __device__ __forceinline__ int cellSlot(int cx, int cy, int cz, int ox, int oy, 
 }
 
 // ------------------------------------------------------------------ P2G over particle bricks (standalone)
-__global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P, StatePtrs cur, uint32_t n, BrickBuffers B, GridBuffers G,
-                                                         float dtStress) {
+// P2G of the particles in sorted slots [start, end) of brick `b` (the scene's own brick id).
+__device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, P2GSmem& sm, uint32_t b, uint32_t start, uint32_t end, StatePtrs cur,
+                                             uint32_t n, const BrickBuffers& B, const GridBuffers& G, float dtStress) {
+  int bx, by, bz;
+  mortonDecode(b, bx, by, bz);
+  const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
+  for (uint32_t base = start; base < end; base += kChunk) {
+    const uint32_t t = base + threadIdx.x;
+    int key = -1;
+    uint32_t rank = 0;
+    if (t < end) {
+      const uint32_t s = B.perm[t];
+      if (s < n) {
+        const PState st = loadState(cur.f, s);
+        int cx, cy, cz;
+        cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
+        float4* row = sm.rows + threadIdx.x * kRow;
+        p2gRow(P, st, dtStress, cx, cy, cz, row);
+        key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
+        if (key >= 0) rank = atomicAdd(&sm.cellCount[key], 1u);
+        else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+      }
+    }
+    p2gChunk(P, sm, key, rank, tx, ty, tz);
+  }
+  p2gFlush(P, sm, tx, ty, tz, G.acc);
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P0, SceneTable T, StatePtrs cur, uint32_t n, BrickBuffers B,
+                                                         GridBuffers G, float dtStress) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
   const uint32_t numPB = B.counters[kCntNumPB];
@@ -467,29 +533,19 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P, StateP
     const uint32_t i = sm.item;
     if (i >= numPB) break;
     const uint32_t b = B.pbBrick[i], end = min(B.pbStart[i + 1], n), start = min(B.pbStart[i], end);
-    int bx, by, bz;
-    mortonDecode(b, bx, by, bz);
-    const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
-    for (uint32_t base = start; base < end; base += kChunk) {
-      const uint32_t t = base + threadIdx.x;
-      int key = -1;
-      uint32_t rank = 0;
-      if (t < end) {
-        const uint32_t s = B.perm[t];
-        if (s < n) {
-          const PState st = loadState(cur.f, s);
-          int cx, cy, cz;
-          cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
-          float4* row = sm.rows + threadIdx.x * kRow;
-          p2gRow(P, st, dtStress, cx, cy, cz, row);
-          key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
-          if (key >= 0) rank = atomicAdd(&sm.cellCount[key], 1u);
-          else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
-        }
+    if constexpr (BATCH) {
+      __shared__ SubstepParams sP;
+      __shared__ uint32_t sBase;
+      if (threadIdx.x < 32) {
+        const uint32_t sc = findScene(T.brickBase, T.count, b);
+        copyParams(&sP, T.params + sc, threadIdx.x, 32);
+        if (threadIdx.x == 0) sBase = T.brickBase[sc];
       }
-      p2gChunk(P, sm, key, rank, tx, ty, tz);
+      __syncthreads();
+      p2gBrickItem(sP, sm, b - sBase, start, end, cur, n, B, offsetGrid(G, sBase), sP.dt);
+    } else {
+      p2gBrickItem(P0, sm, b, start, end, cur, n, B, G, dtStress);
     }
-    p2gFlush(P, sm, tx, ty, tz, G.acc);
     __syncthreads();
   }
 }
@@ -511,6 +567,40 @@ __global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, Brick
   }
 }
 
+// Batched grid update: one warp per listed grid brick, two nodes per lane, the
+// brick's scene parameters in a warp-private shared copy.
+__global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, uint32_t substep, BrickBuffers B, GridBuffers G) {
+  __shared__ SubstepParams sP[kThreads / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t numGB = B.counters[kCntNumGB];
+  for (uint32_t gb = blockIdx.x * (kThreads / 32) + warp; gb < numGB; gb += gridDim.x * (kThreads / 32)) {
+    const uint32_t bg = B.gbBrick[gb];
+    const uint32_t sc = findScene(T.brickBase, T.count, bg);
+    const uint32_t base = T.brickBase[sc];
+    __syncwarp();
+    copyParams(&sP[warp], T.params + sc, lane, 32);
+    __syncwarp();
+    if (lane == 0) sP[warp].colliders += size_t(substep) * sP[warp].colliderCount;
+    __syncwarp();
+    const SubstepParams& P = sP[warp];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t sub = uint32_t(lane + 32 * h);
+      const uint32_t local = ((bg - base) << 6) | sub;
+      if (local >= P.hashCells) continue;
+      const size_t code = (size_t(bg) << 6) | sub;
+      const float4 a = G.acc[code];
+      G.acc[code] = make_float4(0.f, 0.f, 0.f, 0.f);
+      int ix, iy, iz;
+      mortonDecode(local, ix, iy, iz);
+      float3 v, vo;
+      const bool ok = gridNode(P, ix, iy, iz, a.w, a.x, a.y, a.z, v, vo);
+      G.vel[code] = ok ? make_float4(v.x, v.y, v.z, a.w) : make_float4(0.f, 0.f, 0.f, a.w);
+      if (G.vold) G.vold[code] = ok ? make_float4(vo.x, vo.y, vo.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridBuffers G) {
   const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
   for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
@@ -520,10 +610,85 @@ __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridB
 }
 
 // ------------------------------------------------------------------ fused G2P -> update -> P2G
+// One particle brick: G2P of the particles in sorted slots [start, end) of
+// brick `b` (the scene's own brick id) from the staged grid, particle update,
+// binning count under the global brick key brickBase + (Morton >> 6), and P2G
+// of the updated particles.
 template <bool FLIP>
-__global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
-                                                    uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G, float dtStress,
-                                                    uint32_t* err) {
+__device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP>& S, uint32_t b, uint32_t start, uint32_t end,
+                                          uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
+                                          uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B, const GridBuffers& G,
+                                          float dtStress, uint32_t* err) {
+  P2GSmem& sm = S.p2g;
+  int bx, by, bz;
+  mortonDecode(b, bx, by, bz);
+  // stage the 6^3 nodes [4b-1, 4b+4]^3 (nodes outside [0, gridRes) read as empty)
+  const int sx = 4 * bx - 1, sy = 4 * by - 1, sz = 4 * bz - 1;
+  for (int q = threadIdx.x; q < 216; q += blockDim.x) {
+    const int x = sx + q % 6, y = sy + (q / 6) % 6, z = sz + q / 36;
+    const bool valid = x >= 0 && y >= 0 && z >= 0 && x < P.gridRes[0] && y < P.gridRes[1] && z < P.gridRes[2];
+    const uint32_t c = valid ? mortonEncode(x, y, z) : 0u;
+    float4 v = valid ? G.vel[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool live = v.w >= 1e-10f;  // the nodes the shader gathers from
+    if (!live) v = make_float4(0.f, 0.f, 0.f, v.w);
+    S.v[q] = v;
+    if (FLIP) S.vo[q] = live ? G.vold[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
+  const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
+  for (uint32_t base = start; base < end; base += kChunk) {
+    const uint32_t t = base + threadIdx.x;
+    const bool act = t < end;
+    const uint32_t mask = __ballot_sync(0xffffffffu, act);
+    int key = -1;
+    uint32_t rank = 0;
+    if (act) {
+      const uint32_t s = B.perm[t];
+      const bool valid = s < n;
+      PState st;
+      int cx = 0, cy = 0, cz = 0;
+      uint32_t nb = 0;
+      if (valid) {
+        st = loadState(cur.f, s);
+        const uint32_t pid = pidCur[s];
+        float vpic[3], vpo[3], Gv[3][3], Bn[3][3];
+        if (!g2pGatherStaged<FLIP>(P, st, S.v, S.vo, sx, sy, sz, vpic, vpo, Gv, Bn)) gatherFallback<FLIP>(P, st, grid, vpic, vpo, Gv, Bn);
+        g2pUpdate(P, st, P.dt, vpic, vpo, Gv, Bn);
+        storeState(nxt.f, t, st);
+        pidNxt[t] = pid;
+        if (!(isfinite(st.P.x) && isfinite(st.P.y) && isfinite(st.P.z))) atomicOr(err, kErrNonFinite);
+        cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
+        nb = brickBase + (mortonEncode(cx, cy, cz) >> 6);
+      } else {
+        atomicOr(err, kErrBinRange);  // a slot that maps nowhere: only after an expired scan wait
+      }
+      // every active lane reaches this one call site
+      const uint32_t r = warpAggInc(mask, B.brickCount, nb);
+      B.binKey[t] = nb;
+      B.binRank[t] = r;
+      if (valid) {
+        markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
+        float4* row = sm.rows + threadIdx.x * kRow;
+        p2gRow(P, st, dtStress, cx, cy, cz, row);
+        key = cellSlot(cx, cy, cz, sx, sy, sz);
+        if (key >= 0) {
+          rank = atomicAdd(&sm.cellCount[key], 1u);
+        } else {
+          p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+          atomicAdd(B.counters + kCntOverflow, 1u);
+        }
+      }
+    }
+    p2gChunk(P, sm, key, rank, tx, ty, tz);
+  }
+  p2gFlush(P, sm, tx, ty, tz, G.acc);
+}
+
+template <bool FLIP, bool BATCH>
+__global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
+                                                    StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G,
+                                                    float dtStress, uint32_t* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   G2P2GSmem<FLIP>& S = *reinterpret_cast<G2P2GSmem<FLIP>*>(smem_raw);
   P2GSmem& sm = S.p2g;
@@ -535,69 +700,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_g2p2g(SubstepParams P, StatePtr
     const uint32_t i = sm.item;
     if (i >= numPB) break;
     const uint32_t b = B.pbBrick[i], end = min(B.pbStart[i + 1], n), start = min(B.pbStart[i], end);
-    int bx, by, bz;
-    mortonDecode(b, bx, by, bz);
-    // stage the 6^3 nodes [4b-1, 4b+4]^3 (nodes outside [0, gridRes) read as empty)
-    const int sx = 4 * bx - 1, sy = 4 * by - 1, sz = 4 * bz - 1;
-    for (int q = threadIdx.x; q < 216; q += blockDim.x) {
-      const int x = sx + q % 6, y = sy + (q / 6) % 6, z = sz + q / 36;
-      const bool valid = x >= 0 && y >= 0 && z >= 0 && x < P.gridRes[0] && y < P.gridRes[1] && z < P.gridRes[2];
-      const uint32_t c = valid ? mortonEncode(x, y, z) : 0u;
-      float4 v = valid ? G.vel[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const bool live = v.w >= 1e-10f;  // the nodes the shader gathers from
-      if (!live) v = make_float4(0.f, 0.f, 0.f, v.w);
-      S.v[q] = v;
-      if (FLIP) S.vo[q] = live ? G.vold[c] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    __syncthreads();
-    const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
-    const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
-    for (uint32_t base = start; base < end; base += kChunk) {
-      const uint32_t t = base + threadIdx.x;
-      const bool act = t < end;
-      const uint32_t mask = __ballot_sync(0xffffffffu, act);
-      int key = -1;
-      uint32_t rank = 0;
-      if (act) {
-        const uint32_t s = B.perm[t];
-        const bool valid = s < n;
-        PState st;
-        int cx = 0, cy = 0, cz = 0;
-        uint32_t nb = 0;
-        if (valid) {
-          st = loadState(cur.f, s);
-          const uint32_t pid = pidCur[s];
-          float vpic[3], vpo[3], Gv[3][3], Bn[3][3];
-          if (!g2pGatherStaged<FLIP>(P, st, S.v, S.vo, sx, sy, sz, vpic, vpo, Gv, Bn)) gatherFallback<FLIP>(P, st, grid, vpic, vpo, Gv, Bn);
-          g2pUpdate(P, st, P.dt, vpic, vpo, Gv, Bn);
-          storeState(nxt.f, t, st);
-          pidNxt[t] = pid;
-          if (!(isfinite(st.P.x) && isfinite(st.P.y) && isfinite(st.P.z))) atomicOr(err, kErrNonFinite);
-          cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
-          nb = mortonEncode(cx, cy, cz) >> 6;
-        } else {
-          atomicOr(err, kErrBinRange);  // a slot that maps nowhere: only after an expired scan wait
-        }
-        // every active lane reaches this one call site
-        const uint32_t r = warpAggInc(mask, B.brickCount, nb);
-        B.binKey[t] = nb;
-        B.binRank[t] = r;
-        if (valid) {
-          markStencilBricks(P, cx, cy, cz, B.brickFlag);
-          float4* row = sm.rows + threadIdx.x * kRow;
-          p2gRow(P, st, dtStress, cx, cy, cz, row);
-          key = cellSlot(cx, cy, cz, sx, sy, sz);
-          if (key >= 0) {
-            rank = atomicAdd(&sm.cellCount[key], 1u);
-          } else {
-            p2gRowGlobal(P, row, cx, cy, cz, G.acc);
-            atomicAdd(B.counters + kCntOverflow, 1u);
-          }
-        }
+    if constexpr (BATCH) {
+      __shared__ SubstepParams sP;
+      __shared__ uint32_t sBase;
+      if (threadIdx.x < 32) {
+        const uint32_t sc = findScene(T.brickBase, T.count, b);
+        copyParams(&sP, T.params + sc, threadIdx.x, 32);
+        if (threadIdx.x == 0) sBase = T.brickBase[sc];
       }
-      p2gChunk(P, sm, key, rank, tx, ty, tz);
+      __syncthreads();
+      const uint32_t base = sBase;
+      g2p2gItem<FLIP>(sP, S, b - base, start, end, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
+    } else {
+      g2p2gItem<FLIP>(P0, S, b, start, end, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
     }
-    p2gFlush(P, sm, tx, ty, tz, G.acc);
     __syncthreads();
   }
 }
@@ -630,13 +746,52 @@ template <class K> int persistentBlocks(K kernel, int numSMs, size_t smem = 0) {
   return perSM * numSMs;
 }
 
+template <class K> int setupBigSmem(K kernel, size_t smem, int numSMs) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  return persistentBlocks(kernel, numSMs, smem);
+}
+
+// Persistent grid sizes of every kernel, resolved once (kernel attributes and
+// occupancy queries stay outside stream capture).
+struct LaunchShapes {
+  bool ready = false;
+  int p2g[2] = {0, 0};        // [BATCH]
+  int grid = 0, gridBatch = 0;
+  int fused[2][2] = {{0, 0}, {0, 0}};  // [FLIP][BATCH]
+};
+LaunchShapes g_shapes;
+
+const LaunchShapes& shapes(int numSMs) {
+  if (g_shapes.ready) return g_shapes;
+  LaunchShapes& L = g_shapes;
+  L.p2g[0] = setupBigSmem(k_p2g_bricks<false>, sizeof(P2GSmem), numSMs);
+  L.p2g[1] = setupBigSmem(k_p2g_bricks<true>, sizeof(P2GSmem), numSMs);
+  L.grid = persistentBlocks(k_grid_bricks, numSMs);
+  L.gridBatch = persistentBlocks(k_grid_bricks_batch, numSMs);
+  L.fused[0][0] = setupBigSmem(k_g2p2g<false, false>, sizeof(G2P2GSmem<false>), numSMs);
+  L.fused[0][1] = setupBigSmem(k_g2p2g<false, true>, sizeof(G2P2GSmem<false>), numSMs);
+  L.fused[1][0] = setupBigSmem(k_g2p2g<true, false>, sizeof(G2P2GSmem<true>), numSMs);
+  L.fused[1][1] = setupBigSmem(k_g2p2g<true, true>, sizeof(G2P2GSmem<true>), numSMs);
+  L.ready = true;
+  return L;
+}
+
 }  // namespace
+
+void prepareBrickKernels(int numSMs) { (void)shapes(numSMs); }
 
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches) {
   (void)err;
   if (n == 0) return cudaSuccess;
-  k_brick_count<<<blocksFor(n), kThreads, 0, s>>>(P, pos, n, b);
+  k_brick_count<false><<<blocksFor(n), kThreads, 0, s>>>(P, SceneTable{}, pos, n, b);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32_t n, const BrickBuffers& b, cudaStream_t s, uint64_t* launches) {
+  if (n == 0) return cudaSuccess;
+  k_brick_count<true><<<blocksFor(n), kThreads, 0, s>>>(SubstepParams{}, T, pos, n, b);
   ++*launches;
   return cudaGetLastError();
 }
@@ -654,25 +809,29 @@ cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, 
   return cudaGetLastError();
 }
 
-template <class K> int setupBigSmem(K kernel, size_t smem, int numSMs) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  return persistentBlocks(kernel, numSMs, smem);
-}
-
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
                             int numSMs, cudaStream_t s, uint64_t* launches) {
-  static int blocks = 0;
-  const size_t smem = sizeof(P2GSmem);
-  if (!blocks) blocks = setupBigSmem(k_p2g_bricks, smem, numSMs);
-  k_p2g_bricks<<<blocks, kThreads, smem, s>>>(P, cur, n, b, g, dtStress);
+  k_p2g_bricks<false><<<shapes(numSMs).p2g[0], kThreads, sizeof(P2GSmem), s>>>(P, SceneTable{}, cur, n, b, g, dtStress);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, int numSMs,
+                                 cudaStream_t s, uint64_t* launches) {
+  k_p2g_bricks<true><<<shapes(numSMs).p2g[1], kThreads, sizeof(P2GSmem), s>>>(SubstepParams{}, T, cur, n, b, g, 0.f);
   ++*launches;
   return cudaGetLastError();
 }
 
 cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches) {
-  static int blocks = 0;
-  if (!blocks) blocks = persistentBlocks(k_grid_bricks, numSMs);
-  k_grid_bricks<<<blocks, kThreads, 0, s>>>(P, b, g);
+  k_grid_bricks<<<shapes(numSMs).grid, kThreads, 0, s>>>(P, b, g);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s,
+                                  uint64_t* launches) {
+  k_grid_bricks_batch<<<shapes(numSMs).gridBatch, kThreads, 0, s>>>(T, substep, b, g);
   ++*launches;
   return cudaGetLastError();
 }
@@ -685,16 +844,26 @@ cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, 
 
 cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                         const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches) {
+  const LaunchShapes& L = shapes(numSMs);
   if (P.flip_ratio > 0.01f) {
-    static int blocks = 0;
-    const size_t smem = sizeof(G2P2GSmem<true>);
-    if (!blocks) blocks = setupBigSmem(k_g2p2g<true>, smem, numSMs);
-    k_g2p2g<true><<<blocks, kThreads, smem, s>>>(P, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+    k_g2p2g<true, false><<<L.fused[1][0], kThreads, sizeof(G2P2GSmem<true>), s>>>(P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress,
+                                                                                  err);
   } else {
-    static int blocks = 0;
-    const size_t smem = sizeof(G2P2GSmem<false>);
-    if (!blocks) blocks = setupBigSmem(k_g2p2g<false>, smem, numSMs);
-    k_g2p2g<false><<<blocks, kThreads, smem, s>>>(P, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+    k_g2p2g<false, false><<<L.fused[0][0], kThreads, sizeof(G2P2GSmem<false>), s>>>(P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g,
+                                                                                    dtStress, err);
+  }
+  ++*launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                             const BrickBuffers& b, GridBuffers g, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches) {
+  const LaunchShapes& L = shapes(numSMs);
+  if (flip) {
+    k_g2p2g<true, true><<<L.fused[1][1], kThreads, sizeof(G2P2GSmem<true>), s>>>(SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err);
+  } else {
+    k_g2p2g<false, true><<<L.fused[0][1], kThreads, sizeof(G2P2GSmem<false>), s>>>(SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f,
+                                                                                   err);
   }
   ++*launches;
   return cudaGetLastError();

@@ -42,6 +42,18 @@ struct BrickBuffers {
   uint32_t* perm;             // [cap] sorted slot -> buffer index
 };
 
+// The scenes of a batch share one brick space: scene s owns the global bricks
+// [brickBase[s], brickBase[s+1]) and the particle slots [partBase[s],
+// partBase[s+1]) of every brick-ordered buffer (a sort by global brick keeps
+// each scene's particles together).  Grid arrays are indexed by global cell
+// code = 64 * brickBase[s] + the scene's own Morton code.
+struct SceneTable {
+  const SubstepParams* params;  // [count] per-scene substep parameters
+  const uint32_t* brickBase;    // [count + 1]
+  const uint32_t* partBase;     // [count + 1]
+  uint32_t count;
+};
+
 struct GridBuffers {
   float4* acc;   // [ncPad] (mom.xyz, mass) accumulated by P2G
   float4* vel;   // [ncPad] (v.xyz, mass) after the grid update
@@ -64,6 +76,19 @@ cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, 
 // The fused G2P -> particle update -> P2G + binning count.
 cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                         const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches);
+// Batched forms: every scene of `T` in one launch.  `substep` selects the
+// colliders of this substep on each scene's collider track
+// (params.colliders + substep * params.colliderCount).
+cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32_t n, const BrickBuffers& b, cudaStream_t s, uint64_t* launches);
+cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, int numSMs,
+                                 cudaStream_t s, uint64_t* launches);
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s,
+                                  uint64_t* launches);
+cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                             const BrickBuffers& b, GridBuffers g, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches);
+// Resolve every launcher's one-time set-up (shared-memory limits, persistent
+// block counts) outside any stream capture.
+void prepareBrickKernels(int numSMs);
 // out[pid[i]] = in[i] for the 8 fields (original particle order).
 cudaError_t launchUnpermute(StatePtrs in, const uint32_t* pid, StatePtrs out, uint32_t n, cudaStream_t s, uint64_t* launches);
 cudaError_t launchIota(uint32_t* pid, uint32_t n, cudaStream_t s, uint64_t* launches);

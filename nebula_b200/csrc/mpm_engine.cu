@@ -277,7 +277,20 @@ void MPMEngine::setColliders(const nebula_mpm_collider* c, uint32_t n) {
   if (n && !c) throw Error(NEBULA_MPM_ERR_INVALID, "null colliders");
   prepareHostAccess(false);
   colliderCount_ = n;
+  colliderTrackLen_ = 1;
   if (n) check(cudaMemcpy(colliders_.ptr, c, n * sizeof(Collider), cudaMemcpyHostToDevice), "upload colliders");
+}
+
+void MPMEngine::setColliderTrack(const nebula_mpm_collider* c, uint32_t perSubstep, uint32_t substeps) {
+  if (perSubstep > uint32_t(kMaxColliders)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 64 colliders per substep");
+  if (substeps == 0) throw Error(NEBULA_MPM_ERR_INVALID, "a collider track needs at least one substep");
+  const size_t total = size_t(perSubstep) * substeps;
+  if (total && !c) throw Error(NEBULA_MPM_ERR_INVALID, "null colliders");
+  prepareHostAccess(false);
+  colliders_.ensure(std::max(total, size_t(kMaxColliders)) * sizeof(Collider));
+  colliderCount_ = perSubstep;
+  colliderTrackLen_ = substeps;
+  if (total) check(cudaMemcpy(colliders_.ptr, c, total * sizeof(Collider), cudaMemcpyHostToDevice), "upload collider track");
 }
 
 void MPMEngine::clearAnalyticColliders() { colliderCount_ = 0; }
@@ -585,17 +598,23 @@ void MPMEngine::step(float dt, cudaStream_t s) {
   const float subDt = dt / float(n);  // MPMEngine.cpp:413
   const SubstepParams P = buildParams(subDt);
   if (params_.numSubsteps <= 0 || live_ == 0) return;
+  // substep k reads collider set min(k, trackLen - 1) of the track
+  auto atSubstep = [&](int k) {
+    SubstepParams Pk = P;
+    Pk.colliders += size_t(std::min(uint32_t(k), colliderTrackLen_ - 1)) * colliderCount_;
+    return Pk;
+  };
   if (pipeline_ == NEBULA_MPM_PIPELINE_DENSE) {
     normalizeOrder(s);
     discardPending(s);
-    for (int k = 0; k < params_.numSubsteps; ++k) substepDense(P, s);
+    for (int k = 0; k < params_.numSubsteps; ++k) substepDense(atSubstep(k), s);
     return;
   }
   if (!pendingMatches(subDt)) {
     discardPending(s);
     buildPending(P, s);
   }
-  for (int k = 0; k < params_.numSubsteps; ++k) substepFused(P, s);
+  for (int k = 0; k < params_.numSubsteps; ++k) substepFused(atSubstep(k), s);
 }
 
 void MPMEngine::exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt) {
@@ -770,6 +789,9 @@ int nebula_mpm_set_particle_material_ids(nebula_mpm* e, const uint32_t* ids, uin
 }
 int nebula_mpm_set_colliders(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t n) {
   return guarded([&] { E(e).setColliders(c, n); });
+}
+int nebula_mpm_set_collider_track(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t perSubstep, uint32_t substeps) {
+  return guarded([&] { E(e).setColliderTrack(c, perSubstep, substeps); });
 }
 int nebula_mpm_clear_analytic_colliders(nebula_mpm* e) {
   return guarded([&] { E(e).clearAnalyticColliders(); });

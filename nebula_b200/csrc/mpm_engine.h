@@ -32,6 +32,20 @@ struct DevBuf {
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+    o.ptr = nullptr;
+    o.bytes = 0;
+  }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      reset();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~DevBuf();
   void alloc(size_t n);
   void ensure(size_t n);
@@ -48,6 +62,7 @@ class MPMEngine {
   void setMaterials(const nebula_mpm_material* mats, uint32_t n);
   void setParticleMaterialIds(const uint32_t* ids, uint32_t n);
   void setColliders(const nebula_mpm_collider* c, uint32_t n);
+  void setColliderTrack(const nebula_mpm_collider* c, uint32_t perSubstep, uint32_t substeps);
   void clearAnalyticColliders();
   void setColliderSDF(const float* sdf, uint64_t n);
   void setColliderSphere(float radius, float cx, float cy, float cz);
@@ -134,6 +149,7 @@ class MPMEngine {
   DevBuf materials_, colliders_, forces_, sdf_, err_;
   std::vector<Material> hostMaterials_;
   uint32_t colliderCount_ = 0;
+  uint32_t colliderTrackLen_ = 1;
   uint32_t forceCount_ = 0;
   bool hasSdf_ = false;
 

@@ -125,6 +125,14 @@ class MPMEngine:
         a = np.ascontiguousarray(np.asarray(cols, dtype=COLLIDER_DTYPE).reshape(-1))
         call("nebula_mpm_set_colliders", self._h, _ptr(a), len(a))
 
+    def setColliderTrack(self, track):
+        """track: (substeps, perSubstep) collider records; substep k of each
+        later step uses set min(k, substeps - 1)."""
+        a = np.ascontiguousarray(np.asarray(track, dtype=COLLIDER_DTYPE))
+        if a.ndim == 1:
+            a = a.reshape(-1, 1)
+        call("nebula_mpm_set_collider_track", self._h, _ptr(a), a.shape[1], a.shape[0])
+
     def clearAnalyticColliders(self):
         call("nebula_mpm_clear_analytic_colliders", self._h)
 

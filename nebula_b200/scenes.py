@@ -396,6 +396,17 @@ def batch_mix(seed=4, n_scenes=64, substeps=200, dt=1e-4, nmin=2000, nmax=200000
     return scenes
 
 
+def collider_track(scene, substeps, start=0):
+    """The scene's colliders over `substeps` substeps from substep `start`: each
+    moves with its own velocity, pos(k) = pos + vel * (start + k) * dt.
+    Returns a (substeps, colliders) record array (one set per substep)."""
+    cols = scene.params.colliders_array()[: len(scene.params.colliders)]
+    k = (np.arange(substeps, dtype=np.float64) + start) * np.float64(np.float32(scene.params.dt))
+    out = np.repeat(cols[None, :], substeps, axis=0)
+    out["pos"] = (cols["pos"][None, :, :].astype(np.float64) + k[:, None, None] * cols["vel"][None, :, :]).astype(np.float32)
+    return out
+
+
 def diff_block(seed=5, n=50000, res=64, substeps=200, dt=1e-4):
     """50,000-particle elastic block for the adjoint: 37x37x37 lattice truncated to
     50,000 points, per-particle E log-uniform in [5e3, 5e4], initial velocity
