@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--cpu-sample-substeps", type=int, default=0, help="oracle substeps timed for cpu_baseline (0 = auto)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement on the 64-scene mix")
     ap.add_argument("--batch-steps", type=int, default=5, help="timed steps of the batched / plain comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-vs-forward measurement")
     return ap.parse_args()
 
 
@@ -300,6 +301,61 @@ def measure_batch(steps: int, warmup: int, substeps: int) -> dict:
                     "replay; plain: the same kernels per scene, 64 engines in sequence"}
 
 
+# ----------------------------------------------------------------------------- adjoint
+def measure_adjoint(steps: int, warmup: int) -> dict:
+    """Forward rollout (with checkpoints) and its reverse pass on the
+    differentiable 50,000-particle workload, each replayed from a CUDA graph,
+    timed with CUDA events on one stream; the single-scene engine's forward on
+    the same scene (uniform E) is timed beside it."""
+    import torch
+
+    from nebula_b200 import scenes as S
+    from nebula_b200.adjoint import Rollout
+    from nebula_b200.engine import engine_for_scene
+
+    sc = S.diff_block()
+    roll = Rollout.for_scene(sc)
+    side = torch.cuda.Stream()
+    x0 = torch.from_numpy(sc.state["P"]).cuda()
+    v0 = torch.from_numpy(sc.state["v"]).cuda()
+    E = torch.from_numpy(sc.extra["E"]).cuda()
+    fwd_ms, bwd_ms = [], []
+    with torch.cuda.stream(side):
+        for it in range(warmup + steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record(side)
+            loss = roll.forward(x0, v0, E, sc.extra["target"])
+            ev[1].record(side)
+            roll.backward(1.0)
+            ev[2].record(side)
+            torch.cuda.synchronize()
+            if it >= warmup:
+                fwd_ms.append(ev[0].elapsed_time(ev[1]))
+                bwd_ms.append(ev[1].elapsed_time(ev[2]))
+    events = roll.events()
+    launches = roll.launches()
+    roll.cleanup()
+    eng = engine_for_scene(sc)
+    eng.numSubsteps = sc.substeps
+    eng.step(sc.params.dt * sc.substeps, side)
+    eng.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(side)
+    for _ in range(steps):
+        eng.step(sc.params.dt * sc.substeps, side)
+    e1.record(side)
+    torch.cuda.synchronize()
+    eng_ms = e0.elapsed_time(e1) / steps
+    eng.cleanup()
+    f, b = float(np.median(fwd_ms)), float(np.median(bwd_ms))
+    return {"workload": sc.name, "particles": sc.n, "grid": list(sc.params.grid_res), "substeps": sc.substeps,
+            "checkpoint_every": sc.extra["checkpoint_every"], "forward_ms": f, "backward_ms": b, "ratio_backward_to_forward": b / f,
+            "ratio_backward_to_engine_forward": b / eng_ms, "engine_forward_ms": eng_ms, "loss": float(loss), "events": events,
+            "steps": steps, "warmup": warmup, "launches_total": launches,
+            "note": "forward = rollout with checkpoint copies; backward = segment recomputation + reverse G2P/grid/P2G; "
+                    "engine_forward = the brick-sparse engine advancing the same scene (uniform E) for the same substeps"}
+
+
 # ----------------------------------------------------------------------------- nebula arm
 def main():
     args = parse()
@@ -463,6 +519,8 @@ def main():
     eng.cleanup()
     if not args.no_batch:
         line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20)
+    if not args.no_adjoint:
+        line["adjoint"] = measure_adjoint(3, 2)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

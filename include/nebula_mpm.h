@@ -275,6 +275,45 @@ int nebula_mpm_batch_scene_info(const nebula_mpm_batch* b, uint32_t scene, nebul
  * nebula_mpm_set_colliders resets it to one set. */
 int nebula_mpm_set_collider_track(nebula_mpm* e, const nebula_mpm_collider* c, uint32_t perSubstep, uint32_t substeps);
 
+/* ---------------------------------------------------------------- differentiable rollout
+ * No counterpart in the reference (it has no adjoint).  A rollout of
+ * `substeps` substeps of `dt` of an APIC, ELASTIC (Hencky) body with a
+ * per-particle Young's modulus (uniform nu and rho0), gravity and the grid
+ * wall band, on a dense grid of domainSize / cellSize; the loss is
+ * |COM(x_T) - target|^2 with the mass-weighted centre of mass.  backward()
+ * returns dL/dv0, dL/dE (and dL/dx0) by a hand-written reverse pass of G2P,
+ * grid update and P2G with checkpoints every `checkpointEvery` substeps
+ * (float32; the SVD and the Hencky-stress derivative in float64).  Arrays are
+ * DEVICE pointers: pos4 = (x, Vp), vel4 = (v, -), E per particle, outputs of
+ * the same shapes.  Forward and backward are replayed from CUDA graphs
+ * captured on first use when `stream` is not NULL.  Events seen by the last
+ * forward (bits: 1 J reset, 2 world clamp, 4 speed cap) make the gradient
+ * one of a non-smooth map there. */
+typedef struct nebula_mpm_adjoint nebula_mpm_adjoint;
+typedef struct nebula_mpm_adjoint_config {
+  float domainSize[3];
+  float cellSize;
+  uint32_t particles;
+  uint32_t substeps;
+  uint32_t checkpointEvery;
+  float dt;
+  float gravity[3];
+  float nu;
+  float rho0;
+} nebula_mpm_adjoint_config;
+int nebula_mpm_adjoint_create(const nebula_mpm_adjoint_config* cfg, nebula_mpm_adjoint** out);
+int nebula_mpm_adjoint_destroy(nebula_mpm_adjoint* a);
+/* dLoss (device, 1 float, may be NULL) receives the loss. */
+int nebula_mpm_adjoint_forward(nebula_mpm_adjoint* a, const float* dPos4, const float* dVel4, const float* dE, const float target[3],
+                               float* dLoss, void* stream);
+/* Gradients of lossGrad * L for the inputs of the last forward; NULL outputs are skipped. */
+int nebula_mpm_adjoint_backward(nebula_mpm_adjoint* a, float lossGrad, float* dGradVel4, float* dGradE, float* dGradPos4, void* stream);
+/* Field `field` of the final state of the last forward, to host (count = 4 * particles). */
+int nebula_mpm_adjoint_download(nebula_mpm_adjoint* a, int field, float* host, uint64_t count);
+int nebula_mpm_adjoint_events(nebula_mpm_adjoint* a, uint32_t* events);
+int nebula_mpm_adjoint_set_graphs(nebula_mpm_adjoint* a, int enable);
+int nebula_mpm_adjoint_launches(nebula_mpm_adjoint* a, uint64_t* launches);
+
 /* Domain helpers (src/core/Domain.h:14-39). */
 void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint32_t out[3]);
 uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]);

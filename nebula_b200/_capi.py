@@ -63,6 +63,11 @@ class BatchStats(C.Structure):
                 ("kernel_launches", C.c_uint64), ("graph_launches", C.c_uint64), ("error_flags", C.c_uint32)]
 
 
+class AdjointConfig(C.Structure):
+    _fields_ = [("domainSize", C.c_float * 3), ("cellSize", C.c_float), ("particles", C.c_uint32), ("substeps", C.c_uint32),
+                ("checkpointEvery", C.c_uint32), ("dt", C.c_float), ("gravity", C.c_float * 3), ("nu", C.c_float), ("rho0", C.c_float)]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -114,6 +119,14 @@ _SIGS = {
     "nebula_mpm_batch_sync": (C.c_int, [C.c_void_p]),
     "nebula_mpm_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     "nebula_mpm_batch_scene_info": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(SceneInfo)]),
+    "nebula_mpm_adjoint_create": (C.c_int, [C.POINTER(AdjointConfig), C.POINTER(C.c_void_p)]),
+    "nebula_mpm_adjoint_destroy": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float * 3, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_adjoint_backward": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_adjoint_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_adjoint_events": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "nebula_mpm_adjoint_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_adjoint_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "nebula_mpm_domain_grid_res": (None, [C.c_float * 3, C.c_float, C.c_uint32 * 3]),
     "nebula_mpm_domain_cube_res": (C.c_uint32, [C.c_uint32 * 3]),
     "nebula_mpm_domain_hash_cells": (C.c_uint32, [C.c_uint32 * 3]),

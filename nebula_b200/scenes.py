@@ -407,21 +407,26 @@ def collider_track(scene, substeps, start=0):
     return out
 
 
-def diff_block(seed=5, n=50000, res=64, substeps=200, dt=1e-4):
-    """50,000-particle elastic block for the adjoint: 37x37x37 lattice truncated to
-    50,000 points, per-particle E log-uniform in [5e3, 5e4], initial velocity
-    (0.3, 0, -0.2) + U(+/-0.05), APIC, dt=1e-4; target point seeded."""
+def diff_block(seed=5, n=50000, res=64, substeps=200, dt=1e-4, side=37, y0_cells=3.0, vy=-2.0):
+    """50,000-particle elastic block for the adjoint: a 37x37x37 lattice (spacing
+    0.5h, jitter +/-0.25h) truncated to n points, its base y0_cells cells above
+    the floor and falling at vy, so it reaches the wall band and is compressed
+    there for the last ~60% of the rollout (with no contact the COM loss would
+    not depend on E at all: internal forces conserve momentum).  Per-particle E
+    log-uniform in [5e3, 5e4], nu = 0.3, rho0 = 1000, initial velocity
+    (0.3, vy, -0.2) + U(+/-0.05), APIC, dt = 1e-4; target point seeded."""
     h = 1.0 / res
     sp = 0.5 * h
-    side = 37
-    pos = jittered_lattice(seed, 0, (side, side, side), sp, (0.5 - 18 * sp, 0.5, 0.5 - 18 * sp), 0.25 * h)[:n]
+    half = (side - 1) / 2.0
+    pos = jittered_lattice(seed, 0, (side, side, side), sp, (0.5 - half * sp, y0_cells * h, 0.5 - half * sp), 0.25 * h)[:n]
+    n = pos.shape[0]
     noise = uniform(seed, 3 * n, 1, -0.05, 0.05).reshape(n, 3)
-    vel = (np.array([0.3, 0.0, -0.2]) + noise).astype(np.float32)
+    vel = (np.array([0.3, vy, -0.2]) + noise).astype(np.float32)
     E = np.exp(uniform(seed, n, 2, math.log(5e3), math.log(5e4))).astype(np.float32)
-    target = (np.array([0.5, 0.5, 0.5]) + uniform(seed, 3, 3, -0.05, 0.05)).astype(np.float32)
+    target = (np.array([0.5, 0.3, 0.5]) + uniform(seed, 3, 3, -0.05, 0.05)).astype(np.float32)
     params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
                         materials=[material(MAT_ELASTIC, 1e4, 0.3, 1000.0)], forces=[gravity()])
     params.mu_lame, params.lambda_lame = lame(1e4, 0.3)
     sc = Scene("diff_block_50k_64", params, make_state(pos, np.float32(sp) ** 3, vel=vel), substeps)
-    sc.extra = {"E": E, "nu": 0.3, "target": target, "checkpoint_every": 20}
+    sc.extra = {"E": E, "nu": 0.3, "rho0": 1000.0, "target": target, "checkpoint_every": 20}
     return sc

@@ -361,3 +361,18 @@ def hencky_ref64_vjp(F, mu, lam, tbar):
     lb = np.zeros(1)
     lib().adj_hencky_vjp(_ptr(f), mu, lam, _ptr(tb), _ptr(fb), _ptr(mb), _ptr(lb))
     return fb.reshape(3, 3), float(mb[0]), float(lb[0])
+
+
+def fd_slope(loss_at, eps):
+    """Derivative at t = 0 of t -> loss_at(t) from five evaluations, robust to
+    an isolated jump: of the one-sided slopes on [-2e, -e], [-e, 0], [0, e],
+    [e, 2e], the one farthest from their median is dropped and the median of
+    the other three is returned.  The reference forward has sparse small jumps
+    (a grid node whose mass crosses the 1e-10 activation threshold enters
+    G2P with its stress-driven velocity), so a plain central difference that
+    straddles one is meaningless; one jump spoils at most one of the four
+    slopes.  Returns (median, slopes)."""
+    L = {k: loss_at(k * eps) for k in (-2, -1, 0, 1, 2)}
+    s = np.array([(L[-1] - L[-2]) / eps, (L[0] - L[-1]) / eps, (L[1] - L[0]) / eps, (L[2] - L[1]) / eps])
+    keep = np.delete(s, np.argmax(np.abs(s - np.median(s))))
+    return float(np.median(keep)), s
