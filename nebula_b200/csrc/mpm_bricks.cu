@@ -253,29 +253,43 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 
 // ------------------------------------------------------------------ shared-memory P2G
 // A CTA handles one particle brick at a time, in chunks of kChunk particles.
-// Each particle's P2G inputs go to a shared row, counting-sorted by the cell
-// its stencil is centred on (6^3 cells around the brick).  A warp then takes
-// whole cells: lanes 0..26 own the cell's 27 stencil nodes and accumulate the
-// contributions of all the cell's particles in registers, then add them with
-// plain stores into the warp's private 8^3 tile (lanes own distinct nodes, one
-// cell per warp at a time, so nothing races).  The brick ends with one sum over
-// the private tiles and one vector reduction per non-zero node.
+// Each particle's P2G inputs go to a shared row, and the row is pushed onto a
+// linked list of the cell its stencil is centred on (6^3 cells around the
+// brick; the first row of a cell also appends the cell to the chunk's list of
+// non-empty cells).  A warp then takes whole cells: lanes 0..26 own the cell's
+// 27 stencil nodes, walk the cell's list and accumulate its particles'
+// contributions in registers, then add them into the brick's 8^3 tile (see
+// kTileCopies).  Two barriers per chunk.  The brick ends with one vector
+// reduction per non-zero node of the tile.
 constexpr int kChunk = kThreads;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRow = 10;        // float4 per input row: 3 axes x 3 offsets of (A0, A1, A2, W), then (m, -, -, -)
 constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
 
+constexpr uint32_t kNoRow = 0xFFFFu;  // end of a cell's list
+// Copies of the brick's 8^3 accumulation tile: 1 = one tile shared by the
+// warps, updated with shared-memory float reductions (a warp owns one cell at
+// a time, so warps collide only on the nodes where neighbouring cells'
+// stencils overlap); kWarps = one private tile per warp with plain adds.
+constexpr int kTileCopies = 1;
+
 struct P2GSmem {
   float4 rows[kChunk * kRow];
-  float tiles[kWarps * 4 * kTileNodes];
-  uint32_t cellCount[kCellSlots];
-  uint32_t cellStart[kCellSlots];
-  uint16_t order[kChunk];
-  uint16_t cells[kCellSlots];
-  uint32_t numCells;
+  float tiles[kTileCopies * 4 * kTileNodes];
+  uint32_t head[kCellSlots];   // first row of each cell's list (kNoRow: empty)
+  uint16_t next[kChunk];       // next row of the same cell
+  uint16_t cells[kCellSlots];  // the chunk's non-empty cells
+  uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
   uint32_t item;
 };
+
+// Push this thread's row onto the list of cell `key` (`par`: the chunk's parity).
+__device__ __forceinline__ void p2gRegister(P2GSmem& sm, int key, uint32_t par) {
+  const uint32_t prev = atomicExch(&sm.head[key], threadIdx.x);
+  sm.next[threadIdx.x] = uint16_t(prev);
+  if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(key);
+}
 
 template <bool FLIP>
 struct G2P2GSmem {
@@ -358,83 +372,58 @@ __device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* 
 }
 
 __device__ __forceinline__ void p2gZeroTiles(P2GSmem& sm) {
-  for (int q = threadIdx.x; q < kWarps * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
-  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.cellCount[q] = 0u;
+  for (int q = threadIdx.x; q < kTileCopies * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
+  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.head[q] = kNoRow;
+  if (threadIdx.x < 2) sm.numCells[threadIdx.x] = 0u;
 }
 
-// Called by every thread once the chunk's rows are written and each thread
-// holding an in-tile particle has its cell key (< 216) and rank; ends synced.
-// Tile origin (node) = (bx, by, bz) * 4 - 2; stencil-centre cells start at + 1.
-__device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, int key, uint32_t rank, int tx, int ty, int tz) {
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    // exclusive scan of the 216 cell counts + list of non-empty cells
-    const int lane = threadIdx.x;
-    uint32_t c[7], sum = 0, ne = 0;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const int q = lane * 7 + k;
-      c[k] = q < kCellSlots ? sm.cellCount[q] : 0u;
-      sum += c[k];
-      ne += c[k] ? 1u : 0u;
-    }
-    uint32_t is = sum, in = ne;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t ys = __shfl_up_sync(0xffffffffu, is, o), yn = __shfl_up_sync(0xffffffffu, in, o);
-      if (lane >= o) {
-        is += ys;
-        in += yn;
-      }
-    }
-    uint32_t run = is - sum, pos = in - ne;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const int q = lane * 7 + k;
-      if (q < kCellSlots) {
-        sm.cellStart[q] = run;
-        if (c[k]) sm.cells[pos++] = uint16_t(q);
-      }
-      run += c[k];
-    }
-    if (lane == 31) sm.numCells = in;
-  }
-  __syncthreads();
-  if (key >= 0) sm.order[sm.cellStart[key] + rank] = uint16_t(threadIdx.x);
+// Called by every thread once the chunk's rows are written and registered;
+// ends synced.  Tile origin (node) = (bx, by, bz) * 4 - 2; stencil-centre
+// cells start at + 1.
+__device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, uint32_t par, int tx, int ty, int tz) {
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
   const int cr = int(P.cubeRes);
-  float* tile = sm.tiles + warp * 4 * kTileNodes;
-  const uint32_t numCells = sm.numCells;
+  float* tile = sm.tiles + (kTileCopies == 1 ? 0 : warp) * 4 * kTileNodes;
+  const uint32_t numCells = sm.numCells[par];
   for (uint32_t ci = warp; ci < numCells; ci += kWarps) {
     const int q = sm.cells[ci];
     const int rx = q % 6, ry = (q / 6) % 6, rz = q / 36;
-    if (lane >= 27) continue;
     const int lx = rx + dx, ly = ry + dy, lz = rz + dz;  // tile-local node
     const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
-    if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
-    float a[4] = {0.f, 0.f, 0.f, 0.f};
-    const uint32_t st = sm.cellStart[q], en = st + sm.cellCount[q];
-    for (uint32_t j = st; j < en; ++j) p2gNodeTerm(sm.rows + sm.order[j] * kRow, dx, dy, dz, a);
-    const int t = (lz * 8 + ly) * 8 + lx;
-    tile[t] += a[3];
-    tile[kTileNodes + t] += a[0];
-    tile[2 * kTileNodes + t] += a[1];
-    tile[3 * kTileNodes + t] += a[2];
+    if (lane < 27 && nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr) {
+      float a[4] = {0.f, 0.f, 0.f, 0.f};
+      // a list holds at most kChunk rows; the bound keeps the walk finite whatever the list holds
+      uint32_t j = sm.head[q] & 0xFFFFu;
+      for (int it = 0; j < uint32_t(kChunk) && it < kChunk; ++it, j = sm.next[j]) p2gNodeTerm(sm.rows + j * kRow, dx, dy, dz, a);
+      const int t = (lz * 8 + ly) * 8 + lx;
+      if (kTileCopies == 1) {
+        atomicAdd(tile + t, a[3]);
+        atomicAdd(tile + kTileNodes + t, a[0]);
+        atomicAdd(tile + 2 * kTileNodes + t, a[1]);
+        atomicAdd(tile + 3 * kTileNodes + t, a[2]);
+      } else {
+        tile[t] += a[3];
+        tile[kTileNodes + t] += a[0];
+        tile[2 * kTileNodes + t] += a[1];
+        tile[3 * kTileNodes + t] += a[2];
+      }
+    }
+    __syncwarp();
+    if (lane == 0) sm.head[q] = kNoRow;  // every lane has read it
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.cellCount[q] = 0u;
-  __syncthreads();
+  if (threadIdx.x == 0) sm.numCells[par] = 0u;  // reused two chunks later, after another barrier
 }
 
-// Sum the private tiles and add every non-zero node to the global grid.
+// Sum the tile copies and add every non-zero node to the global grid.
 __device__ __forceinline__ void p2gFlush(const SubstepParams& P, P2GSmem& sm, int tx, int ty, int tz, float4* acc) {
   const int cr = int(P.cubeRes);
   for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
     float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
+    for (int w = 0; w < kTileCopies; ++w) {
       const float* t = sm.tiles + w * 4 * kTileNodes;
       m += t[q];
       mx += t[kTileNodes + q];
@@ -498,10 +487,9 @@ __device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, P2GSmem& sm
   int bx, by, bz;
   mortonDecode(b, bx, by, bz);
   const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
-  for (uint32_t base = start; base < end; base += kChunk) {
+  uint32_t par = 0;
+  for (uint32_t base = start; base < end; base += kChunk, par ^= 1u) {
     const uint32_t t = base + threadIdx.x;
-    int key = -1;
-    uint32_t rank = 0;
     if (t < end) {
       const uint32_t s = B.perm[t];
       if (s < n) {
@@ -510,12 +498,12 @@ __device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, P2GSmem& sm
         cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
         float4* row = sm.rows + threadIdx.x * kRow;
         p2gRow(P, st, dtStress, cx, cy, cz, row);
-        key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
-        if (key >= 0) rank = atomicAdd(&sm.cellCount[key], 1u);
+        const int key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
+        if (key >= 0) p2gRegister(sm, key, par);
         else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
       }
     }
-    p2gChunk(P, sm, key, rank, tx, ty, tz);
+    p2gChunk(P, sm, par, tx, ty, tz);
   }
   p2gFlush(P, sm, tx, ty, tz, G.acc);
 }
@@ -637,12 +625,11 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
   __syncthreads();
   const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
   const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
-  for (uint32_t base = start; base < end; base += kChunk) {
+  uint32_t par = 0;
+  for (uint32_t base = start; base < end; base += kChunk, par ^= 1u) {
     const uint32_t t = base + threadIdx.x;
     const bool act = t < end;
     const uint32_t mask = __ballot_sync(0xffffffffu, act);
-    int key = -1;
-    uint32_t rank = 0;
     if (act) {
       const uint32_t s = B.perm[t];
       const bool valid = s < n;
@@ -671,16 +658,16 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
         markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
         float4* row = sm.rows + threadIdx.x * kRow;
         p2gRow(P, st, dtStress, cx, cy, cz, row);
-        key = cellSlot(cx, cy, cz, sx, sy, sz);
+        const int key = cellSlot(cx, cy, cz, sx, sy, sz);
         if (key >= 0) {
-          rank = atomicAdd(&sm.cellCount[key], 1u);
+          p2gRegister(sm, key, par);
         } else {
           p2gRowGlobal(P, row, cx, cy, cz, G.acc);
           atomicAdd(B.counters + kCntOverflow, 1u);
         }
       }
     }
-    p2gChunk(P, sm, key, rank, tx, ty, tz);
+    p2gChunk(P, sm, par, tx, ty, tz);
   }
   p2gFlush(P, sm, tx, ty, tz, G.acc);
 }
