@@ -261,6 +261,107 @@ template <class T> __device__ __forceinline__ void svd3(const m3<T>& F, m3<T>& U
   }
 }
 
+// ---- float64 decomposition of the return maps, with cheap rotations.
+// One Jacobi rotation zeroing A[P0][P1] (the pivot rule, stopping rule and
+// angle formula of mpm_common.glsl:224-244): the angle's tangent t is
+// evaluated in float, then (c, s) are made exactly orthonormal in double
+// (c = 1/sqrt(1 + t^2), s = t c) and A is transformed as the full similarity
+// R^T A R.  An angle off by float rounding therefore leaves an off-diagonal
+// ~1e-7 of the one removed, which later rotations remove; A and V stay a
+// float64-exact similarity and an orthonormal basis.  This replaces three
+// float64 divisions and two square roots per rotation by one rsqrt.
+template <int P0, int P1>
+__device__ __forceinline__ void jacobiRotateMixed(m3<double>& A, m3<double>& V) {
+  constexpr int R = 3 - P0 - P1;
+  const double apq = A.m[P0][P1], app = A.m[P0][P0], aqq = A.m[P1][P1];
+  const float tau = float(aqq - app) / (2.0f * float(apq));
+  const float at = fabsf(tau);
+  const float tf = at < 1e18f ? gsign(tau) / (at + sqrtf(1.0f + tau * tau)) : 0.5f / tau;
+  const double t = double(tf);
+  const double c = rsqrt(1.0 + t * t);
+  const double sn = t * c;
+  const double cc = c * c, ss = sn * sn, cs = c * sn;
+  A.m[P0][P0] = cc * app - 2.0 * cs * apq + ss * aqq;
+  A.m[P1][P1] = ss * app + 2.0 * cs * apq + cc * aqq;
+  const double off = cs * (app - aqq) + (cc - ss) * apq;
+  A.m[P0][P1] = off;
+  A.m[P1][P0] = off;
+  const double arp = A.m[R][P0], arq = A.m[R][P1];
+  A.m[R][P0] = c * arp - sn * arq;
+  A.m[P0][R] = A.m[R][P0];
+  A.m[R][P1] = sn * arp + c * arq;
+  A.m[P1][R] = A.m[R][P1];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const double vrp = V.m[q][P0], vrq = V.m[q][P1];
+    V.m[q][P0] = c * vrp - sn * vrq;
+    V.m[q][P1] = sn * vrp + c * vrq;
+  }
+}
+
+// svd3 of the return maps: same eigen-decomposition of F^T F (<= 20 rotations,
+// stop below 1e-8), descending sort, U columns F v_i / sigma_i and the sign
+// fix-up; sigma_i and 1/sigma_i come from one rsqrt of the eigenvalue.
+__device__ __forceinline__ void svd3Mixed(const m3<double>& F, m3<double>& U, double sigma[3], m3<double>& V) {
+  m3<double> A;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) A.m[j][i] = F.m[i][0] * F.m[j][0] + F.m[i][1] * F.m[j][1] + F.m[i][2] * F.m[j][2];
+  V = m3ident<double>();
+#pragma unroll 1
+  for (int iter = 0; iter < 20; iter++) {
+    const double b01 = fabs(A.m[0][1]), b02 = fabs(A.m[0][2]), b12 = fabs(A.m[1][2]);
+    if (fmax(b01, fmax(b02, b12)) < 1e-8) break;
+    if (b01 >= fmax(b02, b12)) jacobiRotateMixed<0, 1>(A, V);
+    else if (b02 >= b12) jacobiRotateMixed<0, 2>(A, V);
+    else jacobiRotateMixed<1, 2>(A, V);
+  }
+  double inv[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double l = fmax(A.m[i][i], 0.0);
+    const double r = l > 0.0 ? rsqrt(l) : 0.0;
+    sigma[i] = l * r;
+    inv[i] = r;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = i + 1; j < 3; j++) {
+      if (sigma[j] > sigma[i]) {
+        double tmp = sigma[i]; sigma[i] = sigma[j]; sigma[j] = tmp;
+        tmp = inv[i]; inv[i] = inv[j]; inv[j] = tmp;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { double v = V.m[k][i]; V.m[k][i] = V.m[k][j]; V.m[k][j] = v; }
+      }
+    }
+  U = m3zero<double>();
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    if (sigma[i] > 1e-8) {
+      const double v0 = V.m[0][i], v1 = V.m[1][i], v2 = V.m[2][i];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) U.m[k][i] = (F.m[0][k] * v0 + F.m[1][k] * v1 + F.m[2][k] * v2) * inv[i];
+    } else {
+      U.m[i][i] = 1.0;
+    }
+  }
+  if (m3det(U) < 0.0) {
+    U.m[0][2] = -U.m[0][2];
+    U.m[1][2] = -U.m[1][2];
+    U.m[2][2] = -U.m[2][2];
+    sigma[2] = -sigma[2];
+  }
+}
+
+// Hencky principal stresses from log-strains e_i = log(max(|sigma_i|, 1e-6)).
+__device__ __forceinline__ void henckyFromLogStrain(const double e[3], double mu, double lam, double k[3]) {
+  const double tr = e[0] + e[1] + e[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) k[i] = lam * tr + 2.0 * mu * e[i];
+}
+
 // Hencky principal Kirchhoff stresses k_i = lam*tr(eps) + 2 mu eps_i with
 // eps = log(max(|sigma|, 1e-6)).
 template <class T> __device__ __forceinline__ void henckyPrincipal(const T sigma[3], T mu, T lam, T k[3]) {
@@ -325,7 +426,7 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
   const double mu = mu_f, lam = lam_f;
   m3<double> Fd = m3cast<double>(F), U, V;
   double s[3];
-  svd3(Fd, U, s, V);
+  svd3Mixed(Fd, U, s, V);
   double eps[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) eps[i] = log(fmax(fabs(s[i]), 1e-6));
@@ -362,15 +463,18 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
   }
   double k[3];
   if (rebuild) {
-    double sp[3];
+    double sp[3], e[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) sp[i] = exp(eps[i]);
+    for (int i = 0; i < 3; ++i) {
+      sp[i] = exp(eps[i]);
+      e[i] = fmax(eps[i], -13.815510557964274);  // log(max(exp(eps), 1e-6)) = max(eps, log 1e-6)
+    }
     m3<double> Fn = rebuildUSVt(U, sp, V);
     F = m3cast<float>(Fn);
-    henckyPrincipal(sp, mu, lam, k);
+    henckyFromLogStrain(e, mu, lam, k);
     tau = m3cast<float>(stressRebuilt(U, k));
   } else {
-    henckyPrincipal(s, mu, lam, k);
+    henckyFromLogStrain(eps, mu, lam, k);  // eps = log(max(|s|, 1e-6)) already
     tau = m3cast<float>(stressUDUt(U, k));
   }
 }
