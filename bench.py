@@ -232,19 +232,26 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------------------- batched vs plain
-def measure_batch(steps: int, warmup: int, substeps: int) -> dict:
+def measure_batch(steps: int, warmup: int, substeps: int, dist=None) -> dict:
     """The 64-scene mix advanced by the batched engine (one set of launches
-    per substep, replayed from a CUDA graph) and by 64 single-scene engines
+    per substep, replayed from a CUDA graph) and by single-scene engines
     stepped one after another, on the same stream, with each scene's moving
-    sphere re-uploaded as a collider track before every step in both forms."""
+    sphere re-uploaded as a collider track before every step in both forms.
+    With several ranks the scenes are partitioned by particle count
+    (nebula_b200.shard); each rank runs its share and the time is the maximum
+    over ranks (the total work is fixed: strong scaling)."""
     import torch
 
     from nebula_b200 import scenes as S
+    from nebula_b200 import shard
     from nebula_b200.batch import batch_for_scenes
     from nebula_b200.engine import engine_for_scene
 
-    scenes = S.batch_mix()
-    n = sum(sc.n for sc in scenes)
+    rank, world, _ = shard.rank_info()
+    sizes = S.batch_mix_sizes()
+    mine = shard.partition_scenes(sizes, world)[rank]
+    scenes = S.batch_mix(only=set(mine))
+    n_all = sum(sizes)
     dt = scenes[0].params.dt
     frames = warmup + steps
     tracks = [[S.collider_track(sc, substeps, k * substeps) for k in range(frames)] for sc in scenes]
@@ -254,13 +261,17 @@ def measure_batch(steps: int, warmup: int, substeps: int) -> dict:
         for k in range(warmup):
             step_fn(k)
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for k in range(warmup, frames):
             step_fn(k)
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        if dist is not None:
+            dist.barrier()
+        return shard.max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
 
     b, ids = batch_for_scenes(scenes)
 
@@ -292,13 +303,15 @@ def measure_batch(steps: int, warmup: int, substeps: int) -> dict:
     launches_p = int(sum(e.stats()["kernel_launches"] for e in engines) - l0)
     for e in engines:
         e.cleanup()
-    ps = float(n) * substeps * steps
-    return {"workload": "batch_mix_64", "scenes": len(scenes), "particles": n, "substeps_per_step": substeps, "steps": steps,
+    ps = float(n_all) * substeps * steps
+    return {"workload": "batch_mix_64", "scenes": len(sizes), "particles": n_all, "substeps_per_step": substeps, "steps": steps,
             "warmup": warmup, "dt": dt, "value": ps / (ms_b * 1e-3), "ms_per_step": ms_b / steps, "plain_value": ps / (ms_p * 1e-3),
             "plain_ms_per_step": ms_p / steps, "speedup": ms_p / ms_b, "unit": UNIT, "gpu_launches": launches_b,
-            "plain_gpu_launches": launches_p,
+            "plain_gpu_launches": launches_p, "n_gpus": world, "scaling": "strong" if world > 1 else "single",
+            "scenes_on_rank0": len(mine),
             "note": "batched: one grid update + one fused G2P/P2G + scan + permutation per substep over all scenes, graph "
-                    "replay; plain: the same kernels per scene, 64 engines in sequence"}
+                    "replay; plain: the same kernels per scene, one engine per scene in sequence; ranks take scenes by a "
+                    "particle-balanced greedy partition, time = max over ranks"}
 
 
 # ----------------------------------------------------------------------------- adjoint
@@ -518,7 +531,7 @@ def main():
                                 "sample": "%d substeps of %s (after one untimed), CPU oracle ref32 mode, OpenMP" % (k, sc.name)}
     eng.cleanup()
     if not args.no_batch:
-        line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20)
+        line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20, dist)
     if not args.no_adjoint:
         line["adjoint"] = measure_adjoint(3, 2)
     if rank == 0:

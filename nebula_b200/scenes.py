@@ -362,22 +362,40 @@ def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, wi
     return Scene("slope_flow_1m_256", params, make_state(pos, vp), substeps, sdf=sdf)
 
 
-def batch_mix(seed=4, n_scenes=64, substeps=200, dt=1e-4, nmin=2000, nmax=200000):
+def _mix_shape(u_row, nmin, nmax):
+    """Grid resolution and lattice counts of one scene of the mix."""
+    n_target = int(round(math.exp(math.log(nmin) + (math.log(nmax) - math.log(nmin)) * u_row[0])))
+    res = (64, 96, 128)[min(2, int(u_row[1] * 3))]
+    side = max(2, int(round(n_target ** (1.0 / 3.0))))
+    ny = max(1, n_target // (side * side))
+    return res, (side, ny, side)
+
+
+def batch_mix_sizes(seed=4, n_scenes=64, nmin=2000, nmax=200000):
+    """Particle count of every scene of batch_mix, without building the scenes."""
+    u = uniform(seed, n_scenes * 8, 11).reshape(n_scenes, 8)
+    out = []
+    for s in range(n_scenes):
+        _, (nx, ny, nz) = _mix_shape(u[s], nmin, nmax)
+        out.append(nx * ny * nz)
+    return out
+
+
+def batch_mix(seed=4, n_scenes=64, substeps=200, dt=1e-4, nmin=2000, nmax=200000, only=None):
     """64 independent scenes: particle counts log-uniform in [2e3, 2e5], grids
     64^3 / 96^3 / 128^3 (unit cube), a jittered box with initial velocity
     U[-1,1]^3, ELASTIC or VON_MISES, and one sphere collider of radius 0.1
-    moving with a seeded velocity."""
+    moving with a seeded velocity.  `only` (a set of scene indices) builds a
+    subset, e.g. one rank's share."""
     scenes = []
     u = uniform(seed, n_scenes * 8, 11).reshape(n_scenes, 8)
     for s in range(n_scenes):
-        n_target = int(round(math.exp(math.log(nmin) + (math.log(nmax) - math.log(nmin)) * u[s, 0])))
-        res = (64, 96, 128)[min(2, int(u[s, 1] * 3))]
+        if only is not None and s not in only:
+            continue
+        res, cnt = _mix_shape(u[s], nmin, nmax)
         h = float(np.float32(1.0) / np.float32(res))
         sp = 0.5 * h
-        side = max(2, int(round(n_target ** (1.0 / 3.0))))
-        nxz = side
-        ny = max(1, n_target // (nxz * nxz))
-        cnt = (nxz, ny, nxz)
+        nxz, ny = cnt[0], cnt[1]
         n = nxz * ny * nxz
         ox = 0.5 - sp * (nxz - 1) / 2.0
         oy = 0.45
