@@ -47,6 +47,31 @@ __device__ __forceinline__ void markStencilBricks(const SubstepParams& P, int cx
       for (int bx = x0; bx <= x1; ++bx) flag[mortonEncode(bx, by, bz)] = 1u;
 }
 
+// Bit (dz*9 + dy*3 + dx) of the 3^3 bricks around brick (bx, by, bz) for every
+// brick the stencil of cell (cx,cy,cz) touches; false when one lies outside
+// that neighbourhood (the caller then marks globally).
+__device__ __forceinline__ bool stencilBrickMask(const SubstepParams& P, int cx, int cy, int cz, int bx, int by, int bz, uint32_t& mask) {
+  const int cr = int(P.cubeRes) - 1;
+  const int x0 = max(cx - 1, 0) >> 2, x1 = min(cx + 1, cr) >> 2;
+  const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, cr) >> 2;
+  const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, cr) >> 2;
+  if (x0 < bx - 1 || x1 > bx + 1 || y0 < by - 1 || y1 > by + 1 || z0 < bz - 1 || z1 > bz + 1) return false;
+  for (int z = z0; z <= z1; ++z)
+    for (int y = y0; y <= y1; ++y)
+      for (int x = x0; x <= x1; ++x) mask |= 1u << ((z - bz + 1) * 9 + (y - by + 1) * 3 + (x - bx + 1));
+  return true;
+}
+
+// Flags of the marked neighbour bricks of item brick (bx, by, bz); run by threads 0..26.
+__device__ __forceinline__ void flushBrickMarks(const SubstepParams& P, uint32_t mask, int bx, int by, int bz, uint32_t* flag) {
+  const int t = threadIdx.x;
+  if (t >= 27 || !((mask >> t) & 1u)) return;
+  const int x = bx + t % 3 - 1, y = by + (t / 3) % 3 - 1, z = bz + t / 9 - 1;
+  const int bmax = (int(P.cubeRes) - 1) >> 2;
+  if (x < 0 || y < 0 || z < 0 || x > bmax || y > bmax || z > bmax) return;
+  flag[mortonEncode(x, y, z)] = 1u;
+}
+
 // ------------------------------------------------------------------ batch scenes
 // The scene s with base[s] <= x < base[s+1] (base non-decreasing, x < base[count]).
 __device__ __forceinline__ uint32_t findScene(const uint32_t* __restrict__ base, uint32_t count, uint32_t x) {
@@ -327,6 +352,7 @@ struct P2GSmem {
   uint16_t next[kChunk];       // next row of the same cell
   uint16_t cells[kCellSlots];  // the chunk's non-empty cells
   uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
+  uint32_t markMask;           // grid-active marks of the item brick's 3^3 neighbour bricks
   uint32_t item;
 };
 
@@ -421,6 +447,7 @@ __device__ __forceinline__ void p2gZeroTiles(P2GSmem& sm) {
   for (int q = threadIdx.x; q < kTileCopies * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
   for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.head[q] = kNoRow;
   if (threadIdx.x < 2) sm.numCells[threadIdx.x] = 0u;
+  if (threadIdx.x == 0) sm.markMask = 0u;
 }
 
 // Called by every thread once the chunk's rows are written and registered;
@@ -699,6 +726,7 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
     const uint32_t t = base + threadIdx.x;
     const bool act = t < end;
     const uint32_t mask = __ballot_sync(0xffffffffu, act);
+    uint32_t marks = 0;
     if (act) {
       const uint32_t s = B.perm[t];
       const bool valid = s < n;
@@ -724,7 +752,7 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
       B.binKey[t] = nb;
       B.binRank[t] = r;
       if (valid) {
-        markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
+        if (!stencilBrickMask(P, cx, cy, cz, bx, by, bz, marks)) markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
         float4* row = sm.rows + threadIdx.x * kRow;
         p2gRow(P, st, dtStress, cx, cy, cz, row);
         const int key = cellSlot(cx, cy, cz, sx, sy, sz);
@@ -736,8 +764,12 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
         }
       }
     }
+    marks = __reduce_or_sync(0xffffffffu, marks);
+    if ((threadIdx.x & 31) == 0 && marks) atomicOr(&sm.markMask, marks);
     p2gChunk(P, sm, par, tx, ty, tz);
   }
+  // p2gChunk ended with a barrier: every warp's marks are in
+  flushBrickMarks(P, sm.markMask, bx, by, bz, B.brickFlag + brickBase);
   p2gFlush(P, sm, tx, ty, tz, G.acc);
 }
 
