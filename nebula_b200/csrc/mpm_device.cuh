@@ -427,9 +427,12 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
   m3<double> Fd = m3cast<double>(F), U, V;
   double s[3];
   svd3Mixed(Fd, U, s, V);
+  // The decomposition is float64; the log-strains and their exponentials are
+  // scalar functions of well-separated magnitudes and run in float, the
+  // precision of the reference (F' is stored in float in any case).
   double eps[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) eps[i] = log(fmax(fabs(s[i]), 1e-6));
+  for (int i = 0; i < 3; ++i) eps[i] = double(logf(fmaxf(fabsf(float(s[i])), 1e-6f)));
   double trEps = eps[0] + eps[1] + eps[2];
   double dev[3];
 #pragma unroll
@@ -466,7 +469,7 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
     double sp[3], e[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      sp[i] = exp(eps[i]);
+      sp[i] = double(expf(float(eps[i])));
       e[i] = fmax(eps[i], -13.815510557964274);  // log(max(exp(eps), 1e-6)) = max(eps, log 1e-6)
     }
     m3<double> Fn = rebuildUSVt(U, sp, V);
