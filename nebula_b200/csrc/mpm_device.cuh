@@ -169,6 +169,9 @@ template <class A, class B> __device__ __forceinline__ m3<A> m3cast(const m3<B>&
 template <class T> __device__ __forceinline__ T dsqrt(T x);
 template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrtf(x); }
 template <> __device__ __forceinline__ double dsqrt<double>(double x) { return sqrt(x); }
+template <class T> __device__ __forceinline__ T rcpsqrt(T x);
+template <> __device__ __forceinline__ float rcpsqrt<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ double rcpsqrt<double>(double x) { return rsqrt(x); }
 template <class T> __device__ __forceinline__ T dlog(T x);
 template <> __device__ __forceinline__ float dlog<float>(float x) { return logf(x); }
 template <> __device__ __forceinline__ double dlog<double>(double x) { return log(x); }
@@ -185,7 +188,7 @@ __device__ __forceinline__ void jacobiRotate(m3<T>& A, m3<T>& V) {
   const T app = A.m[P0][P0], aqq = A.m[P1][P1];
   const T tau = (aqq - app) / (T(2) * apq);
   const T t = gsign(tau) / (fabs(tau) + dsqrt<T>(T(1) + tau * tau));
-  const T c = T(1) / dsqrt<T>(T(1) + t * t);
+  const T c = rcpsqrt<T>(T(1) + t * t);
   const T s = t * c;
   A.m[P0][P0] = app - t * apq;
   A.m[P1][P1] = aqq + t * apq;
@@ -247,8 +250,9 @@ template <class T> __device__ __forceinline__ void svd3(const m3<T>& F, m3<T>& U
   for (int i = 0; i < 3; i++) {
     if (sigma[i] > T(1e-8)) {
       T v0 = V.m[0][i], v1 = V.m[1][i], v2 = V.m[2][i];
+      const T inv = T(1) / sigma[i];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) U.m[k][i] = (F.m[0][k] * v0 + F.m[1][k] * v1 + F.m[2][k] * v2) / sigma[i];
+      for (int k = 0; k < 3; ++k) U.m[k][i] = (F.m[0][k] * v0 + F.m[1][k] * v1 + F.m[2][k] * v2) * inv;
     } else {
       U.m[i][i] = T(1);
     }
