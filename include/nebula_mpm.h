@@ -151,8 +151,40 @@ int nebula_mpm_set_forces(nebula_mpm* e, const nebula_mpm_force* f, uint32_t n);
  * vel4=(v, id bits); F=I, B=0, stress=0; truncated at capacity.  *appended
  * (may be NULL) receives the count actually added. */
 int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* vel4, uint32_t n, uint32_t* appended);
-/* MPMEngine::resetParticles (MPMEngine.cpp:281-287). */
+/* MPMEngine::resetParticles (MPMEngine.cpp:281-287); also rewinds the emitters. */
 int nebula_mpm_reset_particles(nebula_mpm* e);
+
+/* Emitter (src/core/Emitter.h:39-224) as used by MPMEngine::emitFromEmitters
+ * (MPMEngine.cpp:289-352).  shape 0 AABB: size = full edge lengths; 1 SPHERE:
+ * size[0] = radius; 2 ELLIPSE: size[0] = semi-axis along x, size[1] = along
+ * y, z fixed at center[2].  step_count 0 = every step, -1 = first step only,
+ * >0 = that many steps.  particleVolume <= 0 takes the config's
+ * (domainSize/n)^3 product, as the reference does.
+ * At the start of each nebula_mpm_step every due emitter appends
+ * min(particles_per_step, capacity - live) particles IN A KERNEL on the step's
+ * stream (no host upload, no synchronisation), then moves its centre by
+ * center_vel * dt.  Positions and velocity randomness come from a
+ * counter-based hash of (seed, emission, particle): the same shapes and
+ * distributions as the reference's std::mt19937 sampling, not its numbers. */
+typedef struct nebula_mpm_emitter {
+  uint32_t shape;
+  float center[3];
+  float size[3];
+  float vel[3];
+  float center_vel[3];
+  int32_t particles_per_step;
+  uint32_t particleType;      /* material id of the emitted particles */
+  uint32_t emitAlongNormal;   /* 1: |vel| along the shape's outward normal */
+  float velocityRandomness;   /* > 0: + U(-r, r)^3 per particle */
+  int32_t step_count;
+  float particleVolume;
+  uint32_t pad;
+} nebula_mpm_emitter;
+/* MPMEngine::addEmitter / clearEmitters (MPMEngine.cpp:271-279). */
+int nebula_mpm_add_emitter(nebula_mpm* e, const nebula_mpm_emitter* em, uint32_t* index);
+int nebula_mpm_clear_emitters(nebula_mpm* e);
+/* The emitter's current record (its centre moves with center_vel) and how many times it has emitted. */
+int nebula_mpm_get_emitter(const nebula_mpm* e, uint32_t index, nebula_mpm_emitter* em, int32_t* stepsDone);
 /* Replace the full state of particles [0, n) (n <= capacity; sets the live
  * count to n) from 8 host float4 arrays in the reference layout (P, v, F0..B2). */
 int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_t n);

@@ -87,6 +87,9 @@ _SIGS = {
     "nebula_mpm_set_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "nebula_mpm_append_particles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "nebula_mpm_reset_particles": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_add_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "nebula_mpm_clear_emitters": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_get_emitter": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_int32)]),
     "nebula_mpm_upload_state": (C.c_int, [C.c_void_p, C.c_void_p * 8, C.c_uint32]),
     "nebula_mpm_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint64]),
     "nebula_mpm_step": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p]),

@@ -355,6 +355,65 @@ uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32
 void MPMEngine::resetParticles() {
   prepareHostAccess(true);
   live_ = 0;
+  std::fill(emitterDone_.begin(), emitterDone_.end(), 0);  // MPMEngine.cpp:285-286
+  emitEvents_ = 0;
+}
+
+uint32_t MPMEngine::addEmitter(const nebula_mpm_emitter& em) {
+  if (em.shape > 2u) throw Error(NEBULA_MPM_ERR_INVALID, "emitter shape must be 0 (AABB), 1 (SPHERE) or 2 (ELLIPSE)");
+  if (em.particles_per_step < 0) throw Error(NEBULA_MPM_ERR_INVALID, "particles_per_step must be >= 0");
+  if (em.step_count < -1) throw Error(NEBULA_MPM_ERR_INVALID, "step_count must be -1, 0 or positive");
+  for (int a = 0; a < 3; ++a)
+    if (!(em.size[a] >= 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "emitter size must be >= 0");
+  if (!(em.particleVolume > 0.f) && (cfg_.nx == 0 || cfg_.ny == 0 || cfg_.nz == 0))
+    throw Error(NEBULA_MPM_ERR_INVALID, "emitter particleVolume <= 0 needs the config's nx, ny, nz (MPMConfig::particleVolume)");
+  EmitterRec r;
+  static_assert(sizeof(r) == sizeof(em), "emitter record");
+  std::memcpy(&r, &em, sizeof(r));
+  emitters_.push_back(r);
+  emitterDone_.push_back(0);
+  return uint32_t(emitters_.size() - 1);
+}
+
+void MPMEngine::clearEmitters() {
+  emitters_.clear();
+  emitterDone_.clear();
+}
+
+void MPMEngine::getEmitter(uint32_t i, nebula_mpm_emitter* em, int32_t* done) const {
+  if (i >= emitters_.size()) throw Error(NEBULA_MPM_ERR_INVALID, "emitter index out of range");
+  std::memcpy(em, &emitters_[i], sizeof(*em));
+  if (done) *done = emitterDone_[i];
+}
+
+// MPMEngine::emitFromEmitters (MPMEngine.cpp:289-352): the same schedule,
+// count, truncation and centre motion; the particles are written by a kernel
+// on the step's stream.  Returns whether any particle was added.
+bool MPMEngine::emitFromEmitters(float dt, cudaStream_t s) {
+  bool added = false;
+  for (size_t si = 0; si < emitters_.size(); ++si) {
+    EmitterRec& em = emitters_[si];
+    int32_t& done = emitterDone_[si];
+    const bool due = em.step_count == -1 ? done == 0 : (em.step_count == 0 ? true : done < em.step_count);
+    if (!due) continue;
+    const int64_t available = int64_t(capacity_) - int64_t(live_);
+    const int64_t nNew = std::min<int64_t>(em.particles_per_step, available);
+    if (nNew <= 0) {
+      ++done;
+      continue;
+    }
+    const float Vp = em.particleVolume > 0.f ? em.particleVolume
+                                             : (cfg_.domainSize[0] / float(cfg_.nx)) * (cfg_.domainSize[1] / float(cfg_.ny)) *
+                                                   (cfg_.domainSize[2] / float(cfg_.nz));
+    check(launchEmit(em, Vp, kEmitSeed, emitEvents_++, uint32_t(nNew), statePtrs(cur_), static_cast<uint32_t*>(pid_[cur_].ptr), live_, s,
+                     &launches_),
+          "emit");
+    live_ += uint32_t(nNew);
+    ++done;
+    for (int a = 0; a < 3; ++a) em.center[a] += em.center_vel[a] * dt;
+    added = true;
+  }
+  return added;
 }
 
 void MPMEngine::uploadState(const float* const f[8], uint32_t n) {
@@ -594,6 +653,8 @@ void MPMEngine::step(float dt, cudaStream_t s) {
     quiesce();
     lastStream_ = s;
   }
+  // the emitters run first (MPMEngine.cpp:406); new particles invalidate the pending P2G
+  if (!emitters_.empty() && emitFromEmitters(dt, s)) discardPending(s);
   const int n = std::max(1, params_.numSubsteps);
   const float subDt = dt / float(n);  // MPMEngine.cpp:413
   const SubstepParams P = buildParams(subDt);
@@ -812,6 +873,22 @@ int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* v
   return guarded([&] {
     uint32_t k = E(e).appendParticles(pos4, vel4, n);
     if (appended) *appended = k;
+  });
+}
+int nebula_mpm_add_emitter(nebula_mpm* e, const nebula_mpm_emitter* em, uint32_t* index) {
+  return guarded([&] {
+    if (!em) throw Error(NEBULA_MPM_ERR_INVALID, "null emitter");
+    const uint32_t i = E(e).addEmitter(*em);
+    if (index) *index = i;
+  });
+}
+int nebula_mpm_clear_emitters(nebula_mpm* e) {
+  return guarded([&] { E(e).clearEmitters(); });
+}
+int nebula_mpm_get_emitter(const nebula_mpm* e, uint32_t index, nebula_mpm_emitter* em, int32_t* stepsDone) {
+  return guarded([&] {
+    if (!em) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    E(e).getEmitter(index, em, stepsDone);
   });
 }
 int nebula_mpm_reset_particles(nebula_mpm* e) {

@@ -10,6 +10,7 @@
 #include "../../include/nebula_mpm.h"
 #include "mpm_bricks.cuh"
 #include "mpm_device.cuh"
+#include "mpm_emit.cuh"
 #include "mpm_internal.h"
 
 namespace nebula {
@@ -69,6 +70,9 @@ class MPMEngine {
   void clearCollider();
   void setForces(const nebula_mpm_force* f, uint32_t n);
   uint32_t appendParticles(const float* pos4, const float* vel4, uint32_t n);
+  uint32_t addEmitter(const nebula_mpm_emitter& em);
+  void clearEmitters();
+  void getEmitter(uint32_t i, nebula_mpm_emitter* em, int32_t* done) const;
   void resetParticles();
   void uploadState(const float* const f[8], uint32_t n);
   void download(int field, float* host, uint64_t count);
@@ -118,6 +122,7 @@ class MPMEngine {
   void substepFused(const SubstepParams& P, cudaStream_t s);
   void prepareHostAccess(bool modifiesParticles);
   bool pendingMatches(float subDt) const;
+  bool emitFromEmitters(float dt, cudaStream_t s);
 
   nebula_mpm_config cfg_;
   nebula_mpm_params params_{0.3f, 0.0f, 20, 0u, 1e5f, 0.577f, 0.0f, 0.0f};  // MPMEngine.h:72-80
@@ -150,6 +155,10 @@ class MPMEngine {
   std::vector<Material> hostMaterials_;
   uint32_t colliderCount_ = 0;
   uint32_t colliderTrackLen_ = 1;
+  std::vector<EmitterRec> emitters_;
+  std::vector<int32_t> emitterDone_;
+  uint64_t emitEvents_ = 0;  // emissions since create / reset: the counter of the sampling hash
+  static constexpr uint64_t kEmitSeed = 12345;
   uint32_t forceCount_ = 0;
   bool hasSdf_ = false;
 

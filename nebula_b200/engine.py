@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _capi
 from ._capi import call
-from .scenes import COLLIDER_DTYPE, FIELDS, FORCE_DTYPE, MATERIAL_DTYPE
+from .scenes import COLLIDER_DTYPE, EMITTER_DTYPE, FIELDS, FORCE_DTYPE, MATERIAL_DTYPE
 
 FIELD_INDEX = {f: i for i, f in enumerate(FIELDS)}
 
@@ -176,6 +176,23 @@ class MPMEngine:
 
     def resetParticles(self):
         call("nebula_mpm_reset_particles", self._h)
+
+    # ------------------------------------------------------------ emitters (MPMEngine.h:100-104)
+    def addEmitter(self, em) -> int:
+        a = np.ascontiguousarray(np.asarray(em, dtype=EMITTER_DTYPE).reshape(-1)[:1])
+        k = C.c_uint32()
+        call("nebula_mpm_add_emitter", self._h, _ptr(a), C.byref(k))
+        return k.value
+
+    def clearEmitters(self):
+        call("nebula_mpm_clear_emitters", self._h)
+
+    def getEmitter(self, index: int):
+        """(record, times emitted)."""
+        a = np.zeros(1, EMITTER_DTYPE)
+        d = C.c_int32()
+        call("nebula_mpm_get_emitter", self._h, index, _ptr(a), C.byref(d))
+        return a[0], d.value
 
     def upload_state(self, state: dict):
         arrs = [np.ascontiguousarray(state[f], dtype=np.float32).reshape(-1, 4) for f in FIELDS]

@@ -38,6 +38,13 @@ COLLIDER_DTYPE = np.dtype([
     ("vel", "<f4", (3,)), ("restitution", "<f4"), ("friction", "<f4"), ("pad", "<f4", (3,)),
 ])
 FORCE_DTYPE = np.dtype([("type", "<u2"), ("affectMask", "<u2"), ("data", "<f4", (7,))])
+# nebula_mpm_emitter: the MPM fields of Emitter (src/core/Emitter.h:39-82)
+EMITTER_DTYPE = np.dtype([
+    ("shape", "<u4"), ("center", "<f4", (3,)), ("size", "<f4", (3,)), ("vel", "<f4", (3,)), ("center_vel", "<f4", (3,)),
+    ("particles_per_step", "<i4"), ("particleType", "<u4"), ("emitAlongNormal", "<u4"), ("velocityRandomness", "<f4"),
+    ("step_count", "<i4"), ("particleVolume", "<f4"), ("pad", "<u4"),
+])
+EMIT_AABB, EMIT_SPHERE, EMIT_ELLIPSE = range(3)
 assert MATERIAL_DTYPE.itemsize == 64 and COLLIDER_DTYPE.itemsize == 64 and FORCE_DTYPE.itemsize == 32
 
 FIELDS = ("P", "v", "F0", "F1", "F2", "B0", "B1", "B2")
@@ -125,6 +132,55 @@ def material(model, E, nu, rho0, M_friction=0.0, q_cohesion=0.0, q_max=1e5, bulk
     m["mu"], m["lambda"], m["rho0"], m["model"] = mu, lam, rho0, model
     m["M_friction"], m["q_cohesion"], m["q_max"], m["bulkK"], m["viscosity"] = M_friction, q_cohesion, q_max, bulkK, viscosity
     return m[0]
+
+
+# The reference's presets (src/core/MaterialParams.h:46-103), same parameters.
+def preset_jelly(E=1e4, nu=0.4, rho0=1000.0):
+    return material(MAT_ELASTIC, E, nu, rho0)
+
+
+def preset_sand(E=1e5, nu=0.3, rho0=1600.0):
+    return material(MAT_DRUCKER_PRAGER, E, nu, rho0, M_friction=0.577)
+
+
+def preset_water(rho0=1000.0, bulkK=5e3):
+    m = material(MAT_FLUID, 0.0, 0.0, rho0, bulkK=bulkK, viscosity=0.01)
+    m["mu"], m["lambda"], m["fluidGamma"] = 0.0, 0.0, 7.0
+    return m
+
+
+def preset_mud(E=8e4, nu=0.35, rho0=1800.0):
+    return material(MAT_VISCOPLASTIC_MUD, E, nu, rho0, M_friction=0.4, q_cohesion=5e2, viscosity=0.1)
+
+
+def preset_powder(E=5e4, nu=0.25, rho0=1200.0):
+    return material(MAT_GRANULAR_POWDER, E, nu, rho0, M_friction=0.8, q_cohesion=50.0)
+
+
+def emitter(shape, center, size, vel=(0, 0, 0), particles_per_step=1024, particle_type=1, step_count=-1, center_vel=(0, 0, 0),
+            along_normal=False, randomness=0.0, particle_volume=0.0):
+    """An emitter record (defaults as Emitter, src/core/Emitter.h:41-62)."""
+    e = np.zeros(1, EMITTER_DTYPE)
+    e["shape"], e["center"][0], e["size"][0], e["vel"][0] = shape, center, size, vel
+    e["center_vel"][0], e["particles_per_step"], e["particleType"] = center_vel, particles_per_step, particle_type
+    e["emitAlongNormal"], e["velocityRandomness"], e["step_count"], e["particleVolume"] = int(along_normal), randomness, step_count, particle_volume
+    return e[0]
+
+
+def aabb_emitter(lo, hi, vel, particles_per_step, **kw):
+    """AABBEmitter::FromAABB (Emitter.h:136-143)."""
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    return emitter(EMIT_AABB, (lo + hi) * np.float32(0.5), hi - lo, vel, particles_per_step, **kw)
+
+
+def sphere_emitter(center, radius, vel, particles_per_step, **kw):
+    """SphereEmitter::FromSphere (Emitter.h:184-191)."""
+    return emitter(EMIT_SPHERE, center, (radius, radius, radius), vel, particles_per_step, **kw)
+
+
+def ellipse_emitter(center, semi_a, semi_b, vel, particles_per_step, **kw):
+    """EllipseEmitter's sample() convention: semi-axes along x and y, z fixed."""
+    return emitter(EMIT_ELLIPSE, center, (semi_a, semi_b, 0.0), vel, particles_per_step, **kw)
 
 
 def gravity(g=(0.0, -9.8, 0.0)):
@@ -269,19 +325,26 @@ def shear_block(model=MAT_ELASTIC, seed=1, gamma=20.0, substeps=100, dt=1e-4, fl
     c dt / h = 0.74 and the reference algorithm blows up within ~40 substeps in
     float32 and float64 alike), and an initial shear velocity v_x = gamma (y - 0.7)
     so that F develops distinct singular values.  model: ELASTIC (E=1e4),
-    VON_MISES (E=1e4, q_max=200) or DRUCKER_PRAGER (E=3.5e5, rho 1600, 30 deg)."""
+    VON_MISES (E=1e4, q_max=200), DRUCKER_PRAGER (E=3.5e5, rho 1600, 30 deg),
+    or the reference's presets for GRANULAR_POWDER, FLUID and VISCOPLASTIC_MUD."""
     sc = elastic_block(seed=seed, substeps=substeps, dt=dt, flip_ratio=flip_ratio)
     if model == MAT_DRUCKER_PRAGER:
         m = material(model, 3.5e5, 0.3, 1600.0, M_friction=math.tan(math.radians(30.0)))
     elif model == MAT_VON_MISES:
         m = material(model, 1e4, 0.3, 1000.0, q_max=200.0)
+    elif model == MAT_GRANULAR_POWDER:
+        m = preset_powder()
+    elif model == MAT_FLUID:
+        m = preset_water()
+    elif model == MAT_VISCOPLASTIC_MUD:
+        m = preset_mud()
     else:
         m = material(MAT_ELASTIC, 1e4, 0.3, 1000.0)
     sc.params.materials = [m]
     sc.params.rho0 = float(m["rho0"])
     P = sc.state["P"]
     sc.state["v"][:, 0] = (gamma * (P[:, 1].astype(np.float64) - 0.7)).astype(np.float32)
-    sc.name = "shear_block_%s_8k_64" % ("elastic", "vonmises", "druckerprager")[min(model, 2)]
+    sc.name = "shear_block_%s_8k_64" % ("elastic", "vonmises", "druckerprager", "powder", "fluid", "mud")[model]
     return sc
 
 

@@ -25,7 +25,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SRC = HERE / "mpm_oracle.cpp"
-SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp")
+SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp", HERE / "mpm_emit_oracle.cpp")
 LIB = HERE / "libmpm_oracle.so"
 
 MODES = {"ref32": 0, "mixed": 1, "fp64": 2}
@@ -376,3 +376,13 @@ def fd_slope(loss_at, eps):
     s = np.array([(L[-1] - L[-2]) / eps, (L[0] - L[-1]) / eps, (L[1] - L[0]) / eps, (L[2] - L[1]) / eps])
     keep = np.delete(s, np.argmax(np.abs(s - np.median(s))))
     return float(np.median(keep)), s
+
+
+def emit(record, Vp: float, seed: int, event: int, n: int):
+    """n emitted particles of one emission (mpm_emit_oracle.cpp): (pos4, vel4)."""
+    rec = np.ascontiguousarray(np.asarray(record).reshape(-1)[:1])
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    lib().orc_emit(rec.ctypes.data_as(C.c_void_p), C.c_float(Vp), C.c_uint64(seed), C.c_uint64(event), C.c_uint32(n),
+                   pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p))
+    return pos, vel

@@ -205,7 +205,8 @@ def test_g2p_pass_elastic(flip):
     assert et < 1e-4
 
 
-@pytest.mark.parametrize("model", [S.MAT_DRUCKER_PRAGER, S.MAT_VON_MISES], ids=["drucker_prager", "von_mises"])
+@pytest.mark.parametrize("model", [S.MAT_DRUCKER_PRAGER, S.MAT_VON_MISES, S.MAT_GRANULAR_POWDER, S.MAT_VISCOPLASTIC_MUD],
+                         ids=["drucker_prager", "von_mises", "powder", "mud"])
 def test_g2p_pass_plastic(model):
     """Plastic return maps against the oracle in the CUDA path's precision policy.
     The rebuilt F's orientation and the post-return stress are ill-conditioned in
@@ -255,8 +256,10 @@ def test_trajectory_elastic_block_as_specified_20_substeps():
     assert ex <= 1e-4 and eF <= 1e-4
 
 
-@pytest.mark.parametrize("make", [lambda: S.shear_block(S.MAT_DRUCKER_PRAGER), lambda: S.shear_block(S.MAT_VON_MISES), S.multimaterial],
-                         ids=["dp_shear", "vm_shear", "multimaterial_80k_128"])
+@pytest.mark.parametrize("make", [lambda: S.shear_block(S.MAT_DRUCKER_PRAGER), lambda: S.shear_block(S.MAT_VON_MISES),
+                                  lambda: S.shear_block(S.MAT_GRANULAR_POWDER), lambda: S.shear_block(S.MAT_VISCOPLASTIC_MUD),
+                                  S.multimaterial],
+                         ids=["dp_shear", "vm_shear", "powder_shear", "mud_shear", "multimaterial_80k_128"])
 def test_trajectory_plastic_100_substeps(make):
     sc = make()
     gs, r = run_pair(sc, 100, ["mixed", "ref32"])
@@ -271,6 +274,17 @@ def test_trajectory_plastic_100_substeps(make):
     # sanity bounds only
     assert ex <= 1e-4
     assert ev <= 1e-2 and es <= 5e-3 and ed <= 1e-3
+
+
+def test_trajectory_fluid_100_substeps():
+    """FLUID (the reference's water preset): F = J^(1/3) I and tau = K (J - 1) I
+    (mpm_g2p.comp:158-166); no decomposition, so x and F carry the 1e-4 bar."""
+    sc = S.shear_block(S.MAT_FLUID)
+    gs, r = run_pair(sc, 100, ["ref32", "fp64"])
+    ex, eF = rel_l2(gs["P"][:, :3], r["ref32"]["P"][:, :3]), rel_l2(state_F(gs), state_F(r["ref32"]))
+    print("fluid shear 100 substeps: x %.3e F %.3e vs ref32; x %.3e F %.3e vs fp64" %
+          (ex, eF, rel_l2(gs["P"][:, :3], r["fp64"]["P"][:, :3]), rel_l2(state_F(gs), state_F(r["fp64"]))))
+    assert ex <= 1e-4 and eF <= 1e-4
 
 
 def test_trajectory_sdf_terrain_small():
