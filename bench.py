@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement on the 64-scene mix")
     ap.add_argument("--batch-steps", type=int, default=5, help="timed steps of the batched / plain comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-vs-forward measurement")
+    ap.add_argument("--no-mesh-sdf", action="store_true", help="skip the mesh -> SDF build measurement")
+    ap.add_argument("--mesh-sdf-only", action="store_true", help="only the mesh -> SDF build measurement (one JSON line)")
     return ap.parse_args()
 
 
@@ -369,6 +371,56 @@ def measure_adjoint(steps: int, warmup: int) -> dict:
                     "engine_forward = the brick-sparse engine advancing the same scene (uniform E) for the same substeps"}
 
 
+def measure_mesh_sdf(cpu: bool) -> dict:
+    """The collider SDF built from a triangle mesh on the GPU (nebula_mpm_mesh_sdf,
+    the reference's buildMeshSDF): a 20,480-triangle sphere into the 256^3
+    grid of the slope workload and into a 128^3 grid, timed by CUDA events
+    (median of 3 after one untimed); with `cpu`, the CPU oracle (brute force
+    over cells x triangles, OpenMP) on a 1,280-triangle sphere at 48^3 beside
+    the GPU build of the same case."""
+    import ctypes as C
+
+    import torch
+
+    from nebula_b200 import _capi, mesh
+    from nebula_b200 import scenes as S
+
+    def gpu_ms(tris, res):
+        total = S.hash_cells((res, res, res))
+        t = torch.from_numpy(tris).cuda()
+        out = torch.empty(total, dtype=torch.float32, device="cuda")
+        r = (C.c_uint32 * 3)(res, res, res)
+        s = torch.cuda.current_stream()
+        ms = []
+        for it in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            _capi.call("nebula_mpm_mesh_sdf", C.c_void_p(t.data_ptr()), tris.shape[0], r, total, C.c_float(1.0 / res),
+                       C.c_void_p(out.data_ptr()), C.c_void_p(s.cuda_stream))
+            e1.record(s)
+            torch.cuda.synchronize()
+            if it:
+                ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)), out
+
+    res = {}
+    big = mesh.icosphere((0.5, 0.5, 0.5), 0.3, 5)
+    for n in (256, 128):
+        res["gpu_ms_%d" % n], _ = gpu_ms(big, n)
+        res["cell_triangle_pairs_per_s_%d" % n] = n ** 3 * big.shape[0] / (res["gpu_ms_%d" % n] * 1e-3)
+    res["triangles"] = int(big.shape[0])
+    if cpu:
+        import oracle
+        small = mesh.icosphere((0.5, 0.5, 0.5), 0.3, 3)
+        g, out = gpu_ms(small, 48)
+        t0 = time.perf_counter()
+        ref = oracle.mesh_sdf(small, (48, 48, 48), S.hash_cells((48, 48, 48)), 1.0 / 48)
+        cms = (time.perf_counter() - t0) * 1e3
+        res["sample"] = {"triangles": int(small.shape[0]), "grid": 48, "gpu_ms": g, "cpu_ms": cms, "cpu_cores": oracle.num_threads(),
+                         "max_abs_diff": float(np.abs(out.cpu().numpy() - ref).max())}
+    return res
+
+
 # ----------------------------------------------------------------------------- nebula arm
 def main():
     args = parse()
@@ -393,6 +445,12 @@ def main():
         nbuild.build()
     if dist:
         dist.barrier()
+    if args.mesh_sdf_only:
+        if rank == 0:
+            print(json.dumps({"mesh_sdf": measure_mesh_sdf(world == 1 and not args.no_cpu_baseline)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     from nebula_b200.engine import engine_for_scene
 
     sc = make_scene(args.workload)
@@ -534,6 +592,8 @@ def main():
         line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20, dist)
     if not args.no_adjoint:
         line["adjoint"] = measure_adjoint(3, 2)
+    if not args.no_mesh_sdf:
+        line["mesh_sdf"] = measure_mesh_sdf(rank == 0 and world == 1 and not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -143,6 +143,17 @@ int nebula_mpm_set_collider_sdf(nebula_mpm* e, const float* morton_sdf, uint64_t
 /* MPMEngine::setColliderSphere / clearCollider (MPMEngine.cpp:180-202). */
 int nebula_mpm_set_collider_sphere(nebula_mpm* e, float radius, float cx, float cy, float cz);
 int nebula_mpm_clear_collider(nebula_mpm* e);
+/* setColliderSDF(buildMeshSDF(tris, gridRes, hashCells, cellSize)) (MeshSDF.h:98-132):
+ * the signed distance of every cell centre to a triangle mesh, built on the
+ * GPU into the engine's SDF.  tris: n records of 12 host floats (normal, v0,
+ * v1, v2), the binary STL order (loadBinarySTL, MeshSDF.h:22-43). */
+int nebula_mpm_set_collider_mesh(nebula_mpm* e, const float* tris, uint32_t n);
+/* The moving-obstacle rebuild of examples/pyro_basic.cpp:130-134,
+ * setColliderSDF(buildMeshSDF(transformTriangles(tris, t, q), ...)) with
+ * transformTriangles (MeshSDF.h:134-141) and the build on the device, from the
+ * triangles of the last nebula_mpm_set_collider_mesh: no host transfer.
+ * rotation_wxyz: unit quaternion (w, x, y, z). */
+int nebula_mpm_set_collider_mesh_pose(nebula_mpm* e, const float translation[3], const float rotation_wxyz[4]);
 /* EngineBase::setForces / addForce / clearForces (EngineBase.cpp:22-40):
  * replaces the force table (n <= 16).  No shader is rebuilt: forces are a
  * kernel parameter table. */
@@ -351,6 +362,20 @@ void nebula_mpm_domain_grid_res(const float domainSize[3], float cellSize, uint3
 uint32_t nebula_mpm_domain_cube_res(const uint32_t res[3]);
 uint32_t nebula_mpm_domain_hash_cells(const uint32_t res[3]);
 uint32_t nebula_mpm_domain_n_groups(uint32_t cells);
+
+/* buildMeshSDF (src/core/MeshSDF.h:98-132) on DEVICE buffers: dSdf[totalCells]
+ * (totalCells >= cubeRes^3 of realRes) receives the Morton-ordered signed
+ * distances of the cell centres (ix+0.5, iy+0.5, iz+0.5) * cellSize inside
+ * realRes, 1e9 elsewhere; dTris: nTris records of 12 floats (normal, v0, v1, v2),
+ * 16-byte aligned.  The closest point uses the complete Voronoi-region test
+ * (the reference's closestPtOnTriangle, MeshSDF.h:48-78, omits the edge-BC
+ * region). */
+int nebula_mpm_mesh_sdf(const float* dTris, uint32_t nTris, const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf,
+                        void* stream);
+/* The same of transformTriangles(tris, translation, rotation) (MeshSDF.h:134-141),
+ * the pose applied on the device; a null translation or rotation is the identity. */
+int nebula_mpm_mesh_sdf_posed(const float* dTris, uint32_t nTris, const float translation[3], const float rotation_wxyz[4],
+                              const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream);
 
 /* ---------------------------------------------------------------- single passes
  * One reference dispatch each, on caller-owned DEVICE buffers in the reference

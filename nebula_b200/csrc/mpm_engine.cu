@@ -319,6 +319,36 @@ void MPMEngine::setColliderSphere(float radius, float cx, float cy, float cz) {
 
 void MPMEngine::clearCollider() { hasSdf_ = false; }
 
+// setColliderSDF(buildMeshSDF(tris, gridRes, hashCells, cellSize)) (MeshSDF.h:98-132),
+// the SDF built on the GPU straight into the engine's SDF buffer.  The
+// triangles stay on the device for setColliderMeshPose.
+void MPMEngine::setColliderMesh(const float* tris, uint32_t n) {
+  checkMeshArgs(tris, n);  // the host array needs no alignment: only null / count are checked here
+  prepareHostAccess(false);  // a queued substep may still read the old SDF
+  meshTris_.ensure(std::max<size_t>(size_t(n) * 12 * sizeof(float), 16));
+  if (n) check(cudaMemcpy(meshTris_.ptr, tris, size_t(n) * 12 * sizeof(float), cudaMemcpyHostToDevice), "upload triangles");
+  meshN_ = n;
+  hasMesh_ = true;
+  sdf_.ensure(size_t(hashCells_) * sizeof(float));
+  check(launchMeshSdf(static_cast<const float*>(meshTris_.ptr), n, meshPose(nullptr, nullptr), gridRes_, hashCells_, cfg_.cellSize,
+                      static_cast<float*>(sdf_.ptr), lastStream_, &launches_),
+        "mesh sdf");
+  hasSdf_ = true;
+}
+
+// The moving-obstacle rebuild (examples/pyro_basic.cpp:130-134:
+// setColliderSDF(buildMeshSDF(transformTriangles(base, t, q), ...))) from the
+// triangles of the last setColliderMesh, posed and rebuilt on the device.
+// Ordered on the engine's stream after the substeps already queued.
+void MPMEngine::setColliderMeshPose(const float* translation, const float* rotationWxyz) {
+  if (!hasMesh_) throw Error(NEBULA_MPM_ERR_INVALID, "no collider mesh: call setColliderMesh first");
+  if (!translation || !rotationWxyz) throw Error(NEBULA_MPM_ERR_INVALID, "null pose");
+  check(launchMeshSdf(static_cast<const float*>(meshTris_.ptr), meshN_, meshPose(translation, rotationWxyz), gridRes_, hashCells_,
+                      cfg_.cellSize, static_cast<float*>(sdf_.ptr), lastStream_, &launches_),
+        "mesh sdf");
+  hasSdf_ = true;
+}
+
 void MPMEngine::setForces(const nebula_mpm_force* f, uint32_t n) {
   if (n > uint32_t(kMaxForces)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 16 forces");
   if (n && !f) throw Error(NEBULA_MPM_ERR_INVALID, "null forces");
@@ -862,6 +892,12 @@ int nebula_mpm_set_collider_sdf(nebula_mpm* e, const float* sdf, uint64_t n) {
 }
 int nebula_mpm_set_collider_sphere(nebula_mpm* e, float r, float cx, float cy, float cz) {
   return guarded([&] { E(e).setColliderSphere(r, cx, cy, cz); });
+}
+int nebula_mpm_set_collider_mesh(nebula_mpm* e, const float* tris, uint32_t n) {
+  return guarded([&] { E(e).setColliderMesh(tris, n); });
+}
+int nebula_mpm_set_collider_mesh_pose(nebula_mpm* e, const float translation[3], const float rotation_wxyz[4]) {
+  return guarded([&] { E(e).setColliderMeshPose(translation, rotation_wxyz); });
 }
 int nebula_mpm_clear_collider(nebula_mpm* e) {
   return guarded([&] { E(e).clearCollider(); });

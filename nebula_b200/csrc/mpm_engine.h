@@ -22,6 +22,21 @@ struct Error : std::runtime_error {
 void check(cudaError_t e, const char* what);
 extern thread_local std::string g_last_error;
 
+// Rigid pose applied to a mesh on the device (transformTriangles, MeshSDF.h:134-141):
+// v -> q * v + t, n -> q * n; q a unit quaternion (w, x, y, z).
+struct MeshPose {
+  float q[4];
+  float t[3];
+  bool posed;  // false: the triangles as given
+};
+MeshPose meshPose(const float* translation, const float* rotationWxyz);  // null pointers: identity parts
+void checkMeshArgs(const float* tris, uint32_t nTris);  // null with n > 0, count
+
+// Morton-ordered SDF of a triangle mesh (12 floats per triangle: normal, v0, v1, v2;
+// 16-byte aligned), posed by `pose`.
+cudaError_t launchMeshSdf(const float* dTris, uint32_t n, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
+                          float* dSdf, cudaStream_t s, uint64_t* launches);
+
 void domainGridRes(const float size[3], float h, uint32_t out[3]);
 uint32_t domainCubeRes(const uint32_t res[3]);
 uint32_t domainHashCells(const uint32_t res[3]);
@@ -67,6 +82,8 @@ class MPMEngine {
   void clearAnalyticColliders();
   void setColliderSDF(const float* sdf, uint64_t n);
   void setColliderSphere(float radius, float cx, float cy, float cz);
+  void setColliderMesh(const float* tris, uint32_t n);
+  void setColliderMeshPose(const float* translation, const float* rotationWxyz);
   void clearCollider();
   void setForces(const nebula_mpm_force* f, uint32_t n);
   uint32_t appendParticles(const float* pos4, const float* vel4, uint32_t n);
@@ -151,7 +168,9 @@ class MPMEngine {
   bool denseReady_ = false;
   DevBuf gridMom_, gridMass_;
   DevBuf cellCount_, cellStart_, cellEnd_, key_, rank_, sortedTmp_, sorted_, scanWs_;
-  DevBuf materials_, colliders_, forces_, sdf_, err_;
+  DevBuf materials_, colliders_, forces_, sdf_, err_, meshTris_;
+  uint32_t meshN_ = 0;
+  bool hasMesh_ = false;
   std::vector<Material> hostMaterials_;
   uint32_t colliderCount_ = 0;
   uint32_t colliderTrackLen_ = 1;

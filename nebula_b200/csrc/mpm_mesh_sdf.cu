@@ -1,0 +1,289 @@
+// mpm_mesh_sdf.cu -- mesh -> Morton-ordered SDF on the GPU (buildMeshSDF,
+// src/core/MeshSDF.h:98-132, with transformTriangles, MeshSDF.h:134-141,
+// applied on the device).
+//
+// Same definition as the reference: for every cell centre (ix+0.5, iy+0.5,
+// iz+0.5) * cellSize inside gridRes, the distance to the closest triangle,
+// signed by that triangle's normal (outside when dot(p - cp, n) >= 0); the
+// first triangle wins ties (strict <); cells of the Morton cube beyond gridRes
+// hold 1e9.  The closest point is Ericson's complete region test: the
+// reference's closestPtOnTriangle (MeshSDF.h:48-78) leaves out the edge-BC
+// region and then returns a point outside the triangle (too short, wrongly
+// signed distances); that case is added here.
+//
+// The reference loops over all cells x all triangles on the host.  Here a CTA
+// owns 256 consecutive Morton codes (an 8 x 8 x 4 box of cells), one per
+// thread, and culls the triangle list for the whole box before any thread
+// computes a closest point:
+//   1. U = min over triangles and their vertices of the distance from the
+//      vertex to the farthest cell centre of the box.  Every cell of the box
+//      has a triangle within U, so its closest distance is <= U.
+//   2. The triangles are staged through shared memory in tiles of 256, in
+//      list order.  A triangle whose bounding sphere is farther than U from
+//      the box cannot be any cell's closest and is dropped from the tile; the
+//      survivors are compacted in list order.
+//   3. Each thread walks the survivors, skipping a triangle whose bounding
+//      sphere is no closer than min(its best so far, U).
+// Every skipped triangle is strictly farther than the cell's closest one (the
+// bounds carry a margin above float rounding), so the distances and the
+// winning triangle are those of the brute-force loop.
+#include <cstdint>
+
+#include "mpm_device.cuh"
+#include "mpm_engine.h"
+
+namespace nebula {
+namespace {
+
+constexpr int kThreads = 256;  // = the Morton codes of one 8 x 8 x 4 box
+
+struct TriS {  // a, b - a, c - a, normal, bounding sphere (centre, radius)
+  float ax, ay, az, bx, by, bz, cx, cy, cz, nx, ny, nz, sx, sy, sz, sr;
+};
+
+__device__ __forceinline__ float dot3f(float ax, float ay, float az, float bx, float by, float bz) { return ax * bx + ay * by + az * bz; }
+
+// glm::quat * vec3 for a unit quaternion (w, u): v + 2 (w (u x v) + u x (u x v)).
+__device__ __forceinline__ void rotate(const MeshPose& q, float& vx, float& vy, float& vz) {
+  const float cx = q.q[2] * vz - q.q[3] * vy, cy = q.q[3] * vx - q.q[1] * vz, cz = q.q[1] * vy - q.q[2] * vx;
+  const float dx = q.q[2] * cz - q.q[3] * cy, dy = q.q[3] * cx - q.q[1] * cz, dz = q.q[1] * cy - q.q[2] * cx;
+  vx += (cx * q.q[0] + dx) * 2.0f;
+  vy += (cy * q.q[0] + dy) * 2.0f;
+  vz += (cz * q.q[0] + dz) * 2.0f;
+}
+
+// Triangle k as (normal, v0, v1, v2), the binary STL order, after the pose.
+__device__ __forceinline__ void loadTri(const float4* __restrict__ t4, uint32_t k, const MeshPose& p, float (&v)[12]) {
+  const float4 r0 = __ldg(t4 + 3 * size_t(k)), r1 = __ldg(t4 + 3 * size_t(k) + 1), r2 = __ldg(t4 + 3 * size_t(k) + 2);
+  v[0] = r0.x; v[1] = r0.y; v[2] = r0.z; v[3] = r0.w;
+  v[4] = r1.x; v[5] = r1.y; v[6] = r1.z; v[7] = r1.w;
+  v[8] = r2.x; v[9] = r2.y; v[10] = r2.z; v[11] = r2.w;
+  if (p.posed) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) rotate(p, v[3 * j], v[3 * j + 1], v[3 * j + 2]);
+#pragma unroll
+    for (int j = 1; j < 4; ++j) {
+      v[3 * j] += p.t[0];
+      v[3 * j + 1] += p.t[1];
+      v[3 * j + 2] += p.t[2];
+    }
+  }
+}
+
+// Closest point of triangle (a, a + ab, a + ac) to p (MeshSDF.h:48-78).
+__device__ __forceinline__ void closestOnTriangle(const TriS& t, float px, float py, float pz, float& qx, float& qy, float& qz) {
+  const float apx = px - t.ax, apy = py - t.ay, apz = pz - t.az;
+  const float d1 = dot3f(t.bx, t.by, t.bz, apx, apy, apz), d2 = dot3f(t.cx, t.cy, t.cz, apx, apy, apz);
+  if (d1 <= 0.f && d2 <= 0.f) {
+    qx = t.ax; qy = t.ay; qz = t.az;
+    return;
+  }
+  const float bpx = apx - t.bx, bpy = apy - t.by, bpz = apz - t.bz;  // p - b
+  const float d3 = dot3f(t.bx, t.by, t.bz, bpx, bpy, bpz), d4 = dot3f(t.cx, t.cy, t.cz, bpx, bpy, bpz);
+  if (d3 >= 0.f && d4 <= d3) {
+    qx = t.ax + t.bx; qy = t.ay + t.by; qz = t.az + t.bz;
+    return;
+  }
+  const float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+    const float v = d1 / (d1 - d3);
+    qx = t.ax + v * t.bx; qy = t.ay + v * t.by; qz = t.az + v * t.bz;
+    return;
+  }
+  const float cpx = apx - t.cx, cpy = apy - t.cy, cpz = apz - t.cz;  // p - c
+  const float d5 = dot3f(t.bx, t.by, t.bz, cpx, cpy, cpz), d6 = dot3f(t.cx, t.cy, t.cz, cpx, cpy, cpz);
+  if (d6 >= 0.f && d5 <= d6) {
+    qx = t.ax + t.cx; qy = t.ay + t.cy; qz = t.az + t.cz;
+    return;
+  }
+  const float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+    const float w = d2 / (d2 - d6);
+    qx = t.ax + w * t.cx; qy = t.ay + w * t.cy; qz = t.az + w * t.cz;
+    return;
+  }
+  const float va = d3 * d6 - d5 * d4;
+  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {  // edge BC (Ericson 5.1.5; left out by MeshSDF.h:76-78)
+    const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    qx = t.ax + t.bx + w * (t.cx - t.bx); qy = t.ay + t.by + w * (t.cy - t.by); qz = t.az + t.bz + w * (t.cz - t.bz);
+    return;
+  }
+  const float sum = va + vb + vc;
+  const float v = vb / sum, w = vc / sum;
+  qx = t.ax + v * t.bx + w * t.cx;
+  qy = t.ay + v * t.by + w * t.cy;
+  qz = t.az + v * t.bz + w * t.cz;
+}
+
+__global__ void __launch_bounds__(kThreads) k_mesh_sdf(const float4* __restrict__ tris, uint32_t n, MeshPose pose, int rx, int ry, int rz,
+                                                       uint32_t totalCells, float cs, float eps, float* __restrict__ sdf) {
+  __shared__ TriS tile[kThreads];
+  __shared__ uint32_t warpCount[kThreads / 32];
+  __shared__ uint32_t boundBits;
+  const uint32_t base = blockIdx.x * kThreads;
+  const uint32_t code = base + threadIdx.x;
+  int bx0, by0, bz0;
+  mortonDecode(base, bx0, by0, bz0);
+  if (bx0 >= rx || by0 >= ry || bz0 >= rz) {  // the whole box lies in the padding of the Morton cube
+    if (code < totalCells) sdf[code] = 1e9f;
+    return;
+  }
+  int bx1, by1, bz1;
+  mortonDecode(base | uint32_t(kThreads - 1), bx1, by1, bz1);
+  const float lox = (float(bx0) + 0.5f) * cs, loy = (float(by0) + 0.5f) * cs, loz = (float(bz0) + 0.5f) * cs;
+  const float hix = (float(min(bx1, rx - 1)) + 0.5f) * cs, hiy = (float(min(by1, ry - 1)) + 0.5f) * cs, hiz = (float(min(bz1, rz - 1)) + 0.5f) * cs;
+
+  // 1. U^2 over the box
+  if (threadIdx.x == 0) boundBits = __float_as_uint(INFINITY);
+  __syncthreads();
+  float u2 = INFINITY;
+  for (uint32_t k = threadIdx.x; k < n; k += kThreads) {
+    float v[12];
+    loadTri(tris, k, pose, v);
+#pragma unroll
+    for (int j = 1; j < 4; ++j) {
+      const float ex = fmaxf(v[3 * j] - lox, hix - v[3 * j]);
+      const float ey = fmaxf(v[3 * j + 1] - loy, hiy - v[3 * j + 1]);
+      const float ez = fmaxf(v[3 * j + 2] - loz, hiz - v[3 * j + 2]);
+      u2 = fminf(u2, ex * ex + ey * ey + ez * ez);
+    }
+  }
+  u2 = __uint_as_float(__reduce_min_sync(0xffffffffu, __float_as_uint(u2)));  // non-negative floats order as their bits
+  if ((threadIdx.x & 31) == 0) atomicMin(&boundBits, __float_as_uint(u2));
+  __syncthreads();
+  const float U = sqrtf(__uint_as_float(boundBits)) * (1.0f + 1e-5f) + eps;
+
+  int ix = 0, iy = 0, iz = 0;
+  if (code < totalCells) mortonDecode(code, ix, iy, iz);
+  const bool inside = code < totalCells && ix < rx && iy < ry && iz < rz;
+  const float px = (float(ix) + 0.5f) * cs, py = (float(iy) + 0.5f) * cs, pz = (float(iz) + 0.5f) * cs;
+  float best = 1e9f;
+  bool outer = true;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t t0 = 0; t0 < n; t0 += kThreads) {
+    // 2. stage the tile's triangles that can be closest to some cell of the box
+    const uint32_t k = t0 + threadIdx.x;
+    TriS t;
+    bool keep = false;
+    if (k < n) {
+      float v[12];
+      loadTri(tris, k, pose, v);
+      t.nx = v[0]; t.ny = v[1]; t.nz = v[2];
+      t.ax = v[3]; t.ay = v[4]; t.az = v[5];
+      t.bx = v[6] - v[3]; t.by = v[7] - v[4]; t.bz = v[8] - v[5];
+      t.cx = v[9] - v[3]; t.cy = v[10] - v[4]; t.cz = v[11] - v[5];
+      t.sx = (v[3] + v[6] + v[9]) * (1.0f / 3.0f);
+      t.sy = (v[4] + v[7] + v[10]) * (1.0f / 3.0f);
+      t.sz = (v[5] + v[8] + v[11]) * (1.0f / 3.0f);
+      float rr = 0.f;
+#pragma unroll
+      for (int j = 1; j < 4; ++j) {
+        const float dx = v[3 * j] - t.sx, dy = v[3 * j + 1] - t.sy, dz = v[3 * j + 2] - t.sz;
+        rr = fmaxf(rr, dx * dx + dy * dy + dz * dz);
+      }
+      t.sr = sqrtf(rr) * 1.0001f + eps;  // covers the triangle despite rounding
+      const float gx = fmaxf(fmaxf(lox - t.sx, t.sx - hix), 0.f), gy = fmaxf(fmaxf(loy - t.sy, t.sy - hiy), 0.f),
+                  gz = fmaxf(fmaxf(loz - t.sz, t.sz - hiz), 0.f);
+      keep = sqrtf(gx * gx + gy * gy + gz * gz) - t.sr <= U;
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+    __syncthreads();  // the previous tile has been consumed
+    if (lane == 0) warpCount[warp] = __popc(mask);
+    __syncthreads();
+    uint32_t off = 0, m = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+      const uint32_t c = warpCount[w];
+      off += uint32_t(w) < warp ? c : 0u;
+      m += c;
+    }
+    if (keep) tile[off + __popc(mask & ((1u << lane) - 1u))] = t;
+    __syncthreads();
+    if (!inside) continue;
+    // 3. closest points against the survivors, in list order
+    for (uint32_t j = 0; j < m; ++j) {
+      const TriS& s = tile[j];
+      const float ex = px - s.sx, ey = py - s.sy, ez = pz - s.sz;
+      const float dc = sqrtf(ex * ex + ey * ey + ez * ez);
+      if (dc - s.sr >= fminf(best, U)) continue;  // every point of the triangle is at least this far
+      float qx, qy, qz;
+      closestOnTriangle(s, px, py, pz, qx, qy, qz);
+      const float dx = px - qx, dy = py - qy, dz = pz - qz;
+      const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+      if (d < best) {
+        best = d;
+        outer = dot3f(dx, dy, dz, s.nx, s.ny, s.nz) >= 0.f;
+      }
+    }
+  }
+  if (code < totalCells) sdf[code] = inside ? (outer ? best : -best) : 1e9f;
+}
+
+}  // namespace
+
+cudaError_t launchMeshSdf(const float* dTris, uint32_t n, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
+                          float* dSdf, cudaStream_t s, uint64_t* launches) {
+  if (totalCells == 0) return cudaSuccess;
+  // Margin of the culling bounds over float rounding: distances within the
+  // domain are O(cellSize * cubeRes).
+  const float extent = cellSize * float(domainCubeRes(res));
+  const float eps = 1e-5f * fmaxf(extent, 1.0f);
+  k_mesh_sdf<<<(totalCells + kThreads - 1) / kThreads, kThreads, 0, s>>>(reinterpret_cast<const float4*>(dTris), n, pose, int(res[0]),
+                                                                         int(res[1]), int(res[2]), totalCells, cellSize, eps, dSdf);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+MeshPose meshPose(const float* translation, const float* rotationWxyz) {
+  MeshPose p{};
+  p.q[0] = 1.0f;
+  if (translation)
+    for (int i = 0; i < 3; ++i) p.t[i] = translation[i];
+  if (rotationWxyz)
+    for (int i = 0; i < 4; ++i) p.q[i] = rotationWxyz[i];
+  p.posed = translation != nullptr || rotationWxyz != nullptr;
+  return p;
+}
+
+void checkMeshArgs(const float* tris, uint32_t nTris) {
+  if (nTris && !tris) throw Error(NEBULA_MPM_ERR_INVALID, "null triangles");
+  if (nTris > (1u << 26)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 2^26 triangles");
+}
+
+}  // namespace nebula
+
+using namespace nebula;
+
+extern "C" {
+
+int nebula_mpm_mesh_sdf(const float* dTris, uint32_t nTris, const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf,
+                        void* stream) {
+  return nebula_mpm_mesh_sdf_posed(dTris, nTris, nullptr, nullptr, realRes, totalCells, cellSize, dSdf, stream);
+}
+
+int nebula_mpm_mesh_sdf_posed(const float* dTris, uint32_t nTris, const float translation[3], const float rotationWxyz[4],
+                              const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream) {
+  try {
+    if (!realRes || !dSdf) throw Error(NEBULA_MPM_ERR_INVALID, "null argument");
+    checkMeshArgs(dTris, nTris);
+    if (reinterpret_cast<uintptr_t>(dTris) % 16u) throw Error(NEBULA_MPM_ERR_INVALID, "triangles must be 16-byte aligned");
+    if (!(cellSize > 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "cellSize must be > 0");
+    if (!realRes[0] || !realRes[1] || !realRes[2]) throw Error(NEBULA_MPM_ERR_INVALID, "realRes must be >= 1");
+    const uint32_t cube = domainCubeRes(realRes);
+    if (cube > 1024u || uint64_t(totalCells) < uint64_t(cube) * cube * cube)
+      throw Error(NEBULA_MPM_ERR_INVALID, "totalCells must hold the Morton cube of realRes (cubeRes <= 1024)");
+    uint64_t l = 0;
+    check(launchMeshSdf(dTris, nTris, meshPose(translation, rotationWxyz), realRes, totalCells, cellSize, dSdf,
+                        static_cast<cudaStream_t>(stream), &l),
+          "mesh sdf");
+    return NEBULA_MPM_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return NEBULA_MPM_ERR_INVALID;
+  }
+}
+
+}  // extern "C"

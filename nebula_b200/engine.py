@@ -146,6 +146,19 @@ class MPMEngine:
     def clearCollider(self):
         call("nebula_mpm_clear_collider", self._h)
 
+    def setColliderMesh(self, tris):
+        """setColliderSDF(buildMeshSDF(tris, ...)) with the SDF built on the GPU; tris (n, 12)."""
+        a = np.ascontiguousarray(tris, dtype=np.float32).reshape(-1, 12)
+        call("nebula_mpm_set_collider_mesh", self._h, _ptr(a), a.shape[0])
+
+    def setColliderMeshPose(self, translation, rotation=(1.0, 0.0, 0.0, 0.0)):
+        """setColliderSDF(buildMeshSDF(transformTriangles(tris, translation,
+        rotation))) for the triangles of the last setColliderMesh, on the
+        device; rotation is a unit quaternion (w, x, y, z)."""
+        t = np.ascontiguousarray(translation, dtype=np.float32).reshape(3)
+        q = np.ascontiguousarray(rotation, dtype=np.float32).reshape(4)
+        call("nebula_mpm_set_collider_mesh_pose", self._h, _ptr(t), _ptr(q))
+
     def setForces(self, forces):
         self._forces = list(forces)
         a = np.zeros(max(1, len(self._forces)), FORCE_DTYPE)

@@ -25,7 +25,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SRC = HERE / "mpm_oracle.cpp"
-SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp", HERE / "mpm_emit_oracle.cpp")
+SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp", HERE / "mpm_emit_oracle.cpp", HERE / "mpm_mesh_sdf_oracle.cpp")
 LIB = HERE / "libmpm_oracle.so"
 
 MODES = {"ref32": 0, "mixed": 1, "fp64": 2}
@@ -386,3 +386,15 @@ def emit(record, Vp: float, seed: int, event: int, n: int):
     lib().orc_emit(rec.ctypes.data_as(C.c_void_p), C.c_float(Vp), C.c_uint64(seed), C.c_uint64(event), C.c_uint32(n),
                    pos.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p))
     return pos, vel
+
+
+def mesh_sdf(tris, res, total_cells: int, cell_size: float, complete: bool = True):
+    """buildMeshSDF restated on the CPU (mpm_mesh_sdf_oracle.cpp): Morton-ordered
+    float32 SDF; complete=False reproduces the reference's closest-point steps
+    (edge-BC region left out)."""
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 12)
+    r = np.ascontiguousarray(res, np.uint32)
+    out = np.empty(int(total_cells), np.float32)
+    lib().orc_mesh_sdf(t.ctypes.data_as(C.c_void_p), C.c_uint32(t.shape[0]), r.ctypes.data_as(C.c_void_p), C.c_uint32(int(total_cells)),
+                       C.c_float(cell_size), out.ctypes.data_as(C.c_void_p), C.c_int(int(bool(complete))))
+    return out

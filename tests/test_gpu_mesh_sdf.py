@@ -1,0 +1,113 @@
+"""Mesh -> SDF on the GPU (nebula_mpm_mesh_sdf, nebula_mpm_set_collider_mesh)
+against the CPU oracle (complete closest-point test; see
+tests/test_mesh_sdf_oracle.py for the reference's defect)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from nebula_b200 import _capi, mesh
+from nebula_b200 import scenes as S
+from nebula_b200.engine import engine_for_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_mesh_sdf(tris, res, total, h):
+    t = torch.from_numpy(np.ascontiguousarray(tris, np.float32)).cuda()
+    out = torch.empty(total, dtype=torch.float32, device="cuda")
+    r = (C.c_uint32 * 3)(*res)
+    _capi.call("nebula_mpm_mesh_sdf", C.c_void_p(t.data_ptr()), tris.shape[0], r, total, C.c_float(h), C.c_void_p(out.data_ptr()),
+               C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["sphere_32", "torus_48", "sphere_non_cubic", "coarse_sphere_80"])
+def test_mesh_sdf_matches_oracle(case):
+    if case == "coarse_sphere_80":  # fewer triangles than one shared-memory tile
+        tris, res, total, h = mesh.icosphere((0.45, 0.5, 0.55), 0.3, 1), (20, 20, 20), 32 ** 3, 1 / 20
+    elif case == "sphere_32":
+        tris, res, total, h = mesh.icosphere((0.5, 0.5, 0.5), 0.25, 3), (32, 32, 32), 32 ** 3, 1 / 32
+    elif case == "torus_48":
+        tris, res, total, h = mesh.torus((0.5, 0.5, 0.5), 0.25, 0.08, 48, 24), (48, 48, 48), 64 ** 3, 1 / 48
+    else:
+        tris, res, total, h = mesh.icosphere((0.4, 0.5, 0.6), 0.2, 2), (24, 40, 32), 64 ** 3, 1 / 40
+    got = gpu_mesh_sdf(tris, res, total, h)
+    want = oracle.mesh_sdf(tris, res, total, h)
+    assert np.all((got == np.float32(1e9)) == (want == np.float32(1e9)))
+    assert np.abs(got - want).max() < 1e-5
+    clear = np.abs(want) > 1e-5
+    assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
+
+
+def test_posed_mesh_sdf_matches_oracle_of_moved_mesh():
+    """transformTriangles on the device (nebula_mpm_mesh_sdf_posed) against the
+    oracle of the mesh moved on the host: a torus tilted 30 degrees about x."""
+    tris = mesh.torus((0.0, 0.0, 0.0), 0.22, 0.07, 40, 20)
+    t = np.array([0.5, 0.45, 0.52], np.float32)
+    half = np.radians(15.0)
+    q = np.array([np.cos(half), np.sin(half), 0.0, 0.0], np.float32)
+    res, total, h = (40, 40, 40), 64 ** 3, 1 / 40
+    d = torch.from_numpy(tris).cuda()
+    out = torch.empty(total, dtype=torch.float32, device="cuda")
+    r = (C.c_uint32 * 3)(*res)
+    _capi.call("nebula_mpm_mesh_sdf_posed", C.c_void_p(d.data_ptr()), tris.shape[0], t.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p),
+               r, total, C.c_float(h), C.c_void_p(out.data_ptr()), None)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    want = oracle.mesh_sdf(mesh.transform_triangles(tris, t, q), res, total, h)
+    assert np.abs(got - want).max() < 1e-5
+    clear = np.abs(want) > 1e-5
+    assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
+
+
+def test_engine_mesh_pose_equals_uploaded_sdf_of_moved_mesh():
+    """setColliderMeshPose rebuilds the engine's SDF from its device copy of
+    the mesh: the same trajectory as setColliderSDF(oracle SDF of the mesh
+    moved on the host), and a second pose replaces the first."""
+    sc = S.shear_block()
+    base = mesh.icosphere((0.0, 0.0, 0.0), 0.12, 3)
+    res, sp = sc.params.grid_res, sc.params
+    a = engine_for_scene(sc)
+    a.setColliderMesh(base)
+    a.setColliderMeshPose((0.3, 0.3, 0.3), (1.0, 0.0, 0.0, 0.0))  # replaced by the next pose
+    q = (np.cos(0.2), 0.0, np.sin(0.2), 0.0)
+    a.setColliderMeshPose((0.5, 0.45, 0.5), q)
+    b = engine_for_scene(sc)
+    b.setColliderSDF(oracle.mesh_sdf(mesh.transform_triangles(base, (0.5, 0.45, 0.5), q), res, sp.hash_cells, sp.cell_size))
+    for e in (a, b):
+        e.run_substeps(sp.dt, 40)
+    pa, pb = a.download("P")[:, :3], b.download("P")[:, :3]
+    assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-5
+    with pytest.raises(_capi.NebulaError):
+        engine_for_scene(sc).setColliderMeshPose((0.5, 0.5, 0.5))  # no mesh yet
+
+
+def test_engine_collider_mesh_equals_uploaded_sdf():
+    """An engine whose collider SDF is built on the GPU from a mesh behaves as
+    one given the oracle's SDF of the same mesh."""
+    sc = S.shear_block()
+    tris = mesh.icosphere((0.5, 0.45, 0.5), 0.12, 3)
+    res = sc.params.grid_res
+    sdf = oracle.mesh_sdf(tris, res, sc.params.hash_cells, sc.params.cell_size)
+    a = engine_for_scene(sc)
+    b = engine_for_scene(sc)
+    a.setColliderMesh(tris)
+    b.setColliderSDF(sdf)
+    for e in (a, b):
+        e.run_substeps(sc.params.dt, 40)
+    pa, pb = a.download("P")[:, :3], b.download("P")[:, :3]
+    assert np.linalg.norm(pa - pb) / np.linalg.norm(pb) < 1e-5
+
+
+def test_empty_mesh_and_argument_checks():
+    got = gpu_mesh_sdf(np.zeros((0, 12), np.float32), (8, 8, 8), 8 ** 3, 0.125)
+    assert np.all(got == np.float32(1e9))  # buildMeshSDF: minD starts at 1e9
+    out = torch.empty(8 ** 3, dtype=torch.float32, device="cuda")
+    r = (C.c_uint32 * 3)(8, 8, 8)
+    for total, h in ((8 ** 3 - 1, 0.125), (8 ** 3, 0.0)):
+        with pytest.raises(_capi.NebulaError):
+            _capi.call("nebula_mpm_mesh_sdf", None, 0, r, total, C.c_float(h), C.c_void_p(out.data_ptr()), None)
