@@ -421,6 +421,59 @@ def measure_mesh_sdf(cpu: bool) -> dict:
     return res
 
 
+def measure_pbf_hash(cpu: bool) -> dict:
+    """The PBF engine's spatial hash on the shared counting sort
+    (nebula_hash_bin): the default FluidEngine buffer (160,592 slots, 30,000 of
+    them unused, 64^3 cells; L2-resident and launch-bound) and 8,388,608
+    uniform particles on 128^3 cells (160 MB of inputs, larger than L2), timed
+    by CUDA events (median of 20 after 3 untimed).  Algorithmic bytes per build: 20 per slot
+    (predP + typeFlag read), 4 per included particle (sortedIdx), 12 per cell
+    (cellCount zeroed and written, cellOffset written)."""
+    import torch
+
+    from nebula_b200 import hash as H
+
+    def timed(grid, p, f):
+        hs = H.SpatialHash(grid, len(p))
+        pt = torch.from_numpy(p).cuda()
+        ft = torch.from_numpy(f.view(np.int32)).cuda()
+        s = torch.cuda.current_stream()
+        ms = []
+        for it in range(23):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            hs.build(pt, ft, s)
+            e1.record(s)
+            torch.cuda.synchronize()
+            if it >= 3:
+                ms.append(e0.elapsed_time(e1))
+        t = float(np.median(ms))
+        m = int((f != H.TYPE_FLAG_UNUSED).sum())
+        byts = 20.0 * len(p) + 4.0 * m + 12.0 * grid.hash_cells
+        return {"slots": len(p), "included": m, "hash_cells": grid.hash_cells, "ms": t, "particles_per_s": len(p) / (t * 1e-3),
+                "algorithmic_bytes": byts, "gbs": byts / (t * 1e-3) / 1e9}
+
+    out = {}
+    p, f = H.fluid_layout()
+    out["fluid_default"] = timed(H.FluidGrid(), p, f)
+    rng = np.random.default_rng(12)
+    n = 1 << 23
+    q = np.zeros((n, 4), np.float32)
+    q[:, :3] = rng.uniform(0.0, 20.0, (n, 3)).astype(np.float32)
+    fq = np.zeros(n, np.uint32)
+    out["uniform_8m_128"] = timed(H.FluidGrid(cell_size=20.0 / 128.0), q, fq)
+    out["uniform_8m_128"]["hbm_frac_of_measured"] = out["uniform_8m_128"]["gbs"] / peaks()[0]
+    if cpu:
+        import oracle
+        g = H.FluidGrid()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            oracle.hash_bin(p, f, g.world_min, g.cell_size, g.grid_res, g.hash_cells)
+        out["cpu_fluid_default_ms"] = (time.perf_counter() - t0) * 1e3 / 5
+        out["cpu_note"] = "CPU oracle, one thread, same buffer"
+    return out
+
+
 # ----------------------------------------------------------------------------- nebula arm
 def main():
     args = parse()
@@ -447,7 +500,8 @@ def main():
         dist.barrier()
     if args.mesh_sdf_only:
         if rank == 0:
-            print(json.dumps({"mesh_sdf": measure_mesh_sdf(world == 1 and not args.no_cpu_baseline)}), flush=True)
+            print(json.dumps({"mesh_sdf": measure_mesh_sdf(world == 1 and not args.no_cpu_baseline),
+                              "pbf_hash": measure_pbf_hash(world == 1 and not args.no_cpu_baseline)}), flush=True)
         if dist:
             dist.destroy_process_group()
         return
@@ -594,6 +648,7 @@ def main():
         line["adjoint"] = measure_adjoint(3, 2)
     if not args.no_mesh_sdf:
         line["mesh_sdf"] = measure_mesh_sdf(rank == 0 and world == 1 and not args.no_cpu_baseline)
+        line["pbf_hash"] = measure_pbf_hash(rank == 0 and world == 1 and not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

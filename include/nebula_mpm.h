@@ -437,6 +437,33 @@ int nebula_mpm_grid_update(const nebula_mpm_pass* pass, float* dGridMom, const f
 int nebula_mpm_g2p(const nebula_mpm_pass* pass, const nebula_mpm_particles* parts, const float* dGridMom, const float* dGridMass,
                    const nebula_mpm_material* dMaterials, const float* dSdf, void* stream);
 
+/* ---------------------------------------------------------------- PBF spatial hash
+ * The same counting sort serving the PBF fluid engine's neighbour search:
+ * zero_cells + hash_count + hash_scan_local/global + hash_add_base + hash_sort
+ * (shaders/hash_count.comp, hash_scan_*.comp, hash_add_base.comp,
+ * hash_sort.comp; dispatched by FluidEngine.cpp:445-474 and
+ * tests/helpers/PBFHarness.cpp:153-180).  Cell of a particle = Morton code of
+ * clamp((predP.xyz - worldMin) / cellSize, 0, gridRes - 1) truncated
+ * (common.glsl:100-105).  Particles whose typeFlag is 6 (TYPE_FLAG_UNUSED,
+ * empty boundary slots) are left out (hash_count.comp:9-16,
+ * hash_sort.comp:14-17); dTypeFlag may be NULL (nothing left out).
+ * Outputs, in the state the pbf_* shaders read them: cellCount[hashCells];
+ * cellOffset[hashCells] = END of each cell's range (hash_sort consumes the
+ * exclusive offsets, so readers take start = cellOffset - cellCount,
+ * pbf_density.comp:50-51); sortedIdx[0, m) the m included particles, in
+ * ascending index inside each cell (the shader's order is that of its
+ * atomics); sortedIdx[m, particleCount) is not written.  The scan covers any
+ * hashCells (hash_scan_global.comp handles at most 1,024 group sums). */
+typedef struct nebula_hash_grid {
+  float worldMin[3];
+  float cellSize;
+  uint32_t gridRes[3];
+  uint32_t hashCells; /* >= cubeRes^3 of gridRes */
+} nebula_hash_grid;
+size_t nebula_hash_bin_workspace_size(uint32_t hashCells, uint32_t particleCount);
+int nebula_hash_bin(const nebula_hash_grid* grid, const float* dPredP4, const uint32_t* dTypeFlag, uint32_t particleCount,
+                    uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSortedIdx, void* dWorkspace, size_t workspaceBytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -140,6 +140,9 @@ _SIGS = {
     "nebula_mpm_domain_hash_cells": (C.c_uint32, [C.c_uint32 * 3]),
     "nebula_mpm_domain_n_groups": (C.c_uint32, [C.c_uint32]),
     "nebula_mpm_bin_workspace_size": (C.c_size_t, [C.c_uint32, C.c_uint32]),
+    "nebula_hash_bin_workspace_size": (C.c_size_t, [C.c_uint32, C.c_uint32]),
+    "nebula_hash_bin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                  C.c_void_p]),
     "nebula_mpm_bin": (C.c_int, [C.POINTER(Pass), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     "nebula_mpm_bin_noalloc_max_cells": (C.c_size_t, []),
     "nebula_mpm_bin_noalloc_max_particles": (C.c_size_t, []),

@@ -3,7 +3,9 @@
 // Each call runs one reference dispatch on caller-owned device buffers in the
 // reference layout, the per-pass surface of the reference's test harness
 // (MPMHarness::runZeroGrid / runP2G / runGridUpdate / runG2P and
-// buildHashGridCPU, tests/helpers/MPMHarness.cpp:132-178, 260-282).
+// buildHashGridCPU, tests/helpers/MPMHarness.cpp:132-178, 260-282), plus the
+// PBF engine's spatial hash on the same counting sort (nebula_hash_bin).
+#include <cmath>
 #include <cstring>
 
 #include "mpm_engine.h"
@@ -128,6 +130,52 @@ int nebula_mpm_bin(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dC
     uint64_t launches = 0;
     SubstepParams P = fromPass(*pass, nullptr, nullptr, nullptr, nullptr);
     check(launchBin(P, reinterpret_cast<const float4*>(dPos4), n, b, s, &launches), "bin");
+  });
+}
+
+size_t nebula_hash_bin_workspace_size(uint32_t hashCells, uint32_t particleCount) { return binLayout(hashCells, particleCount).total; }
+
+int nebula_hash_bin(const nebula_hash_grid* grid, const float* dPredP4, const uint32_t* dTypeFlag, uint32_t particleCount,
+                    uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSortedIdx, void* dWorkspace, size_t workspaceBytes, void* stream) {
+  return guarded([&] {
+    if (!grid) throw Error(NEBULA_MPM_ERR_INVALID, "null grid");
+    if (!(grid->cellSize > 0.f) || !std::isfinite(grid->cellSize)) throw Error(NEBULA_MPM_ERR_INVALID, "cellSize must be finite and > 0");
+    for (int a = 0; a < 3; ++a) {
+      if (grid->gridRes[a] == 0) throw Error(NEBULA_MPM_ERR_INVALID, "gridRes must be >= 1");
+      if (!std::isfinite(grid->worldMin[a])) throw Error(NEBULA_MPM_ERR_INVALID, "worldMin must be finite");
+    }
+    const uint32_t cube = domainCubeRes(grid->gridRes);
+    if (cube > 1024u || uint64_t(grid->hashCells) < uint64_t(cube) * cube * cube)
+      throw Error(NEBULA_MPM_ERR_INVALID, "hashCells must hold the Morton cube of gridRes (cubeRes <= 1024)");
+    const uint32_t n = particleCount;
+    BinWorkspaceLayout L = binLayout(grid->hashCells, n);
+    if (!dWorkspace || workspaceBytes < L.total) throw Error(NEBULA_MPM_ERR_INVALID, "hash workspace too small");
+    if (!dCellCount || !dCellOffset || (n && (!dPredP4 || !dSortedIdx))) throw Error(NEBULA_MPM_ERR_INVALID, "null buffer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* ws = static_cast<char*>(dWorkspace);
+    BinBuffers b;
+    b.cellCount = dCellCount;
+    b.cellStart = reinterpret_cast<uint32_t*>(ws + L.cellStart);
+    b.cellEnd = dCellOffset;
+    b.key = reinterpret_cast<uint32_t*>(ws + L.key);
+    b.rank = reinterpret_cast<uint32_t*>(ws + L.rank);
+    b.sortedTmp = reinterpret_cast<uint32_t*>(ws + L.sortedTmp);
+    b.sorted = dSortedIdx;
+    b.tileState = reinterpret_cast<unsigned long long*>(ws + L.tiles);
+    b.tileCounter = reinterpret_cast<uint32_t*>(b.tileState + scanTiles(grid->hashCells));
+    b.err = reinterpret_cast<uint32_t*>(ws + L.err);
+    b.typeFlag = dTypeFlag;
+    check(cudaMemsetAsync(b.err, 0, 4, s), "memset");
+    SubstepParams P{};
+    P.cellSize = grid->cellSize;
+    for (int a = 0; a < 3; ++a) {
+      P.gridRes[a] = int(grid->gridRes[a]);
+      P.worldMin[a] = grid->worldMin[a];
+    }
+    P.cubeRes = cube;
+    P.hashCells = grid->hashCells;
+    uint64_t launches = 0;
+    check(launchBin(P, reinterpret_cast<const float4*>(dPredP4), n, b, s, &launches), "hash bin");
   });
 }
 

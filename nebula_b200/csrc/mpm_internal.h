@@ -30,7 +30,11 @@ struct BinBuffers {
   unsigned long long* tileState;  // scanTiles(hashCells) words
   uint32_t* tileCounter;
   uint32_t* err;
+  // Optional per-particle type flags: particles flagged kTypeFlagUnused stay
+  // out of the bins (the PBF binning, hash_count.comp:9-16).
+  const uint32_t* typeFlag = nullptr;
 };
+constexpr uint32_t kTypeFlagUnused = 6u;
 
 // Bytes of scan workspace (tile status words + counter) for `n` items.
 size_t scanWorkspaceBytes(uint64_t n);

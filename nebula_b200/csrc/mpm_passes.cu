@@ -16,11 +16,17 @@ constexpr int kThreads = 256;
 
 inline uint32_t blocksFor(uint64_t n, int t = kThreads) { return uint32_t((n + t - 1) / t); }
 
-// mpm_hash_count.comp:7-14 (+ the slot the sort would take)
-__global__ void __launch_bounds__(kThreads) k_bin_count(SubstepParams P, const float4* __restrict__ pos, uint32_t n, uint32_t* cellCount,
-                                                        uint32_t* key, uint32_t* rank) {
+constexpr uint32_t kKeyExcluded = 0xffffffffu;
+
+// mpm_hash_count.comp:7-14 / hash_count.comp:7-20 (+ the slot the sort would take)
+__global__ void __launch_bounds__(kThreads) k_bin_count(SubstepParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ typeFlag,
+                                                        uint32_t n, uint32_t* cellCount, uint32_t* key, uint32_t* rank) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (typeFlag && typeFlag[i] == kTypeFlagUnused) {
+    key[i] = kKeyExcluded;
+    return;
+  }
   float4 p = pos[i];
   int cx, cy, cz;
   cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
@@ -41,7 +47,9 @@ __global__ void __launch_bounds__(kThreads) k_bin_scatter(uint32_t n, const uint
                                                           const uint32_t* __restrict__ cellStart, uint32_t* sortedTmp, uint32_t* err) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint32_t slot = cellStart[key[i]] + rank[i];
+  const uint32_t c = key[i];
+  if (c == kKeyExcluded) return;
+  const uint32_t slot = cellStart[c] + rank[i];
   if (slot < n) sortedTmp[slot] = i;
   else atomicOr(err, kErrBinRange);  // only after an expired scan wait
 }
@@ -60,6 +68,25 @@ __global__ void __launch_bounds__(kThreads) k_bin_canon(uint32_t n, const uint32
   }
   uint32_t c = key[i];
   uint32_t st = cellStart[c], cnt = cellCount[c];
+  if (st > n || cnt > n - st) {
+    atomicOr(err, kErrBinRange);
+    return;
+  }
+  uint32_t r = 0;
+  for (uint32_t j = st; j < st + cnt; ++j) r += sortedTmp[j] < i ? 1u : 0u;
+  sorted[st + r] = i;
+}
+
+// The same canonical order indexed by particle, for bins that leave some
+// particles out (their slots do not exist, so the slot count is not n).
+__global__ void __launch_bounds__(kThreads) k_bin_canon_particles(uint32_t n, const uint32_t* __restrict__ key,
+                                                                  const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ cellCount,
+                                                                  const uint32_t* __restrict__ sortedTmp, uint32_t* sorted, uint32_t* err) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = key[i];
+  if (c == kKeyExcluded) return;
+  const uint32_t st = cellStart[c], cnt = cellCount[c];
   if (st > n || cnt > n - st) {
     atomicOr(err, kErrBinRange);
     return;
@@ -143,7 +170,7 @@ cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, con
   cudaError_t e = cudaMemsetAsync(b.cellCount, 0, nc * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   if (n > 0) {
-    k_bin_count<<<blocksFor(n), kThreads, 0, s>>>(P, pos, n, b.cellCount, b.key, b.rank);
+    k_bin_count<<<blocksFor(n), kThreads, 0, s>>>(P, pos, b.typeFlag, n, b.cellCount, b.key, b.rank);
     ++*launches;
   }
   const uint32_t tiles = scanTiles(nc);
@@ -153,7 +180,10 @@ cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, con
   ++*launches;
   if (n > 0) {
     k_bin_scatter<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.rank, b.cellStart, b.sortedTmp, b.err);
-    k_bin_canon<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
+    if (b.typeFlag)
+      k_bin_canon_particles<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
+    else
+      k_bin_canon<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
     *launches += 2;
   }
   return cudaGetLastError();

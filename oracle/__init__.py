@@ -25,7 +25,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 SRC = HERE / "mpm_oracle.cpp"
-SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp", HERE / "mpm_emit_oracle.cpp", HERE / "mpm_mesh_sdf_oracle.cpp")
+SRCS = (HERE / "mpm_oracle.cpp", HERE / "mpm_adjoint.cpp", HERE / "mpm_emit_oracle.cpp", HERE / "mpm_mesh_sdf_oracle.cpp",
+        HERE / "hash_bin_oracle.cpp")
 LIB = HERE / "libmpm_oracle.so"
 
 MODES = {"ref32": 0, "mixed": 1, "fp64": 2}
@@ -398,3 +399,22 @@ def mesh_sdf(tris, res, total_cells: int, cell_size: float, complete: bool = Tru
     lib().orc_mesh_sdf(t.ctypes.data_as(C.c_void_p), C.c_uint32(t.shape[0]), r.ctypes.data_as(C.c_void_p), C.c_uint32(int(total_cells)),
                        C.c_float(cell_size), out.ctypes.data_as(C.c_void_p), C.c_int(int(bool(complete))))
     return out
+
+
+def hash_bin(pred_p, type_flag, world_min, cell_size: float, grid_res, hash_cells: int, sorted_init=0xFFFFFFFF):
+    """The PBF spatial hash restated on the CPU (hash_bin_oracle.cpp):
+    (cellCount, cellOffset = range ends, sortedIdx).  pred_p: (n, 4) float32;
+    type_flag: (n,) uint32 or None.  Slots of sortedIdx past the included
+    particles keep `sorted_init`."""
+    p = np.ascontiguousarray(pred_p, np.float32).reshape(-1, 4)
+    n = p.shape[0]
+    tf = None if type_flag is None else np.ascontiguousarray(type_flag, np.uint32)
+    wm = np.ascontiguousarray(world_min, np.float32)
+    gr = np.ascontiguousarray(grid_res, np.uint32)
+    cnt = np.empty(int(hash_cells), np.uint32)
+    off = np.empty(int(hash_cells), np.uint32)
+    srt = np.full(n, sorted_init, np.uint32)
+    lib().orc_hash_bin(p.ctypes.data_as(C.c_void_p), None if tf is None else tf.ctypes.data_as(C.c_void_p), C.c_uint32(n),
+                       wm.ctypes.data_as(C.c_void_p), C.c_float(cell_size), gr.ctypes.data_as(C.c_void_p), C.c_uint32(int(hash_cells)),
+                       cnt.ctypes.data_as(C.c_void_p), off.ctypes.data_as(C.c_void_p), srt.ctypes.data_as(C.c_void_p))
+    return cnt, off, srt

@@ -22,13 +22,14 @@ def declared_symbols():
     for h in (ROOT / "include").glob("*.h"):
         txt = h.read_text()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-        syms.update(re.findall(r"\b(nebula_mpm_[a-z0-9_]+)\s*\(", txt))
+        syms.update(re.findall(r"\b(nebula_(?:mpm|hash)_[a-z0-9_]+)\s*\(", txt))
     return sorted(syms)
 
 
 def test_header_declares_entry_points():
     syms = declared_symbols()
     assert "nebula_mpm_step" in syms and "nebula_mpm_create" in syms and "nebula_mpm_g2p" in syms
+    assert "nebula_hash_bin" in syms and "nebula_mpm_mesh_sdf_posed" in syms
 
 
 def test_every_declared_symbol_is_exported(lib):
