@@ -18,28 +18,35 @@ inline uint32_t blocksFor(uint64_t n, int t = kThreads) { return uint32_t((n + t
 
 constexpr uint32_t kKeyExcluded = 0xffffffffu;
 
-// mpm_hash_count.comp:7-14 / hash_count.comp:7-20 (+ the slot the sort would take)
+// mpm_hash_count.comp:7-14 / hash_count.comp:7-20 (+ the slot the sort would take).
+// Runs of equal keys in neighbouring lanes (particles stored in cell order, or
+// lattice order along x) take their slots with one atomic per run; the whole
+// warp stays converged for the shuffles, lanes without a particle carrying
+// the excluded key.
 __global__ void __launch_bounds__(kThreads) k_bin_count(SubstepParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ typeFlag,
                                                         uint32_t n, uint32_t* cellCount, uint32_t* key, uint32_t* rank) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (typeFlag && typeFlag[i] == kTypeFlagUnused) {
-    key[i] = kKeyExcluded;
-    return;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t c = kKeyExcluded;
+  if (i < n && !(typeFlag && typeFlag[i] == kTypeFlagUnused)) {
+    const float4 p = pos[i];
+    int cx, cy, cz;
+    cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
+    c = mortonEncode(cx, cy, cz);
   }
-  float4 p = pos[i];
-  int cx, cy, cz;
-  cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
-  uint32_t c = mortonEncode(cx, cy, cz);
-  // warp-aggregated increment: lanes sharing a cell take consecutive slots
-  uint32_t peers = __match_any_sync(__activemask(), c);
-  int leader = __ffs(peers) - 1;
-  uint32_t lane = threadIdx.x & 31;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t up = __shfl_up_sync(0xffffffffu, c, 1);
+  const uint32_t heads = __ballot_sync(0xffffffffu, lane == 0 || up != c);
+  const uint32_t le = 0xffffffffu >> (31u - lane);  // lanes 0..lane
+  const uint32_t head = 31u - __clz(heads & le);     // first lane of this lane's run
+  const uint32_t after = heads & ~le;
+  const uint32_t runEnd = after ? uint32_t(__ffs(after) - 1) : 32u;
   uint32_t base = 0;
-  if (int(lane) == leader) base = atomicAdd(cellCount + c, uint32_t(__popc(peers)));
-  base = __shfl_sync(peers, base, leader);
-  key[i] = c;
-  rank[i] = base + __popc(peers & ((1u << lane) - 1u));
+  if (lane == head && c != kKeyExcluded) base = atomicAdd(cellCount + c, runEnd - lane);
+  base = __shfl_sync(0xffffffffu, base, head);
+  if (i < n) {
+    key[i] = c;
+    rank[i] = base + (lane - head);
+  }
 }
 
 // mpm_hash_sort.comp:7-15 with the slot taken at count time
@@ -54,31 +61,38 @@ __global__ void __launch_bounds__(kThreads) k_bin_scatter(uint32_t n, const uint
   else atomicOr(err, kErrBinRange);  // only after an expired scan wait
 }
 
-// In-cell canonical order (ascending particle index): each slot finds its
-// rank among the slots of its own cell.
-__global__ void __launch_bounds__(kThreads) k_bin_canon(uint32_t n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ cellStart,
-                                                        const uint32_t* __restrict__ cellCount, const uint32_t* __restrict__ sortedTmp,
-                                                        uint32_t* sorted, uint32_t* err) {
-  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  uint32_t i = sortedTmp[s];
-  if (i >= n) {
-    atomicOr(err, kErrBinRange);
-    return;
-  }
-  uint32_t c = key[i];
-  uint32_t st = cellStart[c], cnt = cellCount[c];
+// In-cell canonical order (ascending particle index).  Cells of at most
+// kCanonCellMax particles: one thread per cell loads the cell's slots (the
+// warp reads one contiguous span) and ranks them in registers.  Larger cells:
+// one thread per particle counts the smaller indices of its cell.
+constexpr uint32_t kCanonCellMax = 16;
+
+__global__ void __launch_bounds__(kThreads) k_bin_canon_cells(uint32_t nc, uint32_t n, const uint32_t* __restrict__ cellStart,
+                                                              const uint32_t* __restrict__ cellCount, const uint32_t* __restrict__ sortedTmp,
+                                                              uint32_t* sorted, uint32_t* err) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const uint32_t cnt = cellCount[c];
+  if (cnt == 0 || cnt > kCanonCellMax) return;
+  const uint32_t st = cellStart[c];
   if (st > n || cnt > n - st) {
     atomicOr(err, kErrBinRange);
     return;
   }
-  uint32_t r = 0;
-  for (uint32_t j = st; j < st + cnt; ++j) r += sortedTmp[j] < i ? 1u : 0u;
-  sorted[st + r] = i;
+  uint32_t v[kCanonCellMax];
+#pragma unroll
+  for (uint32_t k = 0; k < kCanonCellMax; ++k) v[k] = k < cnt ? sortedTmp[st + k] : 0xffffffffu;  // padding never ranks below
+#pragma unroll
+  for (uint32_t k = 0; k < kCanonCellMax; ++k) {
+    if (k < cnt) {
+      uint32_t r = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < kCanonCellMax; ++j) r += v[j] < v[k] ? 1u : 0u;
+      sorted[st + r] = v[k];
+    }
+  }
 }
 
-// The same canonical order indexed by particle, for bins that leave some
-// particles out (their slots do not exist, so the slot count is not n).
 __global__ void __launch_bounds__(kThreads) k_bin_canon_particles(uint32_t n, const uint32_t* __restrict__ key,
                                                                   const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ cellCount,
                                                                   const uint32_t* __restrict__ sortedTmp, uint32_t* sorted, uint32_t* err) {
@@ -87,6 +101,7 @@ __global__ void __launch_bounds__(kThreads) k_bin_canon_particles(uint32_t n, co
   const uint32_t c = key[i];
   if (c == kKeyExcluded) return;
   const uint32_t st = cellStart[c], cnt = cellCount[c];
+  if (cnt <= kCanonCellMax) return;  // ranked by k_bin_canon_cells
   if (st > n || cnt > n - st) {
     atomicOr(err, kErrBinRange);
     return;
@@ -180,11 +195,9 @@ cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, con
   ++*launches;
   if (n > 0) {
     k_bin_scatter<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.rank, b.cellStart, b.sortedTmp, b.err);
-    if (b.typeFlag)
-      k_bin_canon_particles<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
-    else
-      k_bin_canon<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
-    *launches += 2;
+    k_bin_canon_cells<<<blocksFor(nc), kThreads, 0, s>>>(uint32_t(nc), n, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
+    k_bin_canon_particles<<<blocksFor(n), kThreads, 0, s>>>(n, b.key, b.cellStart, b.cellCount, b.sortedTmp, b.sorted, b.err);
+    *launches += 3;
   }
   return cudaGetLastError();
 }
