@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=5, help="timed steps of the batched / plain comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-vs-forward measurement")
     ap.add_argument("--no-mesh-sdf", action="store_true", help="skip the mesh -> SDF build measurement")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner's")
     ap.add_argument("--mesh-sdf-only", action="store_true", help="only the mesh -> SDF build measurement (one JSON line)")
     return ap.parse_args()
 
@@ -234,7 +235,7 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------------------- batched vs plain
-def measure_batch(steps: int, warmup: int, substeps: int, dist=None) -> dict:
+def measure_batch(steps: int, warmup: int, substeps: int, dist=None, tune: bool = True) -> dict:
     """The 64-scene mix advanced by the batched engine (one set of launches
     per substep, replayed from a CUDA graph) and by single-scene engines
     stepped one after another, on the same stream, with each scene's moving
@@ -276,6 +277,12 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None) -> dict:
         return shard.max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
 
     b, ids = batch_for_scenes(scenes)
+    tuned = None
+    if tune:
+        from nebula_b200 import autotune
+        _, rep = autotune.tune_batch(b, scenes, ids, substeps=substeps)
+        tuned = {"shape": rep["shape"], "source": rep["source"], "ms_per_substep": rep["ms_per_substep"],
+                 "default_ms_per_substep": rep["default_ms_per_substep"], "shapes_tried": len(rep["tried"]), "key": rep["key"]}
 
     def batch_step(k):
         for i, s in enumerate(ids):
@@ -310,7 +317,7 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None) -> dict:
             "warmup": warmup, "dt": dt, "value": ps / (ms_b * 1e-3), "ms_per_step": ms_b / steps, "plain_value": ps / (ms_p * 1e-3),
             "plain_ms_per_step": ms_p / steps, "speedup": ms_p / ms_b, "unit": UNIT, "gpu_launches": launches_b,
             "plain_gpu_launches": launches_p, "n_gpus": world, "scaling": "strong" if world > 1 else "single",
-            "scenes_on_rank0": len(mine),
+            "scenes_on_rank0": len(mine), "autotune": tuned,
             "note": "batched: one grid update + one fused G2P/P2G + scan + permutation per substep over all scenes, graph "
                     "replay; plain: the same kernels per scene, one engine per scene in sequence; ranks take scenes by a "
                     "particle-balanced greedy partition, time = max over ranks"}
@@ -521,13 +528,19 @@ def main():
     active = int((mass >= 1e-10).sum())
     del mom, mass
 
+    # ---- launch shape: the autotuner's pick for this GPU and workload (timed outside the bench region)
+    tuned = None
+    if not args.no_tune and args.pipeline == "fused":
+        from nebula_b200 import autotune
+        shape, rep = autotune.tune_engine(eng, sc, substeps=S)
+        tuned = {"shape": rep["shape"], "source": rep["source"], "ms_per_substep": rep["ms_per_substep"],
+                 "default_ms_per_substep": rep["default_ms_per_substep"], "shapes_tried": len(rep["tried"]), "key": rep["key"]}
+
     for _ in range(args.warmup):
         eng.step(dt_frame, stream)
     eng.sync()
 
     # ---- device-timed region
-    eng.profile(True)
-    eng.profile_read(reset=True)
     st0 = eng.stats()
     clocks = ClockSampler(local)
     clocks.start()
@@ -546,9 +559,16 @@ def main():
     eng.sync()
     ms = e0.elapsed_time(e1)
     st1 = eng.stats()
+    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
+    # per-phase split from a separate run with events between the phases (not in the timed region)
+    prof_steps = max(1, min(args.steps, 5))
+    eng.profile(True)
+    eng.profile_read(reset=True)
+    for _ in range(prof_steps):
+        eng.step(dt_frame, stream)
+    eng.sync()
     phases = eng.profile_read(reset=True)
     eng.profile(False)
-    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -592,7 +612,7 @@ def main():
     sdf = sc.sdf is not None
     dom = max((p for p in phases if phases[p][1] > 0), key=lambda p: phases[p][0])
     dom_ms, dom_launches = phases[dom]
-    calls = args.steps * S
+    calls = prof_steps * S
     per_launch_ms = dom_ms / calls
     alg = algorithmic_bytes(dom, n, active, sp.hash_cells, flip, sdf)
     achieved = alg / (per_launch_ms * 1e-3) / 1e9
@@ -622,6 +642,7 @@ def main():
                 "steps": e2e_steps},
         "gpu_launches": launches,
         "clocks": ck,
+        "autotune": tuned,
     }
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -643,7 +664,7 @@ def main():
                                 "sample": "%d substeps of %s (after one untimed), CPU oracle ref32 mode, OpenMP" % (k, sc.name)}
     eng.cleanup()
     if not args.no_batch:
-        line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20, dist)
+        line["batched"] = measure_batch(args.batch_steps, max(1, min(args.warmup, 3)), 20, dist, tune=not args.no_tune)
     if not args.no_adjoint:
         line["adjoint"] = measure_adjoint(3, 2)
     if not args.no_mesh_sdf:

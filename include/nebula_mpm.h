@@ -238,6 +238,28 @@ int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_
 #define NEBULA_MPM_PIPELINE_DENSE 0
 #define NEBULA_MPM_PIPELINE_FUSED 1
 int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
+
+/* Launch shape of the per-substep kernels (block and tile sizes), picked per
+ * GPU and workload by the project's autotuner (nebula_b200/autotune.py, a
+ * JSON cache keyed by GPU and configuration).  fused_threads: CTA size of the
+ * fused G2P/P2G kernel = particles per P2G chunk (128 or 256);
+ * fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the fused
+ * and grid-update kernels (0 = as many as fit; larger values are capped at
+ * that); grid_batch: grid nodes per thread per round (2 or 4).  Every shape
+ * computes the same substep (float sums may associate differently).  No
+ * counterpart in the reference (its dispatch sizes are fixed in the shaders). */
+typedef struct nebula_mpm_launch_config {
+  uint32_t fused_threads;
+  uint32_t fused_ctas_per_sm;
+  uint32_t grid_ctas_per_sm;
+  uint32_t grid_batch;
+} nebula_mpm_launch_config;
+int nebula_mpm_set_launch_config(nebula_mpm* e, const nebula_mpm_launch_config* c);
+int nebula_mpm_get_launch_config(nebula_mpm* e, nebula_mpm_launch_config* c);
+/* The most CTAs per SM of each variant on the current device (occupancy):
+ * fused_ctas_per_sm[fused_threads == 256], grid_ctas_per_sm[grid_batch == 4];
+ * flip / batch select the fused kernel's FLIP and batched instantiations. */
+int nebula_mpm_launch_limits(int flip, int batch, uint32_t fused_ctas_per_sm[2], uint32_t grid_ctas_per_sm[2]);
 /* The engine's own brick binning of the current positions (FUSED pipeline):
  * *numBricks listed bricks (brick id = cell Morton code >> 6) with the first
  * sorted slot of each (brickStarts has *numBricks + 1 entries, the last = live
@@ -309,6 +331,9 @@ int nebula_mpm_batch_download(nebula_mpm_batch* b, uint32_t scene, int field, fl
 int nebula_mpm_batch_step(nebula_mpm_batch* b, float dt, uint32_t substeps, void* stream);
 /* Graph capture and replay of steps (default on); off launches eagerly. */
 int nebula_mpm_batch_set_graphs(nebula_mpm_batch* b, int enable);
+/* nebula_mpm_set_launch_config for a batch; drops its captured graphs. */
+int nebula_mpm_batch_set_launch_config(nebula_mpm_batch* b, const nebula_mpm_launch_config* c);
+int nebula_mpm_batch_get_launch_config(nebula_mpm_batch* b, nebula_mpm_launch_config* c);
 int nebula_mpm_batch_sync(nebula_mpm_batch* b);
 int nebula_mpm_batch_get_stats(nebula_mpm_batch* b, nebula_mpm_batch_stats* s);
 int nebula_mpm_batch_scene_info(const nebula_mpm_batch* b, uint32_t scene, nebula_mpm_scene_info* info);

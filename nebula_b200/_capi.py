@@ -48,6 +48,10 @@ class Particles(C.Structure):
     _fields_ = [("f", C.c_void_p * 8)]
 
 
+class LaunchConfig(C.Structure):
+    _fields_ = [("fused_threads", C.c_uint32), ("fused_ctas_per_sm", C.c_uint32), ("grid_ctas_per_sm", C.c_uint32), ("grid_batch", C.c_uint32)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("maxScenes", C.c_uint32), ("maxParticles", C.c_uint32)]
 
@@ -104,6 +108,9 @@ _SIGS = {
     "nebula_mpm_export_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_pipeline": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nebula_mpm_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nebula_mpm_launch_limits": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "nebula_mpm_export_grid": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]),
@@ -124,6 +131,8 @@ _SIGS = {
     "nebula_mpm_batch_download": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64]),
     "nebula_mpm_batch_step": (C.c_int, [C.c_void_p, C.c_float, C.c_uint32, C.c_void_p]),
     "nebula_mpm_batch_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_batch_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nebula_mpm_batch_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_batch_sync": (C.c_int, [C.c_void_p]),
     "nebula_mpm_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     "nebula_mpm_batch_scene_info": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(SceneInfo)]),

@@ -143,6 +143,19 @@ class BatchEngine:
     def run_substeps(self, sub_dt: float, count: int, stream=None):
         self.step(sub_dt * count, count, stream)
 
+    def set_launch_config(self, cfg):
+        """Launch shape of the fused and grid kernels (autotune.LaunchShape or a
+        dict with its fields); drops the batch's captured graphs."""
+        from .autotune import LaunchShape
+        c = LaunchShape.coerce(cfg).to_c()
+        call("nebula_mpm_batch_set_launch_config", self._h, C.byref(c))
+
+    def launch_config(self):
+        from .autotune import LaunchShape
+        c = _capi.LaunchConfig()
+        call("nebula_mpm_batch_get_launch_config", self._h, C.byref(c))
+        return LaunchShape.from_c(c)
+
     def set_graphs(self, enable: bool):
         call("nebula_mpm_batch_set_graphs", self._h, int(bool(enable)))
 

@@ -454,14 +454,23 @@ void BatchEngine::substep(uint32_t k, cudaStream_t st) {
   BrickBuffers B = brickBuffers();
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
-  check(launchGridBricksBatch(T, k, B, G, numSMs_, st, &launches_), "grid bricks");
+  check(launchGridBricksBatch(T, k, B, G, launchCfg_, numSMs_, st, &launches_), "grid bricks");
   check(launchG2P2GBatch(T, G.vold != nullptr, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
-                         static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, err, numSMs_, st, &launches_),
+                         static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, err, launchCfg_, numSMs_, st, &launches_),
         "g2p2g");
   check(launchBrickScan(B, err, st, &launches_), "brick scan");
   check(launchPermScatter(B, live_, err, st, &launches_), "perm scatter");
   cur_ ^= 1;
   permuted_ = true;
+}
+
+// Captured graphs hold the old shape: drop them (after the queued work).
+void BatchEngine::setLaunchConfig(const LaunchConfig& c) {
+  validateLaunchConfig(c);
+  bindDevice();
+  quiesce();
+  clearGraphs();
+  launchCfg_ = c;
 }
 
 void BatchEngine::setGraphs(bool on) {
@@ -678,6 +687,18 @@ int nebula_mpm_batch_step(nebula_mpm_batch* b, float dt, uint32_t substeps, void
 }
 int nebula_mpm_batch_set_graphs(nebula_mpm_batch* b, int enable) {
   return guardedB([&] { B(b).setGraphs(enable != 0); });
+}
+int nebula_mpm_batch_set_launch_config(nebula_mpm_batch* b, const nebula_mpm_launch_config* c) {
+  return guardedB([&] {
+    if (!c) throw Error(NEBULA_MPM_ERR_INVALID, "null launch config");
+    B(b).setLaunchConfig(nebula::fromAbi(*c));
+  });
+}
+int nebula_mpm_batch_get_launch_config(nebula_mpm_batch* b, nebula_mpm_launch_config* c) {
+  return guardedB([&] {
+    if (!c) throw Error(NEBULA_MPM_ERR_INVALID, "null launch config");
+    *c = nebula::toAbi(B(b).launchConfig());
+  });
 }
 int nebula_mpm_batch_sync(nebula_mpm_batch* b) {
   return guardedB([&] {

@@ -36,6 +36,8 @@ class BatchEngine {
   void download(uint32_t s, int field, float* host, uint64_t count);
   void step(float dt, uint32_t substeps, cudaStream_t st);
   void setGraphs(bool on);
+  void setLaunchConfig(const LaunchConfig& c);
+  const LaunchConfig& launchConfig() const { return launchCfg_; }
   uint32_t syncAndCheck();
   void stats(nebula_mpm_batch_stats* out);
   void sceneInfo(uint32_t s, nebula_mpm_scene_info* out) const;
@@ -77,6 +79,7 @@ class BatchEngine {
   nebula_mpm_batch_config cfg_;
   int device_ = 0;
   int numSMs_ = 148;
+  LaunchConfig launchCfg_;
   std::vector<Scene> scenes_;
   uint32_t live_ = 0;
   uint32_t nbTotal_ = 0;

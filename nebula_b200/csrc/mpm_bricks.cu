@@ -12,6 +12,8 @@
 #include "mpm_particle.cuh"
 #include "mpm_scan.cuh"
 
+#include <algorithm>
+
 namespace nebula {
 namespace {
 
@@ -332,8 +334,6 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 // contributions in registers, then add them into the brick's 8^3 tile (see
 // kTileCopies).  Two barriers per chunk.  The brick ends with one vector
 // reduction per non-zero node of the tile.
-constexpr int kChunk = kThreads;
-constexpr int kWarps = kThreads / 32;
 constexpr int kRow = 10;        // float4 per input row: 3 axes x 3 offsets of (A0, A1, A2, W), then (m, -, -, -)
 constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
@@ -345,27 +345,33 @@ constexpr uint32_t kNoRow = 0xFFFFu;  // end of a cell's list
 // stencils overlap); kWarps = one private tile per warp with plain adds.
 constexpr int kTileCopies = 1;
 
-struct P2GSmem {
-  float4 rows[kChunk * kRow];
+// CHUNK = the CTA size = particles per chunk (128 or 256).
+template <int CHUNK>
+struct P2GSmemT {
+  static constexpr int kChunk = CHUNK;
+  static constexpr int kWarps = CHUNK / 32;
+  float4 rows[CHUNK * kRow];
   float tiles[kTileCopies * 4 * kTileNodes];
   uint32_t head[kCellSlots];   // first row of each cell's list (kNoRow: empty)
-  uint16_t next[kChunk];       // next row of the same cell
+  uint16_t next[CHUNK];        // next row of the same cell
   uint16_t cells[kCellSlots];  // the chunk's non-empty cells
   uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
   uint32_t markMask;           // grid-active marks of the item brick's 3^3 neighbour bricks
   uint32_t item;
 };
+using P2GSmem = P2GSmemT<kThreads>;
 
 // Push this thread's row onto the list of cell `key` (`par`: the chunk's parity).
-__device__ __forceinline__ void p2gRegister(P2GSmem& sm, int key, uint32_t par) {
+template <class SM>
+__device__ __forceinline__ void p2gRegister(SM& sm, int key, uint32_t par) {
   const uint32_t prev = atomicExch(&sm.head[key], threadIdx.x);
   sm.next[threadIdx.x] = uint16_t(prev);
   if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(key);
 }
 
-template <bool FLIP>
+template <bool FLIP, int CHUNK>
 struct G2P2GSmem {
-  P2GSmem p2g;
+  P2GSmemT<CHUNK> p2g;
   float4 v[216];
   float4 vo[FLIP ? 216 : 1];
 };
@@ -443,7 +449,8 @@ __device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* 
       }
 }
 
-__device__ __forceinline__ void p2gZeroTiles(P2GSmem& sm) {
+template <class SM>
+__device__ __forceinline__ void p2gZeroTiles(SM& sm) {
   for (int q = threadIdx.x; q < kTileCopies * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
   for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.head[q] = kNoRow;
   if (threadIdx.x < 2) sm.numCells[threadIdx.x] = 0u;
@@ -453,7 +460,9 @@ __device__ __forceinline__ void p2gZeroTiles(P2GSmem& sm) {
 // Called by every thread once the chunk's rows are written and registered;
 // ends synced.  Tile origin (node) = (bx, by, bz) * 4 - 2; stencil-centre
 // cells start at + 1.
-__device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, uint32_t par, int tx, int ty, int tz) {
+template <class SM>
+__device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_t par, int tx, int ty, int tz) {
+  constexpr int kChunk = SM::kChunk, kWarps = SM::kWarps;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
@@ -491,7 +500,8 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, P2GSmem& sm, ui
 }
 
 // Sum the tile copies and add every non-zero node to the global grid.
-__device__ __forceinline__ void p2gFlush(const SubstepParams& P, P2GSmem& sm, int tx, int ty, int tz, float4* acc) {
+template <class SM>
+__device__ __forceinline__ void p2gFlush(const SubstepParams& P, SM& sm, int tx, int ty, int tz, float4* acc) {
   const int cr = int(P.cubeRes);
   for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
     float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
@@ -555,8 +565,10 @@ __device__ __forceinline__ int cellSlot(int cx, int cy, int cz, int ox, int oy, 
 
 // ------------------------------------------------------------------ P2G over particle bricks (standalone)
 // P2G of the particles in sorted slots [start, end) of brick `b` (the scene's own brick id).
-__device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, P2GSmem& sm, uint32_t b, uint32_t start, uint32_t end, StatePtrs cur,
+template <class SM>
+__device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, SM& sm, uint32_t b, uint32_t start, uint32_t end, StatePtrs cur,
                                              uint32_t n, const BrickBuffers& B, const GridBuffers& G, float dtStress) {
+  constexpr int kChunk = SM::kChunk;
   int bx, by, bz;
   mortonDecode(b, bx, by, bz);
   const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
@@ -612,11 +624,11 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P0, Scene
 }
 
 // ------------------------------------------------------------------ sparse grid update
-// Per thread, kGridBatch nodes per round: their brick ids, then their
-// accumulators (and an L1 prefetch of their SDF samples) are loaded before any
-// node is updated, so one round costs about the memory round trips of one node.
-constexpr int kGridBatch = 4;
-
+// Per thread, kGridBatch nodes per round (2 or 4, picked by the launch
+// configuration): their brick ids, then their accumulators (and an L1
+// prefetch of their SDF samples) are loaded before any node is updated, so
+// one round costs about the memory round trips of one node.
+template <int kGridBatch>
 __global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, BrickBuffers B, GridBuffers G) {
   const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -698,12 +710,13 @@ __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridB
 // brick `b` (the scene's own brick id) from the staged grid, particle update,
 // binning count under the global brick key brickBase + (Morton >> 6), and P2G
 // of the updated particles.
-template <bool FLIP>
-__device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP>& S, uint32_t b, uint32_t start, uint32_t end,
+template <bool FLIP, int CHUNK>
+__device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP, CHUNK>& S, uint32_t b, uint32_t start, uint32_t end,
                                           uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
                                           uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B, const GridBuffers& G,
                                           float dtStress, uint32_t* err) {
-  P2GSmem& sm = S.p2g;
+  constexpr int kChunk = CHUNK;
+  auto& sm = S.p2g;
   int bx, by, bz;
   mortonDecode(b, bx, by, bz);
   // stage the 6^3 nodes [4b-1, 4b+4]^3 (nodes outside [0, gridRes) read as empty)
@@ -773,16 +786,17 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
   p2gFlush(P, sm, tx, ty, tz, G.acc);
 }
 
-// 3 CTAs per SM: 80 registers with some spills to L1-cached local memory beat
-// 2 CTAs at 128 registers (measured on the 1M-particle slope: Drucker-Prager
-// -3%, Von Mises -6%, ELASTIC -9% per launch); shared memory is 54 KB per CTA.
-template <bool FLIP, bool BATCH>
-__global__ void __launch_bounds__(kThreads, 3) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
+// 768 / CHUNK CTAs per SM (3 of 256 threads, 6 of 128): 80 registers with some
+// spills to L1-cached local memory beat 2 CTAs of 256 at 128 registers
+// (measured on the 1M-particle slope: Drucker-Prager -3%, Von Mises -6%,
+// ELASTIC -9% per launch); shared memory is 54 KB per 256-thread CTA.
+template <bool FLIP, bool BATCH, int CHUNK>
+__global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
                                                     StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G,
                                                     float dtStress, uint32_t* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  G2P2GSmem<FLIP>& S = *reinterpret_cast<G2P2GSmem<FLIP>*>(smem_raw);
-  P2GSmem& sm = S.p2g;
+  G2P2GSmem<FLIP, CHUNK>& S = *reinterpret_cast<G2P2GSmem<FLIP, CHUNK>*>(smem_raw);
+  auto& sm = S.p2g;
   const uint32_t numPB = B.counters[kCntNumPB];
   for (;;) {
     if (threadIdx.x == 0) sm.item = atomicAdd(B.counters + kCntQueueFused, 1u);
@@ -801,9 +815,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_g2p2g(SubstepParams P0, SceneTa
       }
       __syncthreads();
       const uint32_t base = sBase;
-      g2p2gItem<FLIP>(sP, S, b - base, start, end, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
+      g2p2gItem<FLIP, CHUNK>(sP, S, b - base, start, end, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
     } else {
-      g2p2gItem<FLIP>(P0, S, b, start, end, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
+      g2p2gItem<FLIP, CHUNK>(P0, S, b, start, end, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
     }
     __syncthreads();
   }
@@ -831,45 +845,74 @@ __global__ void __launch_bounds__(kThreads) k_iota(uint32_t* pid, uint32_t n) {
   if (i < n) pid[i] = i;
 }
 
-template <class K> int persistentBlocks(K kernel, int numSMs, size_t smem = 0) {
+template <class K> int ctasPerSm(K kernel, int threads, size_t smem = 0) {
   int perSM = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, smem) != cudaSuccess || perSM < 1) perSM = 1;
-  return perSM * numSMs;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, threads, smem) != cudaSuccess || perSM < 1) perSM = 1;
+  return perSM;
 }
 
-template <class K> int setupBigSmem(K kernel, size_t smem, int numSMs) {
+template <class K> int bigSmemCtasPerSm(K kernel, int threads, size_t smem) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  return persistentBlocks(kernel, numSMs, smem);
+  return ctasPerSm(kernel, threads, smem);
 }
 
-// Persistent grid sizes of every kernel, resolved once (kernel attributes and
-// occupancy queries stay outside stream capture).
+// Most CTAs per SM of every kernel variant, resolved once (kernel attributes
+// and occupancy queries stay outside stream capture).
 struct LaunchShapes {
   bool ready = false;
-  int p2g[2] = {0, 0};        // [BATCH]
-  int grid = 0, gridBatch = 0;
-  int fused[2][2] = {{0, 0}, {0, 0}};  // [FLIP][BATCH]
+  int p2g[2] = {0, 0};                          // [BATCH]
+  int grid[2] = {0, 0};                         // [gridBatch == 4]
+  int gridBatch = 0;                            // batched grid kernel
+  int fused[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};  // [FLIP][BATCH][CHUNK == 256]
 };
 LaunchShapes g_shapes;
 
-const LaunchShapes& shapes(int numSMs) {
+template <bool FLIP, bool BATCH, int CHUNK> void setupFused(LaunchShapes& L) {
+  L.fused[FLIP][BATCH][CHUNK == 256] = bigSmemCtasPerSm(k_g2p2g<FLIP, BATCH, CHUNK>, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>));
+}
+
+const LaunchShapes& shapes() {
   if (g_shapes.ready) return g_shapes;
   LaunchShapes& L = g_shapes;
-  L.p2g[0] = setupBigSmem(k_p2g_bricks<false>, sizeof(P2GSmem), numSMs);
-  L.p2g[1] = setupBigSmem(k_p2g_bricks<true>, sizeof(P2GSmem), numSMs);
-  L.grid = persistentBlocks(k_grid_bricks, numSMs);
-  L.gridBatch = persistentBlocks(k_grid_bricks_batch, numSMs);
-  L.fused[0][0] = setupBigSmem(k_g2p2g<false, false>, sizeof(G2P2GSmem<false>), numSMs);
-  L.fused[0][1] = setupBigSmem(k_g2p2g<false, true>, sizeof(G2P2GSmem<false>), numSMs);
-  L.fused[1][0] = setupBigSmem(k_g2p2g<true, false>, sizeof(G2P2GSmem<true>), numSMs);
-  L.fused[1][1] = setupBigSmem(k_g2p2g<true, true>, sizeof(G2P2GSmem<true>), numSMs);
+  L.p2g[0] = bigSmemCtasPerSm(k_p2g_bricks<false>, kThreads, sizeof(P2GSmem));
+  L.p2g[1] = bigSmemCtasPerSm(k_p2g_bricks<true>, kThreads, sizeof(P2GSmem));
+  L.grid[0] = ctasPerSm(k_grid_bricks<2>, kThreads);
+  L.grid[1] = ctasPerSm(k_grid_bricks<4>, kThreads);
+  L.gridBatch = ctasPerSm(k_grid_bricks_batch, kThreads);
+  setupFused<false, false, 128>(L);
+  setupFused<false, false, 256>(L);
+  setupFused<false, true, 128>(L);
+  setupFused<false, true, 256>(L);
+  setupFused<true, false, 128>(L);
+  setupFused<true, false, 256>(L);
+  setupFused<true, true, 128>(L);
+  setupFused<true, true, 256>(L);
   L.ready = true;
   return L;
 }
 
+// Blocks of a persistent launch: the requested CTAs per SM (0 = most that fit), capped by occupancy.
+int persistentGrid(uint32_t requested, int most, int numSMs) {
+  const int per = requested == 0 ? most : std::min(int(requested), most);
+  return std::max(per, 1) * numSMs;
+}
+
 }  // namespace
 
-void prepareBrickKernels(int numSMs) { (void)shapes(numSMs); }
+LaunchLimits launchLimits(bool flip, bool batch) {
+  const LaunchShapes& L = shapes();
+  LaunchLimits out;
+  out.fusedCtasPerSm[0] = uint32_t(L.fused[flip][batch][0]);
+  out.fusedCtasPerSm[1] = uint32_t(L.fused[flip][batch][1]);
+  out.gridCtasPerSm[0] = uint32_t(L.grid[0]);
+  out.gridCtasPerSm[1] = uint32_t(L.grid[1]);
+  return out;
+}
+
+void prepareBrickKernels(int numSMs) {
+  (void)numSMs;
+  (void)shapes();
+}
 
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches) {
@@ -902,27 +945,32 @@ cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, 
 
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
                             int numSMs, cudaStream_t s, uint64_t* launches) {
-  k_p2g_bricks<false><<<shapes(numSMs).p2g[0], kThreads, sizeof(P2GSmem), s>>>(P, SceneTable{}, cur, n, b, g, dtStress);
+  k_p2g_bricks<false><<<shapes().p2g[0] * numSMs, kThreads, sizeof(P2GSmem), s>>>(P, SceneTable{}, cur, n, b, g, dtStress);
   ++*launches;
   return cudaGetLastError();
 }
 
 cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, int numSMs,
                                  cudaStream_t s, uint64_t* launches) {
-  k_p2g_bricks<true><<<shapes(numSMs).p2g[1], kThreads, sizeof(P2GSmem), s>>>(SubstepParams{}, T, cur, n, b, g, 0.f);
+  k_p2g_bricks<true><<<shapes().p2g[1] * numSMs, kThreads, sizeof(P2GSmem), s>>>(SubstepParams{}, T, cur, n, b, g, 0.f);
   ++*launches;
   return cudaGetLastError();
 }
 
-cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches) {
-  k_grid_bricks<<<shapes(numSMs).grid, kThreads, 0, s>>>(P, b, g);
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                             uint64_t* launches) {
+  const LaunchShapes& L = shapes();
+  if (lc.gridBatch == 2)
+    k_grid_bricks<2><<<persistentGrid(lc.gridCtasPerSm, L.grid[0], numSMs), kThreads, 0, s>>>(P, b, g);
+  else
+    k_grid_bricks<4><<<persistentGrid(lc.gridCtasPerSm, L.grid[1], numSMs), kThreads, 0, s>>>(P, b, g);
   ++*launches;
   return cudaGetLastError();
 }
 
-cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s,
-                                  uint64_t* launches) {
-  k_grid_bricks_batch<<<shapes(numSMs).gridBatch, kThreads, 0, s>>>(T, substep, b, g);
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs,
+                                  cudaStream_t s, uint64_t* launches) {
+  k_grid_bricks_batch<<<persistentGrid(lc.gridCtasPerSm, shapes().gridBatch, numSMs), kThreads, 0, s>>>(T, substep, b, g);
   ++*launches;
   return cudaGetLastError();
 }
@@ -933,29 +981,43 @@ cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, 
   return cudaGetLastError();
 }
 
-cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches) {
-  const LaunchShapes& L = shapes(numSMs);
-  if (P.flip_ratio > 0.01f) {
-    k_g2p2g<true, false><<<L.fused[1][0], kThreads, sizeof(G2P2GSmem<true>), s>>>(P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress,
-                                                                                  err);
+namespace {
+
+template <bool FLIP, bool BATCH, int CHUNK>
+void launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                 const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, int numSMs, cudaStream_t s) {
+  const int blocks = persistentGrid(ctasPerSm, shapes().fused[FLIP][BATCH][CHUNK == 256], numSMs);
+  k_g2p2g<FLIP, BATCH, CHUNK><<<blocks, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>), s>>>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+}
+
+template <bool BATCH>
+void launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur,
+                    StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs,
+                    cudaStream_t s) {
+  const uint32_t k = lc.fusedCtasPerSm;
+  if (flip) {
+    if (lc.fusedThreads == 128) launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
+    else launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
   } else {
-    k_g2p2g<false, false><<<L.fused[0][0], kThreads, sizeof(G2P2GSmem<false>), s>>>(P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g,
-                                                                                    dtStress, err);
+    if (lc.fusedThreads == 128) launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
+    else launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
   }
+}
+
+}  // namespace
+
+cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                        uint64_t* launches) {
+  launchFusedFor<false>(P.flip_ratio > 0.01f, lc, P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
   ++*launches;
   return cudaGetLastError();
 }
 
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                             const BrickBuffers& b, GridBuffers g, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches) {
-  const LaunchShapes& L = shapes(numSMs);
-  if (flip) {
-    k_g2p2g<true, true><<<L.fused[1][1], kThreads, sizeof(G2P2GSmem<true>), s>>>(SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err);
-  } else {
-    k_g2p2g<false, true><<<L.fused[0][1], kThreads, sizeof(G2P2GSmem<false>), s>>>(SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f,
-                                                                                   err);
-  }
+                             const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                             uint64_t* launches) {
+  launchFusedFor<true>(flip, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
   ++*launches;
   return cudaGetLastError();
 }

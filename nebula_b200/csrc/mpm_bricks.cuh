@@ -60,6 +60,21 @@ struct GridBuffers {
   float4* vold;  // [ncPad] pre-force velocity (FLIP), may be null
 };
 
+// Launch shape of the per-substep kernels, picked per GPU and workload by the
+// autotuner (nebula_b200/autotune.py); 0 CTAs per SM = as many as fit.
+struct LaunchConfig {
+  uint32_t fusedThreads = 256;  // k_g2p2g CTA size = particles per P2G chunk: 128 or 256
+  uint32_t fusedCtasPerSm = 0;  // persistent k_g2p2g CTAs per SM
+  uint32_t gridCtasPerSm = 0;   // persistent grid-update CTAs per SM
+  uint32_t gridBatch = 4;       // k_grid_bricks nodes per thread per round: 2 or 4
+};
+// Most CTAs per SM (occupancy) of each variant: [fusedThreads == 256], [gridBatch == 4].
+struct LaunchLimits {
+  uint32_t fusedCtasPerSm[2];
+  uint32_t gridCtasPerSm[2];
+};
+LaunchLimits launchLimits(bool flip, bool batch);
+
 // Standalone binning of the particles in buffer order: counts + stencil marks.
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches);
@@ -70,22 +85,25 @@ cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, 
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
                             int numSMs, cudaStream_t s, uint64_t* launches);
 // Sparse grid update over the listed grid bricks; clears acc as it reads.
-cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                             uint64_t* launches);
 // Zero acc over the listed grid bricks (discarding a pending P2G).
 cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
 // The fused G2P -> particle update -> P2G + binning count.
 cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches);
+                        const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                        uint64_t* launches);
 // Batched forms: every scene of `T` in one launch.  `substep` selects the
 // colliders of this substep on each scene's collider track
 // (params.colliders + substep * params.colliderCount).
 cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32_t n, const BrickBuffers& b, cudaStream_t s, uint64_t* launches);
 cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, int numSMs,
                                  cudaStream_t s, uint64_t* launches);
-cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s,
-                                  uint64_t* launches);
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs,
+                                  cudaStream_t s, uint64_t* launches);
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                             const BrickBuffers& b, GridBuffers g, uint32_t* err, int numSMs, cudaStream_t s, uint64_t* launches);
+                             const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+                             uint64_t* launches);
 // Resolve every launcher's one-time set-up (shared-memory limits, persistent
 // block counts) outside any stream capture.
 void prepareBrickKernels(int numSMs);

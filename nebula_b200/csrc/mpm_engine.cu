@@ -230,6 +230,36 @@ void MPMEngine::setParams(const nebula_mpm_params& p) {
   params_ = p;
 }
 
+void validateLaunchConfig(const LaunchConfig& c) {
+  if (c.fusedThreads != 128 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 128 or 256");
+  if (c.gridBatch != 2 && c.gridBatch != 4) throw Error(NEBULA_MPM_ERR_INVALID, "grid_batch must be 2 or 4");
+  if (c.fusedCtasPerSm > 64 || c.gridCtasPerSm > 64) throw Error(NEBULA_MPM_ERR_INVALID, "CTAs per SM must be <= 64 (0 = as many as fit)");
+}
+
+LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
+  LaunchConfig l;
+  l.fusedThreads = c.fused_threads;
+  l.fusedCtasPerSm = c.fused_ctas_per_sm;
+  l.gridCtasPerSm = c.grid_ctas_per_sm;
+  l.gridBatch = c.grid_batch;
+  return l;
+}
+
+nebula_mpm_launch_config toAbi(const LaunchConfig& l) {
+  nebula_mpm_launch_config c;
+  c.fused_threads = l.fusedThreads;
+  c.fused_ctas_per_sm = l.fusedCtasPerSm;
+  c.grid_ctas_per_sm = l.gridCtasPerSm;
+  c.grid_batch = l.gridBatch;
+  return c;
+}
+
+// Takes effect at the next launch; kernels already queued keep their shape.
+void MPMEngine::setLaunchConfig(const LaunchConfig& c) {
+  validateLaunchConfig(c);
+  launchCfg_ = c;
+}
+
 void MPMEngine::setPipeline(int p) {
   if (p != NEBULA_MPM_PIPELINE_DENSE && p != NEBULA_MPM_PIPELINE_FUSED) throw Error(NEBULA_MPM_ERR_INVALID, "unknown pipeline");
   if (p == pipeline_) return;
@@ -630,12 +660,12 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   uint64_t l0 = launches_;
   phaseBegin(kPhaseGrid, s);
-  check(launchGridBricks(P, B, G, numSMs_, s, &launches_), "grid bricks");
+  check(launchGridBricks(P, B, G, launchCfg_, numSMs_, s, &launches_), "grid bricks");
   phaseEnd(kPhaseGrid, s, l0);
   l0 = launches_;
   phaseBegin(kPhaseFused, s);
   check(launchG2P2G(P, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
-                    static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, P.dt, err, numSMs_, s, &launches_),
+                    static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, P.dt, err, launchCfg_, numSMs_, s, &launches_),
         "g2p2g");
   phaseEnd(kPhaseFused, s, l0);
   l0 = launches_;
@@ -975,6 +1005,30 @@ int nebula_mpm_profile_read(nebula_mpm* e, double ms[NEBULA_MPM_PHASES], uint64_
 }
 int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline) {
   return guarded([&] { E(e).setPipeline(pipeline); });
+}
+int nebula_mpm_set_launch_config(nebula_mpm* e, const nebula_mpm_launch_config* c) {
+  return guarded([&] {
+    if (!c) throw Error(NEBULA_MPM_ERR_INVALID, "null launch config");
+    E(e).setLaunchConfig(nebula::fromAbi(*c));
+  });
+}
+int nebula_mpm_get_launch_config(nebula_mpm* e, nebula_mpm_launch_config* c) {
+  return guarded([&] {
+    if (!c) throw Error(NEBULA_MPM_ERR_INVALID, "null launch config");
+    *c = nebula::toAbi(E(e).launchConfig());
+  });
+}
+int nebula_mpm_launch_limits(int flip, int batch, uint32_t fused_ctas_per_sm[2], uint32_t grid_ctas_per_sm[2]) {
+  return guarded([&] {
+    if (!fused_ctas_per_sm || !grid_ctas_per_sm) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    int dev = 0;
+    nebula::check(cudaGetDevice(&dev), "device");
+    const nebula::LaunchLimits l = nebula::launchLimits(flip != 0, batch != 0);
+    for (int i = 0; i < 2; ++i) {
+      fused_ctas_per_sm[i] = l.fusedCtasPerSm[i];
+      grid_ctas_per_sm[i] = l.gridCtasPerSm[i];
+    }
+  });
 }
 int nebula_mpm_export_brick_bins(nebula_mpm* e, uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids) {
   return guarded([&] {

@@ -15,6 +15,11 @@
 
 namespace nebula {
 
+// Rejects launch shapes outside the compiled variants (NEBULA_MPM_ERR_INVALID).
+void validateLaunchConfig(const LaunchConfig& c);
+LaunchConfig fromAbi(const nebula_mpm_launch_config& c);
+nebula_mpm_launch_config toAbi(const LaunchConfig& c);
+
 struct Error : std::runtime_error {
   int code;
   Error(int code, const std::string& msg);
@@ -103,6 +108,8 @@ class MPMEngine {
   void profileRead(double* ms, uint64_t* launches, bool reset);
   void setPipeline(int p);
   int pipeline() const { return pipeline_; }
+  void setLaunchConfig(const LaunchConfig& c);
+  const LaunchConfig& launchConfig() const { return launchCfg_; }
   void exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids);
 
  private:
@@ -157,6 +164,7 @@ class MPMEngine {
   int cur_ = 0;
   bool permuted_ = false;
   int pipeline_ = NEBULA_MPM_PIPELINE_FUSED;
+  LaunchConfig launchCfg_;
   int numSMs_ = 148;
   // brick-sparse grid + binning
   uint32_t ncPad_ = 64, nb_ = 1, tiles_ = 1;

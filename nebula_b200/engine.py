@@ -250,6 +250,19 @@ class MPMEngine:
         return {k: (list(getattr(s, k)) if k == "grid_res" else getattr(s, k)) for k, _ in s._fields_}
 
     # ------------------------------------------------------------ pipeline
+    def set_launch_config(self, cfg):
+        """Launch shape of the fused and grid kernels (autotune.LaunchShape or a
+        dict with its fields)."""
+        from .autotune import LaunchShape
+        c = LaunchShape.coerce(cfg).to_c()
+        call("nebula_mpm_set_launch_config", self._h, C.byref(c))
+
+    def launch_config(self):
+        from .autotune import LaunchShape
+        c = _capi.LaunchConfig()
+        call("nebula_mpm_get_launch_config", self._h, C.byref(c))
+        return LaunchShape.from_c(c)
+
     def set_pipeline(self, name: str):
         """"fused" (default: brick-sparse, fused G2P+P2G) or "dense" (one kernel per reference dispatch)."""
         call("nebula_mpm_set_pipeline", self._h, {"dense": _capi.PIPELINE_DENSE, "fused": _capi.PIPELINE_FUSED}[name])
