@@ -560,8 +560,12 @@ def main():
     ms = e0.elapsed_time(e1)
     st1 = eng.stats()
     launches = int(st1["kernel_launches"] - st0["kernel_launches"])
-    # per-phase split from a separate run with events between the phases (not in the timed region)
-    prof_steps = max(1, min(args.steps, 5))
+    # per-phase split: the same warm-up and steps replayed from the initial state with events
+    # between the phases (the work per substep grows as the slab settles, so the window must match)
+    prof_steps = args.steps
+    eng.upload_state(sc.state)
+    for _ in range(args.warmup):
+        eng.step(dt_frame, stream)
     eng.profile(True)
     eng.profile_read(reset=True)
     for _ in range(prof_steps):
@@ -584,6 +588,8 @@ def main():
     out = {f: torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy() for f in sc.state}
     from nebula_b200 import _capi
     import ctypes as C
+    from nebula_b200.scenes import FIELDS as STATE_FIELDS
+    out_ptrs = (C.c_void_p * 8)(*[out[f].ctypes.data for f in STATE_FIELDS])
     e2e_steps = max(2, min(args.steps, 10))
     eng.sync()
     if dist:
@@ -594,8 +600,7 @@ def main():
     for _ in range(e2e_steps):
         eng.upload_state(host_state)
         eng.step(dt_frame, stream)
-        for k, f in enumerate(sc.state):
-            _capi.call("nebula_mpm_download", eng._h, k, out[f].ctypes.data_as(C.c_void_p), out[f].size)
+        _capi.call("nebula_mpm_download_state", eng._h, out_ptrs, 4 * n)
     f1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = f0.elapsed_time(f1)

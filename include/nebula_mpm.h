@@ -202,6 +202,9 @@ int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_
 /* Copy field `f` of the live particles (original particle order) to host:
  * count = 4 * live floats. */
 int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count);
+/* All 8 fields at once (P, v, F0, F1, F2, B0, B1, B2), original particle order,
+ * count = 4 * live floats per field; one unpermute and one synchronisation. */
+int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t count);
 /* MPMEngine::step (MPMEngine.cpp:404-474): numSubsteps substeps of dt/numSubsteps,
  * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream). */
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream);

@@ -109,6 +109,7 @@ _SIGS = {
     "nebula_mpm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_pipeline": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nebula_mpm_download_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nebula_mpm_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_launch_limits": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

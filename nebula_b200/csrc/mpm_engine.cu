@@ -300,6 +300,7 @@ void MPMEngine::setParticleMaterialIds(const uint32_t* ids, uint32_t n) {
     v[i] = make_float4(0.f, 0.f, 0.f, w);
   }
   if (n) check(cudaMemcpy(statePtrs(cur_).f[1], v.data(), n * sizeof(float4), cudaMemcpyHostToDevice), "upload ids");
+  ++stateVersion_;
 }
 
 void MPMEngine::setColliders(const nebula_mpm_collider* c, uint32_t n) {
@@ -409,12 +410,14 @@ uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32
   up(6, Z.data());
   up(7, Z.data());
   live_ += nNew;
+  ++stateVersion_;
   return nNew;
 }
 
 void MPMEngine::resetParticles() {
   prepareHostAccess(true);
   live_ = 0;
+  ++stateVersion_;
   std::fill(emitterDone_.begin(), emitterDone_.end(), 0);  // MPMEngine.cpp:285-286
   emitEvents_ = 0;
 }
@@ -483,8 +486,22 @@ void MPMEngine::uploadState(const float* const f[8], uint32_t n) {
   prepareHostAccess(true);
   StatePtrs st = statePtrs(cur_);
   for (int k = 0; k < 8; ++k)
-    if (n) check(cudaMemcpy(st.f[k], f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice), "upload state");
+    if (n) check(cudaMemcpyAsync(st.f[k], f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice, lastStream_), "upload state");
+  quiesce();  // the host arrays may be reused as soon as this returns
   live_ = n;
+  ++stateVersion_;
+}
+
+// The state buffer holding the current particles in their original order:
+// the current buffer, or the idle one after an unpermute (once per state version).
+StatePtrs MPMEngine::originalOrder() {
+  if (!permuted_ || !live_) return statePtrs(cur_);
+  StatePtrs tmp = statePtrs(cur_ ^ 1);  // free between substeps
+  if (unpermutedVersion_ != stateVersion_) {
+    check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, lastStream_, &launches_), "unpermute");
+    unpermutedVersion_ = stateVersion_;
+  }
+  return tmp;
 }
 
 void MPMEngine::download(int field, float* host, uint64_t count) {
@@ -492,15 +509,20 @@ void MPMEngine::download(int field, float* host, uint64_t count) {
   if (count != uint64_t(live_) * 4) throw Error(NEBULA_MPM_ERR_INVALID, "count must be 4 * live particles");
   if (count && !host) throw Error(NEBULA_MPM_ERR_INVALID, "null host buffer");
   bindDevice();
-  const float4* src = statePtrs(cur_).f[field];
-  if (permuted_ && live_) {
-    // original order into the idle buffer (free between substeps)
-    StatePtrs tmp = statePtrs(cur_ ^ 1);
-    check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, lastStream_, &launches_), "unpermute");
-    src = tmp.f[field];
-  }
+  const float4* src = originalOrder().f[field];
   quiesce();
   if (count) check(cudaMemcpy(host, src, count * sizeof(float), cudaMemcpyDeviceToHost), "download");
+}
+
+void MPMEngine::downloadState(float* const host[8], uint64_t count) {
+  if (count != uint64_t(live_) * 4) throw Error(NEBULA_MPM_ERR_INVALID, "count must be 4 * live particles");
+  for (int k = 0; k < 8; ++k)
+    if (count && (!host || !host[k])) throw Error(NEBULA_MPM_ERR_INVALID, "null host buffer");
+  bindDevice();
+  const StatePtrs src = originalOrder();
+  for (int k = 0; k < 8 && count; ++k)
+    check(cudaMemcpyAsync(host[k], src.f[k], count * sizeof(float), cudaMemcpyDeviceToHost, lastStream_), "download");
+  quiesce();
 }
 
 SubstepParams MPMEngine::buildParams(float subDt) const {
@@ -616,6 +638,7 @@ void MPMEngine::normalizeOrder(cudaStream_t s) {
   StatePtrs src = statePtrs(cur_), dst = statePtrs(cur_ ^ 1);
   check(launchUnpermute(src, static_cast<const uint32_t*>(pid_[cur_].ptr), dst, live_, s, &launches_), "unpermute");
   cur_ ^= 1;
+  ++stateVersion_;
   check(launchIota(static_cast<uint32_t*>(pid_[cur_].ptr), capacity_, s, &launches_), "iota");
   permuted_ = false;
   // the pending bins index the old order
@@ -708,6 +731,7 @@ void MPMEngine::substepDense(const SubstepParams& P, cudaStream_t s) {
 void MPMEngine::step(float dt, cudaStream_t s) {
   bindDevice();
   if (!(dt >= 0.f) || !std::isfinite(dt)) throw Error(NEBULA_MPM_ERR_INVALID, "dt must be finite and >= 0");
+  ++stateVersion_;
   if (s != lastStream_) {
     // work queued on the previous stream must finish first
     quiesce();
@@ -742,12 +766,7 @@ void MPMEngine::exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt) {
   bindDevice();
   const SubstepParams P = buildParams(0.f);
   BinBuffers b = binBuffers();
-  const float4* pos = statePtrs(cur_).f[0];
-  if (permuted_ && live_) {
-    StatePtrs tmp = statePtrs(cur_ ^ 1);
-    check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, lastStream_, &launches_), "unpermute");
-    pos = tmp.f[0];
-  }
+  const float4* pos = originalOrder().f[0];
   check(launchBin(P, pos, live_, b, lastStream_, &launches_), "bin");
   quiesce();
   check(cudaMemcpy(cnt, b.cellCount, size_t(hashCells_) * 4, cudaMemcpyDeviceToHost), "download bins");
@@ -968,6 +987,9 @@ int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_
 }
 int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count) {
   return guarded([&] { E(e).download(field, host, count); });
+}
+int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t count) {
+  return guarded([&] { E(e).downloadState(host, count); });
 }
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream) {
   return guarded([&] { E(e).step(dt, static_cast<cudaStream_t>(stream)); });

@@ -98,6 +98,8 @@ class MPMEngine {
   void resetParticles();
   void uploadState(const float* const f[8], uint32_t n);
   void download(int field, float* host, uint64_t count);
+  void downloadState(float* const host[8], uint64_t count);
+  StatePtrs originalOrder();
   void step(float dt, cudaStream_t s);
   uint32_t liveCount() const { return live_; }
   void stats(nebula_mpm_stats* s);
@@ -163,6 +165,10 @@ class MPMEngine {
   DevBuf pid_[2];
   int cur_ = 0;
   bool permuted_ = false;
+  // Bumped by every change of the particle state; the idle state buffer holds
+  // the original-order copy of version unpermutedVersion_ (downloads reuse it).
+  uint64_t stateVersion_ = 0;
+  uint64_t unpermutedVersion_ = ~uint64_t(0);
   int pipeline_ = NEBULA_MPM_PIPELINE_FUSED;
   LaunchConfig launchCfg_;
   int numSMs_ = 148;

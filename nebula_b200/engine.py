@@ -225,7 +225,12 @@ class MPMEngine:
         return out
 
     def state(self) -> dict:
-        return {f: self.download(f) for f in FIELDS}
+        """All 8 fields (one unpermute, one synchronisation)."""
+        n = self.liveParticleCount()
+        out = {f: np.empty((n, 4), np.float32) for f in FIELDS}
+        ptrs = (C.c_void_p * 8)(*[out[f].ctypes.data for f in FIELDS])
+        call("nebula_mpm_download_state", self._h, ptrs, 4 * n)
+        return out
 
     # ------------------------------------------------------------ stepping
     def step(self, dt: float, stream=None):

@@ -189,3 +189,28 @@ def test_fused_export_grid_after_step_is_p2g_of_state():
     fresh = engine_for_scene(sc2)
     fmom, fmass = fresh.export_grid(sc.params.dt)  # standalone P2G
     assert rel_l2(mom[:, :3], fmom[:, :3]) < 1e-5 and rel_l2(mass, fmass) < 1e-5
+
+
+def test_downloads_follow_every_state_change():
+    """The original-order copy behind downloads is rebuilt once per state
+    version: after each step, upload, material-id edit and reset the fields
+    read back are the current ones."""
+    sc = S.shear_block()
+    dt = sc.params.dt
+    a, b = engine_for_scene(sc), engine_for_scene(sc)
+    a.run_substeps(dt, 5)
+    p1, v1 = a.download("P"), a.download("v")
+    assert np.array_equal(a.download("P"), p1)  # same version: same copy
+    a.run_substeps(dt, 5)
+    p2 = a.download("P")
+    b.run_substeps(dt, 10)
+    pb = b.download("P")
+    assert np.abs(p2[:, :3] - p1[:, :3]).max() > 1e-5
+    assert np.linalg.norm(p2 - pb) / np.linalg.norm(pb) < 1e-6
+    a.setParticleMaterialIds(np.zeros(sc.n, np.uint32))
+    assert not a.download("v")[:, :3].any()  # the reference zeroes v with the ids
+    a.upload_state(sc.state)
+    assert np.array_equal(a.download("P"), sc.state["P"]) and np.array_equal(a.download("v"), sc.state["v"])
+    a.run_substeps(dt, 3)
+    a.resetParticles()
+    assert a.liveParticleCount() == 0
