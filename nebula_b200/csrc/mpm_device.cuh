@@ -281,6 +281,15 @@ __device__ __forceinline__ void jacobiRotateMixed(m3<double>& A, m3<double>& V) 
   const float tau = float(aqq - app) / (2.0f * float(apq));
   const float at = fabsf(tau);
   const float tf = at < 1e18f ? gsign(tau) / (at + sqrtf(1.0f + tau * tau)) : 0.5f / tau;
+  if (tf == 0.0f) {
+    // Equal diagonals: GLSL sign(0) = 0 gives t = 0, c = 1, s = 0, and the
+    // shader's update (mpm_common.glsl:229-231) then only zeroes A[p][q].  The
+    // full similarity would leave A unchanged and the loop would repeat this
+    // pivot up to its cap.
+    A.m[P0][P1] = 0.0;
+    A.m[P1][P0] = 0.0;
+    return;
+  }
   const double t = double(tf);
   const double c = rsqrt(1.0 + t * t);
   const double sn = t * c;
