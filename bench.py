@@ -379,12 +379,14 @@ def measure_adjoint(steps: int, warmup: int) -> dict:
 
 
 def measure_mesh_sdf(cpu: bool) -> dict:
-    """The collider SDF built from a triangle mesh on the GPU (nebula_mpm_mesh_sdf,
-    the reference's buildMeshSDF): a 20,480-triangle sphere into the 256^3
-    grid of the slope workload and into a 128^3 grid, timed by CUDA events
-    (median of 3 after one untimed); with `cpu`, the CPU oracle (brute force
-    over cells x triangles, OpenMP) on a 1,280-triangle sphere at 48^3 beside
-    the GPU build of the same case."""
+    """The collider SDF built from a triangle mesh on the GPU (the reference's
+    buildMeshSDF): a 20,480-triangle sphere into the 256^3 grid of the slope
+    workload and into a 128^3 grid, timed by CUDA events (median of 3 after
+    one untimed), through the prepared mesh the engine's setColliderMesh /
+    setColliderMeshPose use (nebula_mpm_mesh_build_sdf: clustered) and through
+    the one-shot call on a device list (nebula_mpm_mesh_sdf); with `cpu`, the
+    CPU oracle (brute force over cells x triangles, OpenMP) on a 1,280-triangle
+    sphere at 48^3 beside the GPU build of the same case."""
     import ctypes as C
 
     import torch
@@ -392,34 +394,47 @@ def measure_mesh_sdf(cpu: bool) -> dict:
     from nebula_b200 import _capi, mesh
     from nebula_b200 import scenes as S
 
-    def gpu_ms(tris, res):
+    def gpu_ms(tris, res, prepared):
         total = S.hash_cells((res, res, res))
-        t = torch.from_numpy(tris).cuda()
         out = torch.empty(total, dtype=torch.float32, device="cuda")
         r = (C.c_uint32 * 3)(res, res, res)
         s = torch.cuda.current_stream()
+        t = torch.from_numpy(tris).cuda()
+        m = C.c_void_p()
+        if prepared:
+            _capi.call("nebula_mpm_mesh_create", tris.ctypes.data_as(C.c_void_p), tris.shape[0], C.byref(m))
         ms = []
-        for it in range(4):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(s)
-            _capi.call("nebula_mpm_mesh_sdf", C.c_void_p(t.data_ptr()), tris.shape[0], r, total, C.c_float(1.0 / res),
-                       C.c_void_p(out.data_ptr()), C.c_void_p(s.cuda_stream))
-            e1.record(s)
-            torch.cuda.synchronize()
-            if it:
-                ms.append(e0.elapsed_time(e1))
+        try:
+            for it in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                if prepared:
+                    _capi.call("nebula_mpm_mesh_build_sdf", m, None, None, r, total, C.c_float(1.0 / res), C.c_void_p(out.data_ptr()),
+                               C.c_void_p(s.cuda_stream))
+                else:
+                    _capi.call("nebula_mpm_mesh_sdf", C.c_void_p(t.data_ptr()), tris.shape[0], r, total, C.c_float(1.0 / res),
+                               C.c_void_p(out.data_ptr()), C.c_void_p(s.cuda_stream))
+                e1.record(s)
+                torch.cuda.synchronize()
+                if it:
+                    ms.append(e0.elapsed_time(e1))
+        finally:
+            if prepared:
+                _capi.call("nebula_mpm_mesh_destroy", m)
         return float(np.median(ms)), out
 
     res = {}
     big = mesh.icosphere((0.5, 0.5, 0.5), 0.3, 5)
     for n in (256, 128):
-        res["gpu_ms_%d" % n], _ = gpu_ms(big, n)
-        res["cell_triangle_pairs_per_s_%d" % n] = n ** 3 * big.shape[0] / (res["gpu_ms_%d" % n] * 1e-3)
+        for prepared, tag in ((True, "prepared"), (False, "one_shot")):
+            ms, _ = gpu_ms(big, n, prepared)
+            res["%s_ms_%d" % (tag, n)] = ms
+            res["%s_cell_triangle_pairs_per_s_%d" % (tag, n)] = n ** 3 * big.shape[0] / (ms * 1e-3)
     res["triangles"] = int(big.shape[0])
     if cpu:
         import oracle
         small = mesh.icosphere((0.5, 0.5, 0.5), 0.3, 3)
-        g, out = gpu_ms(small, 48)
+        g, out = gpu_ms(small, 48, True)
         t0 = time.perf_counter()
         ref = oracle.mesh_sdf(small, (48, 48, 48), S.hash_cells((48, 48, 48)), 1.0 / 48)
         cms = (time.perf_counter() - t0) * 1e3

@@ -400,6 +400,20 @@ uint32_t nebula_mpm_domain_n_groups(uint32_t cells);
  * region). */
 int nebula_mpm_mesh_sdf(const float* dTris, uint32_t nTris, const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf,
                         void* stream);
+/* A mesh prepared on the device for repeated SDF builds (a moving obstacle):
+ * triangles sorted by the Morton code of their centroids and grouped in
+ * clusters of 32 with bounding spheres, so that the build culls clusters
+ * before triangles.  Same result as nebula_mpm_mesh_sdf on the same list
+ * (ties in distance go to the earlier triangle of the list).  tris: n host
+ * records of 12 floats (normal, v0, v1, v2).  Used by
+ * nebula_mpm_set_collider_mesh / _pose. */
+typedef struct nebula_mpm_mesh nebula_mpm_mesh;
+int nebula_mpm_mesh_create(const float* tris, uint32_t n, nebula_mpm_mesh** out);
+int nebula_mpm_mesh_destroy(nebula_mpm_mesh* m);
+/* buildMeshSDF(transformTriangles(tris, translation, rotation), realRes, totalCells, cellSize)
+ * into dSdf on `stream`; null translation / rotation = identity. */
+int nebula_mpm_mesh_build_sdf(const nebula_mpm_mesh* m, const float translation[3], const float rotation_wxyz[4], const uint32_t realRes[3],
+                              uint32_t totalCells, float cellSize, float* dSdf, void* stream);
 /* The same of transformTriangles(tris, translation, rotation) (MeshSDF.h:134-141),
  * the pose applied on the device; a null translation or rotation is the identity. */
 int nebula_mpm_mesh_sdf_posed(const float* dTris, uint32_t nTris, const float translation[3], const float rotation_wxyz[4],

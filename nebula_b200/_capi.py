@@ -90,6 +90,9 @@ _SIGS = {
     "nebula_mpm_clear_collider": (C.c_int, [C.c_void_p]),
     "nebula_mpm_set_collider_mesh": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "nebula_mpm_mesh_sdf": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32 * 3, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_mesh_create": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "nebula_mpm_mesh_destroy": (C.c_int, [C.c_void_p]),
+    "nebula_mpm_mesh_build_sdf": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32 * 3, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]),
     "nebula_mpm_mesh_sdf_posed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32 * 3, C.c_uint32, C.c_float,
                                             C.c_void_p, C.c_void_p]),
     "nebula_mpm_set_collider_mesh_pose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

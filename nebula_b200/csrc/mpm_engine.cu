@@ -351,31 +351,29 @@ void MPMEngine::setColliderSphere(float radius, float cx, float cy, float cz) {
 void MPMEngine::clearCollider() { hasSdf_ = false; }
 
 // setColliderSDF(buildMeshSDF(tris, gridRes, hashCells, cellSize)) (MeshSDF.h:98-132),
-// the SDF built on the GPU straight into the engine's SDF buffer.  The
-// triangles stay on the device for setColliderMeshPose.
+// the SDF built on the GPU straight into the engine's SDF buffer.  The mesh
+// stays on the device, prepared (clustered), for setColliderMeshPose.
 void MPMEngine::setColliderMesh(const float* tris, uint32_t n) {
-  checkMeshArgs(tris, n);  // the host array needs no alignment: only null / count are checked here
-  prepareHostAccess(false);  // a queued substep may still read the old SDF
-  meshTris_.ensure(std::max<size_t>(size_t(n) * 12 * sizeof(float), 16));
-  if (n) check(cudaMemcpy(meshTris_.ptr, tris, size_t(n) * 12 * sizeof(float), cudaMemcpyHostToDevice), "upload triangles");
-  meshN_ = n;
+  checkMeshArgs(tris, n);
+  prepareHostAccess(false);  // a queued substep or rebuild may still read the old SDF or mesh
+  mesh_.build(tris, n);
   hasMesh_ = true;
   sdf_.ensure(size_t(hashCells_) * sizeof(float));
-  check(launchMeshSdf(static_cast<const float*>(meshTris_.ptr), n, meshPose(nullptr, nullptr), gridRes_, hashCells_, cfg_.cellSize,
-                      static_cast<float*>(sdf_.ptr), lastStream_, &launches_),
+  check(launchMeshSdfPrepared(mesh_, meshPose(nullptr, nullptr), gridRes_, hashCells_, cfg_.cellSize, static_cast<float*>(sdf_.ptr), lastStream_,
+                              &launches_),
         "mesh sdf");
   hasSdf_ = true;
 }
 
 // The moving-obstacle rebuild (examples/pyro_basic.cpp:130-134:
 // setColliderSDF(buildMeshSDF(transformTriangles(base, t, q), ...))) from the
-// triangles of the last setColliderMesh, posed and rebuilt on the device.
+// mesh of the last setColliderMesh, posed and rebuilt on the device.
 // Ordered on the engine's stream after the substeps already queued.
 void MPMEngine::setColliderMeshPose(const float* translation, const float* rotationWxyz) {
   if (!hasMesh_) throw Error(NEBULA_MPM_ERR_INVALID, "no collider mesh: call setColliderMesh first");
   if (!translation || !rotationWxyz) throw Error(NEBULA_MPM_ERR_INVALID, "null pose");
-  check(launchMeshSdf(static_cast<const float*>(meshTris_.ptr), meshN_, meshPose(translation, rotationWxyz), gridRes_, hashCells_,
-                      cfg_.cellSize, static_cast<float*>(sdf_.ptr), lastStream_, &launches_),
+  check(launchMeshSdfPrepared(mesh_, meshPose(translation, rotationWxyz), gridRes_, hashCells_, cfg_.cellSize, static_cast<float*>(sdf_.ptr),
+                              lastStream_, &launches_),
         "mesh sdf");
   hasSdf_ = true;
 }

@@ -73,6 +73,22 @@ struct DevBuf {
   void reset();
 };
 
+// A triangle mesh prepared for repeated SDF builds: triangles sorted by the
+// Morton code of their centroids (device, 12 floats each), their indices in
+// the caller's list, and the bounding sphere of every run of kMeshCluster
+// sorted triangles (centre, radius).  Built on the host from a host list.
+constexpr uint32_t kMeshCluster = 32;
+struct PreparedMesh {
+  uint32_t n = 0, clusters = 0;
+  DevBuf tris, index, spheres;
+  void build(const float* hostTris, uint32_t n);
+};
+// SDF of a prepared mesh, posed by `pose` (same result as launchMeshSdf on
+// the caller's list).
+cudaError_t launchMeshSdfPrepared(const PreparedMesh& m, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
+                                  float* dSdf, cudaStream_t s, uint64_t* launches);
+
+
 class MPMEngine {
  public:
   explicit MPMEngine(const nebula_mpm_config& cfg);
@@ -182,8 +198,8 @@ class MPMEngine {
   bool denseReady_ = false;
   DevBuf gridMom_, gridMass_;
   DevBuf cellCount_, cellStart_, cellEnd_, key_, rank_, sortedTmp_, sorted_, scanWs_;
-  DevBuf materials_, colliders_, forces_, sdf_, err_, meshTris_;
-  uint32_t meshN_ = 0;
+  DevBuf materials_, colliders_, forces_, sdf_, err_;
+  PreparedMesh mesh_;
   bool hasMesh_ = false;
   std::vector<Material> hostMaterials_;
   uint32_t colliderCount_ = 0;

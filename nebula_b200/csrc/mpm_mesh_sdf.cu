@@ -27,7 +27,12 @@
 // Every skipped triangle is strictly farther than the cell's closest one (the
 // bounds carry a margin above float rounding), so the distances and the
 // winning triangle are those of the brute-force loop.
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
 
 #include "mpm_device.cuh"
 #include "mpm_engine.h"
@@ -219,6 +224,211 @@ __global__ void __launch_bounds__(kThreads) k_mesh_sdf(const float4* __restrict_
   if (code < totalCells) sdf[code] = inside ? (outer ? best : -best) : 1e9f;
 }
 
+// ---------------------------------------------------------------- prepared meshes
+// The same SDF from a prepared mesh: triangles sorted by the Morton code of
+// their centroids and grouped in clusters of 32 with a bounding sphere each,
+// so culling works on clusters before triangles.  Per CTA (the 256 cells of an
+// 8 x 8 x 4 box):
+//   1. U from one vertex of every cluster (a point on the mesh).
+//   2. Clusters in tiles of 256: those whose sphere comes within U of the box
+//      are compacted; eight at a time, warp w stages the 32 triangles of one
+//      of them and keeps those whose own sphere comes within U of the box.
+//   3. Each thread first tests the triangles of the cluster that gave U (near
+//      every cell of the box), then skips any cluster whose sphere is no
+//      closer than min(its best so far, U) and tests the kept triangles of
+//      the others as before.
+// Triangles are visited out of list order, so a tie in distance goes to the
+// smaller list index: the first triangle of the list reaching the minimum,
+// as in the brute-force loop.
+__device__ __forceinline__ void loadTriS(const float4* __restrict__ t4, uint32_t k, const MeshPose& pose, float eps, TriS& t) {
+  float v[12];
+  loadTri(t4, k, pose, v);
+  t.nx = v[0]; t.ny = v[1]; t.nz = v[2];
+  t.ax = v[3]; t.ay = v[4]; t.az = v[5];
+  t.bx = v[6] - v[3]; t.by = v[7] - v[4]; t.bz = v[8] - v[5];
+  t.cx = v[9] - v[3]; t.cy = v[10] - v[4]; t.cz = v[11] - v[5];
+  t.sx = (v[3] + v[6] + v[9]) * (1.0f / 3.0f);
+  t.sy = (v[4] + v[7] + v[10]) * (1.0f / 3.0f);
+  t.sz = (v[5] + v[8] + v[11]) * (1.0f / 3.0f);
+  float rr = 0.f;
+#pragma unroll
+  for (int j = 1; j < 4; ++j) {
+    const float dx = v[3 * j] - t.sx, dy = v[3 * j + 1] - t.sy, dz = v[3 * j + 2] - t.sz;
+    rr = fmaxf(rr, dx * dx + dy * dy + dz * dz);
+  }
+  t.sr = sqrtf(rr) * 1.0001f + eps;
+}
+
+// Distance from point s to the box [lo, hi] (0 inside).
+__device__ __forceinline__ float boxDistance(float lox, float loy, float loz, float hix, float hiy, float hiz, float sx, float sy, float sz) {
+  const float gx = fmaxf(fmaxf(lox - sx, sx - hix), 0.f), gy = fmaxf(fmaxf(loy - sy, sy - hiy), 0.f), gz = fmaxf(fmaxf(loz - sz, sz - hiz), 0.f);
+  return sqrtf(gx * gx + gy * gy + gz * gz);
+}
+
+__global__ void __launch_bounds__(kThreads) k_mesh_sdf_clusters(const float4* __restrict__ tris, const uint32_t* __restrict__ index,
+                                                                const float4* __restrict__ spheres, uint32_t n, uint32_t nClusters, MeshPose pose,
+                                                                int rx, int ry, int rz, uint32_t totalCells, float cs, float eps,
+                                                                float* __restrict__ sdf) {
+  constexpr int kWarps = kThreads / 32;
+  __shared__ TriS tile[kThreads];
+  __shared__ uint32_t tileIdx[kThreads];
+  __shared__ float4 clus[kThreads];       // surviving clusters of the current cluster tile: posed centre, radius
+  __shared__ uint32_t clusId[kThreads];
+  __shared__ uint32_t warpCount[kWarps];
+  __shared__ uint32_t runStart[kWarps + 1];  // kept triangles of the staged clusters: [runStart[w], runStart[w + 1])
+  __shared__ unsigned long long boundKey;    // (U^2 bits, cluster): the bound and the cluster that gave it
+  const uint32_t base = blockIdx.x * kThreads;
+  const uint32_t code = base + threadIdx.x;
+  int bx0, by0, bz0;
+  mortonDecode(base, bx0, by0, bz0);
+  if (bx0 >= rx || by0 >= ry || bz0 >= rz) {
+    if (code < totalCells) sdf[code] = 1e9f;
+    return;
+  }
+  int bx1, by1, bz1;
+  mortonDecode(base | uint32_t(kThreads - 1), bx1, by1, bz1);
+  const float lox = (float(bx0) + 0.5f) * cs, loy = (float(by0) + 0.5f) * cs, loz = (float(bz0) + 0.5f) * cs;
+  const float hix = (float(min(bx1, rx - 1)) + 0.5f) * cs, hiy = (float(min(by1, ry - 1)) + 0.5f) * cs, hiz = (float(min(bz1, rz - 1)) + 0.5f) * cs;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  // 1. U^2 over the box from the first vertex of every cluster, and the
+  //    cluster that gives it (non-negative floats order as their bits)
+  if (threadIdx.x == 0) boundKey = ~0ull;
+  __syncthreads();
+  unsigned long long key = ~0ull;
+  for (uint32_t c = threadIdx.x; c < nClusters; c += kThreads) {
+    float v[12];
+    loadTri(tris, c * kMeshCluster, pose, v);
+    const float ex = fmaxf(v[3] - lox, hix - v[3]), ey = fmaxf(v[4] - loy, hiy - v[4]), ez = fmaxf(v[5] - loz, hiz - v[5]);
+    const unsigned long long k = (static_cast<unsigned long long>(__float_as_uint(ex * ex + ey * ey + ez * ez)) << 32) | c;
+    key = k < key ? k : key;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  if (lane == 0) atomicMin(&boundKey, key);
+  __syncthreads();
+  const unsigned long long bk = boundKey;
+  const float U = nClusters ? sqrtf(__uint_as_float(uint32_t(bk >> 32))) * (1.0f + 1e-5f) + eps : INFINITY;
+  const uint32_t firstCluster = uint32_t(bk & 0xffffffffu);
+
+  int ix = 0, iy = 0, iz = 0;
+  if (code < totalCells) mortonDecode(code, ix, iy, iz);
+  const bool inside = code < totalCells && ix < rx && iy < ry && iz < rz;
+  const float px = (float(ix) + 0.5f) * cs, py = (float(iy) + 0.5f) * cs, pz = (float(iz) + 0.5f) * cs;
+  float best = 1e9f;
+  uint32_t bestIdx = 0xffffffffu;
+  bool outer = true;
+  auto visit = [&](const TriS& s, uint32_t id) {
+    const float fx = px - s.sx, fy = py - s.sy, fz = pz - s.sz;
+    const float dt = sqrtf(fx * fx + fy * fy + fz * fz);
+    if (dt - s.sr >= fminf(best, U)) return;  // every point of the triangle is at least this far
+    float qx, qy, qz;
+    closestOnTriangle(s, px, py, pz, qx, qy, qz);
+    const float dx = px - qx, dy = py - qy, dz = pz - qz;
+    const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+    if (d < best || (d == best && id < bestIdx)) {
+      best = d;
+      bestIdx = id;
+      outer = dot3f(dx, dy, dz, s.nx, s.ny, s.nz) >= 0.f;
+    }
+  };
+  // the cluster that gave U first: near every cell of the box, it makes each
+  // thread's bound tight before the other clusters are tested
+  if (nClusters) {
+    if (warp == 0) {
+      const uint32_t t = firstCluster * kMeshCluster + lane;
+      if (t < n) {
+        loadTriS(tris, t, pose, eps, tile[lane]);
+        tileIdx[lane] = index[t];
+      }
+    }
+    __syncthreads();
+    if (inside) {
+      const uint32_t m = min(kMeshCluster, n - firstCluster * kMeshCluster);
+      for (uint32_t j = 0; j < m; ++j) visit(tile[j], tileIdx[j]);
+    }
+  }
+  for (uint32_t c0 = 0; c0 < nClusters; c0 += kThreads) {
+    // 2a. the tile's clusters that can hold the closest triangle of some cell of the box
+    const uint32_t c = c0 + threadIdx.x;
+    bool keep = false;
+    float4 sph = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c < nClusters) {
+      sph = spheres[c];
+      if (pose.posed) {
+        rotate(pose, sph.x, sph.y, sph.z);
+        sph.x += pose.t[0];
+        sph.y += pose.t[1];
+        sph.z += pose.t[2];
+      }
+      keep = boxDistance(lox, loy, loz, hix, hiy, hiz, sph.x, sph.y, sph.z) - sph.w <= U;
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+    __syncthreads();  // the previous cluster tile is consumed
+    if (lane == 0) warpCount[warp] = __popc(mask);
+    __syncthreads();
+    uint32_t off = 0, mC = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t k = warpCount[w];
+      off += uint32_t(w) < warp ? k : 0u;
+      mC += k;
+    }
+    if (keep) {
+      const uint32_t at = off + __popc(mask & ((1u << lane) - 1u));
+      clus[at] = sph;
+      clusId[at] = c;
+    }
+    __syncthreads();
+    for (uint32_t k0 = 0; k0 < mC; k0 += kWarps) {
+      // 2b. warp w stages the triangles of surviving cluster k0 + w
+      const uint32_t kc = k0 + warp;
+      const uint32_t t = kc < mC ? clusId[kc] * kMeshCluster + lane : n;
+      TriS tri;
+      bool keepT = false;
+      if (t < n) {
+        loadTriS(tris, t, pose, eps, tri);
+        keepT = boxDistance(lox, loy, loz, hix, hiy, hiz, tri.sx, tri.sy, tri.sz) - tri.sr <= U;
+      }
+      const uint32_t tm = __ballot_sync(0xffffffffu, keepT);
+      __syncthreads();  // the previous staging is consumed
+      if (lane == 0) warpCount[warp] = __popc(tm);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int w = 0; w < kWarps; ++w) {
+          runStart[w] = acc;
+          acc += warpCount[w];
+        }
+        runStart[kWarps] = acc;
+      }
+      uint32_t toff = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) toff += uint32_t(w) < warp ? warpCount[w] : 0u;
+      if (keepT) {
+        const uint32_t at = toff + __popc(tm & ((1u << lane) - 1u));
+        tile[at] = tri;
+        tileIdx[at] = index[t];
+      }
+      __syncthreads();
+      if (!inside) continue;
+      // 3. per cell: clusters first, then their kept triangles
+      const uint32_t nk = min(uint32_t(kWarps), mC - k0);
+      for (uint32_t w = 0; w < nk; ++w) {
+        const float4 cw = clus[k0 + w];
+        const float ex = px - cw.x, ey = py - cw.y, ez = pz - cw.z;
+        const float dc = sqrtf(ex * ex + ey * ey + ez * ez);
+        if (dc - cw.w >= fminf(best, U)) continue;  // every point of the cluster is at least this far
+        for (uint32_t j = runStart[w]; j < runStart[w + 1]; ++j) visit(tile[j], tileIdx[j]);
+      }
+    }
+  }
+  if (code < totalCells) sdf[code] = inside ? (outer ? best : -best) : 1e9f;
+}
+
 }  // namespace
 
 cudaError_t launchMeshSdf(const float* dTris, uint32_t n, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
@@ -232,6 +442,85 @@ cudaError_t launchMeshSdf(const float* dTris, uint32_t n, const MeshPose& pose, 
                                                                          int(res[1]), int(res[2]), totalCells, cellSize, eps, dSdf);
   ++*launches;
   return cudaGetLastError();
+}
+
+cudaError_t launchMeshSdfPrepared(const PreparedMesh& m, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
+                                  float* dSdf, cudaStream_t s, uint64_t* launches) {
+  if (totalCells == 0) return cudaSuccess;
+  const float extent = cellSize * float(domainCubeRes(res));
+  const float eps = 1e-5f * fmaxf(extent, 1.0f);
+  k_mesh_sdf_clusters<<<(totalCells + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+      static_cast<const float4*>(m.tris.ptr), static_cast<const uint32_t*>(m.index.ptr), static_cast<const float4*>(m.spheres.ptr), m.n, m.clusters,
+      pose, int(res[0]), int(res[1]), int(res[2]), totalCells, cellSize, eps, dSdf);
+  ++*launches;
+  return cudaGetLastError();
+}
+
+// Sort by the Morton code of the centroid (10 bits per axis over the mesh's
+// bounding box; ties by list index), group runs of kMeshCluster, and bound
+// each run by the sphere around its vertices' bounding box.
+void PreparedMesh::build(const float* h, uint32_t count) {
+  checkMeshArgs(h, count);
+  n = count;
+  clusters = (count + kMeshCluster - 1) / kMeshCluster;
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  std::vector<float> cen(size_t(count) * 3);
+  for (uint32_t k = 0; k < count; ++k)
+    for (int a = 0; a < 3; ++a) {
+      const float c = (h[12 * size_t(k) + 3 + a] + h[12 * size_t(k) + 6 + a] + h[12 * size_t(k) + 9 + a]) / 3.0f;
+      cen[3 * size_t(k) + a] = c;
+      if (std::isfinite(c)) {
+        lo[a] = std::min(lo[a], c);
+        hi[a] = std::max(hi[a], c);
+      }
+    }
+  std::vector<uint64_t> key(count);
+  for (uint32_t k = 0; k < count; ++k) {
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) {
+      const float ext = hi[a] > lo[a] ? hi[a] - lo[a] : 1.0f;
+      float u = (cen[3 * size_t(k) + a] - lo[a]) / ext * 1023.0f;
+      u = std::isfinite(u) ? std::min(std::max(u, 0.0f), 1023.0f) : 0.0f;
+      q[a] = uint32_t(u);
+    }
+    key[k] = (uint64_t(mortonEncode(int(q[0]), int(q[1]), int(q[2]))) << 32) | k;
+  }
+  std::sort(key.begin(), key.end());
+  std::vector<float> sorted(size_t(count) * 12);
+  std::vector<uint32_t> idx(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    idx[i] = uint32_t(key[i] & 0xffffffffu);
+    std::memcpy(&sorted[12 * size_t(i)], h + 12 * size_t(idx[i]), 12 * sizeof(float));
+  }
+  std::vector<float4> sph(std::max(clusters, 1u));
+  for (uint32_t c = 0; c < clusters; ++c) {
+    const uint32_t t0 = c * kMeshCluster, t1 = std::min(count, t0 + kMeshCluster);
+    float l[3] = {INFINITY, INFINITY, INFINITY}, u[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t t = t0; t < t1; ++t)
+      for (int v = 1; v < 4; ++v)
+        for (int a = 0; a < 3; ++a) {
+          l[a] = std::min(l[a], sorted[12 * size_t(t) + 3 * v + a]);
+          u[a] = std::max(u[a], sorted[12 * size_t(t) + 3 * v + a]);
+        }
+    const float cx = 0.5f * (l[0] + u[0]), cy = 0.5f * (l[1] + u[1]), cz = 0.5f * (l[2] + u[2]);
+    double r2 = 0.0;
+    for (uint32_t t = t0; t < t1; ++t)
+      for (int v = 1; v < 4; ++v) {
+        const double dx = double(sorted[12 * size_t(t) + 3 * v]) - cx, dy = double(sorted[12 * size_t(t) + 3 * v + 1]) - cy,
+                     dz = double(sorted[12 * size_t(t) + 3 * v + 2]) - cz;
+        r2 = std::max(r2, dx * dx + dy * dy + dz * dz);
+      }
+    // covers the cluster despite the device's float rounding of posed points
+    sph[c] = make_float4(cx, cy, cz, float(std::sqrt(r2)) * 1.0001f + 1e-6f * std::max(1.0f, std::fabs(cx) + std::fabs(cy) + std::fabs(cz)));
+  }
+  tris.ensure(std::max<size_t>(sorted.size() * sizeof(float), 16));
+  index.ensure(std::max<size_t>(idx.size() * sizeof(uint32_t), 16));
+  spheres.ensure(sph.size() * sizeof(float4));
+  if (count) {
+    check(cudaMemcpy(tris.ptr, sorted.data(), sorted.size() * sizeof(float), cudaMemcpyHostToDevice), "upload mesh");
+    check(cudaMemcpy(index.ptr, idx.data(), idx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload mesh");
+    check(cudaMemcpy(spheres.ptr, sph.data(), size_t(clusters) * sizeof(float4), cudaMemcpyHostToDevice), "upload mesh");
+  }
 }
 
 MeshPose meshPose(const float* translation, const float* rotationWxyz) {
@@ -254,7 +543,63 @@ void checkMeshArgs(const float* tris, uint32_t nTris) {
 
 using namespace nebula;
 
+struct nebula_mpm_mesh {
+  nebula::PreparedMesh mesh;
+};
+
+namespace {
+template <class F> int guardedMesh(F&& f) {
+  try {
+    f();
+    return NEBULA_MPM_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return NEBULA_MPM_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return NEBULA_MPM_ERR_INVALID;
+  }
+}
+void checkGrid(const uint32_t realRes[3], uint32_t totalCells, float cellSize, const float* dSdf) {
+  if (!realRes || !dSdf) throw Error(NEBULA_MPM_ERR_INVALID, "null argument");
+  if (!(cellSize > 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "cellSize must be > 0");
+  if (!realRes[0] || !realRes[1] || !realRes[2]) throw Error(NEBULA_MPM_ERR_INVALID, "realRes must be >= 1");
+  const uint32_t cube = domainCubeRes(realRes);
+  if (cube > 1024u || uint64_t(totalCells) < uint64_t(cube) * cube * cube)
+    throw Error(NEBULA_MPM_ERR_INVALID, "totalCells must hold the Morton cube of realRes (cubeRes <= 1024)");
+}
+}  // namespace
+
 extern "C" {
+
+int nebula_mpm_mesh_create(const float* tris, uint32_t n, nebula_mpm_mesh** out) {
+  return guardedMesh([&] {
+    if (!out) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    auto m = std::make_unique<nebula_mpm_mesh>();
+    m->mesh.build(tris, n);
+    *out = m.release();
+  });
+}
+
+int nebula_mpm_mesh_destroy(nebula_mpm_mesh* m) {
+  delete m;
+  return NEBULA_MPM_OK;
+}
+
+int nebula_mpm_mesh_build_sdf(const nebula_mpm_mesh* m, const float translation[3], const float rotation_wxyz[4], const uint32_t realRes[3],
+                              uint32_t totalCells, float cellSize, float* dSdf, void* stream) {
+  return guardedMesh([&] {
+    if (!m) throw Error(NEBULA_MPM_ERR_INVALID, "null mesh");
+    checkGrid(realRes, totalCells, cellSize, dSdf);
+    uint64_t l = 0;
+    check(launchMeshSdfPrepared(m->mesh, meshPose(translation, rotation_wxyz), realRes, totalCells, cellSize, dSdf, static_cast<cudaStream_t>(stream),
+                                &l),
+          "mesh sdf");
+  });
+}
 
 int nebula_mpm_mesh_sdf(const float* dTris, uint32_t nTris, const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf,
                         void* stream) {

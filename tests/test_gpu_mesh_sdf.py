@@ -15,18 +15,34 @@ from nebula_b200.engine import engine_for_scene
 pytestmark = pytest.mark.gpu
 
 
-def gpu_mesh_sdf(tris, res, total, h):
-    t = torch.from_numpy(np.ascontiguousarray(tris, np.float32)).cuda()
+def gpu_mesh_sdf(tris, res, total, h, prepared=False, t=None, q=None):
+    """nebula_mpm_mesh_sdf[_posed] on device triangles, or a prepared mesh
+    (nebula_mpm_mesh_create + _build_sdf) from the host list."""
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 12)
     out = torch.empty(total, dtype=torch.float32, device="cuda")
     r = (C.c_uint32 * 3)(*res)
-    _capi.call("nebula_mpm_mesh_sdf", C.c_void_p(t.data_ptr()), tris.shape[0], r, total, C.c_float(h), C.c_void_p(out.data_ptr()),
-               C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    torch.cuda.synchronize()
+    tp = None if t is None else np.ascontiguousarray(t, np.float32).ctypes.data_as(C.c_void_p)
+    qp = None if q is None else np.ascontiguousarray(q, np.float32).ctypes.data_as(C.c_void_p)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if prepared:
+        m = C.c_void_p()
+        _capi.call("nebula_mpm_mesh_create", tris.ctypes.data_as(C.c_void_p), tris.shape[0], C.byref(m))
+        try:
+            _capi.call("nebula_mpm_mesh_build_sdf", m, tp, qp, r, total, C.c_float(h), C.c_void_p(out.data_ptr()), stream)
+            torch.cuda.synchronize()
+        finally:
+            _capi.call("nebula_mpm_mesh_destroy", m)
+    else:
+        d = torch.from_numpy(tris).cuda()
+        _capi.call("nebula_mpm_mesh_sdf_posed", C.c_void_p(d.data_ptr()), tris.shape[0], tp, qp, r, total, C.c_float(h), C.c_void_p(out.data_ptr()),
+                   stream)
+        torch.cuda.synchronize()
     return out.cpu().numpy()
 
 
+@pytest.mark.parametrize("prepared", [False, True])
 @pytest.mark.parametrize("case", ["sphere_32", "torus_48", "sphere_non_cubic", "coarse_sphere_80"])
-def test_mesh_sdf_matches_oracle(case):
+def test_mesh_sdf_matches_oracle(case, prepared):
     if case == "coarse_sphere_80":  # fewer triangles than one shared-memory tile
         tris, res, total, h = mesh.icosphere((0.45, 0.5, 0.55), 0.3, 1), (20, 20, 20), 32 ** 3, 1 / 20
     elif case == "sphere_32":
@@ -35,7 +51,7 @@ def test_mesh_sdf_matches_oracle(case):
         tris, res, total, h = mesh.torus((0.5, 0.5, 0.5), 0.25, 0.08, 48, 24), (48, 48, 48), 64 ** 3, 1 / 48
     else:
         tris, res, total, h = mesh.icosphere((0.4, 0.5, 0.6), 0.2, 2), (24, 40, 32), 64 ** 3, 1 / 40
-    got = gpu_mesh_sdf(tris, res, total, h)
+    got = gpu_mesh_sdf(tris, res, total, h, prepared)
     want = oracle.mesh_sdf(tris, res, total, h)
     assert np.all((got == np.float32(1e9)) == (want == np.float32(1e9)))
     assert np.abs(got - want).max() < 1e-5
@@ -43,25 +59,36 @@ def test_mesh_sdf_matches_oracle(case):
     assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
 
 
-def test_posed_mesh_sdf_matches_oracle_of_moved_mesh():
-    """transformTriangles on the device (nebula_mpm_mesh_sdf_posed) against the
-    oracle of the mesh moved on the host: a torus tilted 30 degrees about x."""
+@pytest.mark.parametrize("prepared", [False, True])
+def test_posed_mesh_sdf_matches_oracle_of_moved_mesh(prepared):
+    """transformTriangles on the device against the oracle of the mesh moved on
+    the host: a torus tilted 30 degrees about x."""
     tris = mesh.torus((0.0, 0.0, 0.0), 0.22, 0.07, 40, 20)
     t = np.array([0.5, 0.45, 0.52], np.float32)
     half = np.radians(15.0)
     q = np.array([np.cos(half), np.sin(half), 0.0, 0.0], np.float32)
     res, total, h = (40, 40, 40), 64 ** 3, 1 / 40
-    d = torch.from_numpy(tris).cuda()
-    out = torch.empty(total, dtype=torch.float32, device="cuda")
-    r = (C.c_uint32 * 3)(*res)
-    _capi.call("nebula_mpm_mesh_sdf_posed", C.c_void_p(d.data_ptr()), tris.shape[0], t.ctypes.data_as(C.c_void_p), q.ctypes.data_as(C.c_void_p),
-               r, total, C.c_float(h), C.c_void_p(out.data_ptr()), None)
-    torch.cuda.synchronize()
-    got = out.cpu().numpy()
+    got = gpu_mesh_sdf(tris, res, total, h, prepared, t, q)
     want = oracle.mesh_sdf(mesh.transform_triangles(tris, t, q), res, total, h)
     assert np.abs(got - want).max() < 1e-5
     clear = np.abs(want) > 1e-5
     assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
+
+
+def test_prepared_mesh_breaks_ties_by_list_order():
+    """Every triangle twice, the copy with its normal flipped: equal distances,
+    so the sign is the earlier copy's.  The prepared mesh visits triangles out
+    of list order and must still pick the earlier one."""
+    base = mesh.icosphere((0.5, 0.5, 0.5), 0.25, 2)
+    flipped = base.copy()
+    flipped[:, 0:3] *= -1.0
+    res, total, h = (32, 32, 32), 32 ** 3, 1 / 32
+    for tris in (np.concatenate([base, flipped]), np.concatenate([flipped, base])):
+        want = oracle.mesh_sdf(tris, res, total, h)
+        got = gpu_mesh_sdf(tris, res, total, h, True)
+        assert np.abs(got - want).max() < 1e-5
+        clear = np.abs(want) > 1e-5
+        assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
 
 
 def test_engine_mesh_pose_equals_uploaded_sdf_of_moved_mesh():
