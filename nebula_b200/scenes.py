@@ -194,6 +194,17 @@ def gravity(g=(0.0, -9.8, 0.0)):
     return f[0]
 
 
+def wind(direction=(1.0, 0.0, 0.0), strength=1.0, affect_mask=0):
+    """A ConstantWindForce record (Force.h:152-170): v += dir * strength * dt on
+    grid nodes; affect_mask 0 = every engine, else bit 0 selects MPM."""
+    f = np.zeros(1, FORCE_DTYPE)
+    f["type"] = FORCE_CONSTANT_WIND
+    f["affectMask"] = affect_mask
+    f["data"][0, :3] = direction
+    f["data"][0, 3] = strength
+    return f[0]
+
+
 def sphere_collider(center, radius, vel=(0, 0, 0), restitution=0.3, friction=0.0):
     c = np.zeros(1, COLLIDER_DTYPE)
     c["type"] = COLL_SPHERE

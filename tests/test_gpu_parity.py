@@ -246,6 +246,21 @@ def test_trajectory_elastic_shear_100_substeps():
     assert ex <= 1e-4 and eF <= 1e-4
 
 
+def test_trajectory_wind_and_masked_force_50_substeps():
+    """Gravity, a constant wind (Force.h:152-170) and a second wind whose
+    affect mask leaves MPM out (bit 0 clear): 50 substeps vs the oracle."""
+    sc = S.shear_block()
+    sc.params.forces = [S.gravity(), S.wind((0.6, 0.0, 0.8), 3.0), S.wind((0.0, 1.0, 0.0), 50.0, affect_mask=2)]
+    gs, r = run_pair(sc, 50, ["ref32"])
+    ex = rel_l2(gs["P"][:, :3], r["ref32"]["P"][:, :3])
+    ev = rel_l2(gs["v"][:, :3], r["ref32"]["v"][:, :3])
+    assert ex <= 1e-5 and ev <= 1e-4
+    # the wind moved the block: mean velocity has the wind's x and z parts (3 m/s^2 over 50 * dt)
+    vm = gs["v"][:, :3].mean(axis=0) - sc.state["v"][:, :3].mean(axis=0)
+    t = 50 * sc.params.dt
+    assert abs(vm[0] - 0.6 * 3.0 * t) < 0.2 * 0.6 * 3.0 * t and abs(vm[2] - 0.8 * 3.0 * t) < 0.2 * 0.8 * 3.0 * t
+
+
 def test_trajectory_elastic_block_as_specified_20_substeps():
     """The 8,000-particle block with rho = 1 is unstable beyond ~30 substeps in
     the reference algorithm itself; its first 20 substeps are compared."""
