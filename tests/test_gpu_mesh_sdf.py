@@ -138,3 +138,18 @@ def test_empty_mesh_and_argument_checks():
     for total, h in ((8 ** 3 - 1, 0.125), (8 ** 3, 0.0)):
         with pytest.raises(_capi.NebulaError):
             _capi.call("nebula_mpm_mesh_sdf", None, 0, r, total, C.c_float(h), C.c_void_p(out.data_ptr()), None)
+
+
+@pytest.mark.parametrize("count", [0, 1, 33])
+def test_prepared_mesh_small_counts(count):
+    """No triangle (every cell 1e9), one triangle, and one more than a cluster."""
+    base = mesh.icosphere((0.5, 0.5, 0.5), 0.3, 2)[:count]
+    res, total, h = (16, 16, 16), 16 ** 3, 1 / 16
+    got = gpu_mesh_sdf(base, res, total, h, True)
+    if count == 0:
+        assert np.all(got == np.float32(1e9))
+        return
+    want = oracle.mesh_sdf(base, res, total, h)
+    assert np.abs(got - want).max() < 1e-5
+    clear = np.abs(want) > 1e-5
+    assert np.array_equal(np.sign(got[clear]), np.sign(want[clear]))
