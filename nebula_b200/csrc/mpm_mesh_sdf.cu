@@ -608,27 +608,15 @@ int nebula_mpm_mesh_sdf(const float* dTris, uint32_t nTris, const uint32_t realR
 
 int nebula_mpm_mesh_sdf_posed(const float* dTris, uint32_t nTris, const float translation[3], const float rotationWxyz[4],
                               const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream) {
-  try {
-    if (!realRes || !dSdf) throw Error(NEBULA_MPM_ERR_INVALID, "null argument");
+  return guardedMesh([&] {
+    checkGrid(realRes, totalCells, cellSize, dSdf);
     checkMeshArgs(dTris, nTris);
     if (reinterpret_cast<uintptr_t>(dTris) % 16u) throw Error(NEBULA_MPM_ERR_INVALID, "triangles must be 16-byte aligned");
-    if (!(cellSize > 0.f)) throw Error(NEBULA_MPM_ERR_INVALID, "cellSize must be > 0");
-    if (!realRes[0] || !realRes[1] || !realRes[2]) throw Error(NEBULA_MPM_ERR_INVALID, "realRes must be >= 1");
-    const uint32_t cube = domainCubeRes(realRes);
-    if (cube > 1024u || uint64_t(totalCells) < uint64_t(cube) * cube * cube)
-      throw Error(NEBULA_MPM_ERR_INVALID, "totalCells must hold the Morton cube of realRes (cubeRes <= 1024)");
     uint64_t l = 0;
     check(launchMeshSdf(dTris, nTris, meshPose(translation, rotationWxyz), realRes, totalCells, cellSize, dSdf,
                         static_cast<cudaStream_t>(stream), &l),
           "mesh sdf");
-    return NEBULA_MPM_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.code;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return NEBULA_MPM_ERR_INVALID;
-  }
+  });
 }
 
 }  // extern "C"
