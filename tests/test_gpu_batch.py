@@ -169,3 +169,28 @@ def test_batch_errors():
         b.add_scene(cfg, pos, vel)  # layout fixed after the first step
     b.sync()
     assert b.download(s, "P").shape == (10, 4)
+
+
+def test_batch_ragged_with_empty_and_single_particle_scenes():
+    """Scenes of 0, 1 and 2,000+ particles mixed (an empty scene first and
+    last): every non-empty scene equals its single-scene run, empty scenes stay
+    empty and the layout tables stay consistent."""
+    base = small_mix(3)
+
+    def cut(sc, k):
+        return dataclasses.replace(sc, state={f: a[:k].copy() for f, a in sc.state.items()}, name="%s_%d" % (sc.name, k))
+
+    scenes = [cut(base[0], 0), cut(base[1], 1), base[2], cut(base[0], 0), cut(base[1], 7)]
+    b, ids = batch_run(scenes, 20)
+    info = [b.scene_info(s) for s in ids]
+    assert [i["particles"] for i in info] == [sc.n for sc in scenes]
+    assert all(i["first_brick"] == sum(j["bricks"] for j in info[:k]) for k, i in enumerate(info))
+    for sc, s in zip(scenes, ids):
+        got = b.state(s)
+        if sc.n == 0:
+            assert got["P"].shape == (0, 4)
+            continue
+        want = plain_run(sc, 20)
+        assert rel_l2(got["P"][:, :3], want["P"][:, :3]) < 1e-5, sc.name
+    assert b.stats()["error_flags"] == 0
+    b.cleanup()
