@@ -158,6 +158,10 @@ int nebula_mpm_set_collider_mesh_pose(nebula_mpm* e, const float translation[3],
  * replaces the force table (n <= 16).  No shader is rebuilt: forces are a
  * kernel parameter table. */
 int nebula_mpm_set_forces(nebula_mpm* e, const nebula_mpm_force* f, uint32_t n);
+/* addForce(GravityForce) as one call (the reference removed its gravity member,
+ * MPMEngine.h:57-58): every GRAVITY entry of the table is replaced by one of
+ * vector (gx, gy, gz); other forces stay; (0, 0, 0) removes gravity. */
+int nebula_mpm_set_gravity(nebula_mpm* e, float gx, float gy, float gz);
 /* MPMEngine::appendParticles (MPMEngine.cpp:211-235): pos4=(x,Vp),
  * vel4=(v, id bits); F=I, B=0, stress=0; truncated at capacity.  *appended
  * (may be NULL) receives the count actually added. */
@@ -205,6 +209,13 @@ int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count);
 /* All 8 fields at once (P, v, F0, F1, F2, B0, B1, B2), original particle order,
  * count = 4 * live floats per field; one unpermute and one synchronisation. */
 int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t count);
+/* getPositionBuffer / getVelocityBuffer (MPMEngine.cpp:165-166) for any field:
+ * the device array of field `f` (4 * live floats) in the original particle
+ * order.  The engine reorders particles during a step, so the pointer is valid
+ * until the next call that steps or changes the particles; query it again
+ * after each step.  Writes through it (stream-ordered by the caller) are seen
+ * by the next step. */
+int nebula_mpm_device_ptr(nebula_mpm* e, int field, float** out);
 /* MPMEngine::step (MPMEngine.cpp:404-474): numSubsteps substeps of dt/numSubsteps,
  * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream). */
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream);

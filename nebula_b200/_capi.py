@@ -113,6 +113,8 @@ _SIGS = {
     "nebula_mpm_set_pipeline": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_download_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "nebula_mpm_set_gravity": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "nebula_mpm_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_launch_limits": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

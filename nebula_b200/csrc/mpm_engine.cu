@@ -386,7 +386,42 @@ void MPMEngine::setForces(const nebula_mpm_force* f, uint32_t n) {
       throw Error(NEBULA_MPM_ERR_UNSUPPORTED, "only GRAVITY and CONSTANT_WIND forces act on the MPM grid in this build");
   prepareHostAccess(false);
   forceCount_ = n;
+  hostForces_.assign(reinterpret_cast<const Force*>(f), reinterpret_cast<const Force*>(f) + n);
   if (n) check(cudaMemcpy(forces_.ptr, f, n * sizeof(Force), cudaMemcpyHostToDevice), "upload forces");
+}
+
+// The gravity entry of the force table: every GRAVITY force is replaced by one
+// of vector g (direction g/|g|, strength |g|, all engines), appended if there
+// was none; the other forces stay.  A zero vector removes gravity.
+void MPMEngine::setGravity(float gx, float gy, float gz) {
+  if (!std::isfinite(gx) || !std::isfinite(gy) || !std::isfinite(gz)) throw Error(NEBULA_MPM_ERR_INVALID, "gravity must be finite");
+  std::vector<Force> t;
+  for (const Force& f : hostForces_)
+    if (f.type != FORCE_GRAVITY) t.push_back(f);
+  const float s = std::sqrt(gx * gx + gy * gy + gz * gz);
+  if (s > 0.f) {
+    Force g{};
+    g.type = FORCE_GRAVITY;
+    g.affectMask = 0;
+    g.data[0] = gx / s;
+    g.data[1] = gy / s;
+    g.data[2] = gz / s;
+    g.data[3] = s;
+    t.push_back(g);
+  }
+  if (t.size() > size_t(kMaxForces)) throw Error(NEBULA_MPM_ERR_INVALID, "at most 16 forces");
+  setForces(reinterpret_cast<const nebula_mpm_force*>(t.data()), uint32_t(t.size()));
+}
+
+// A field's device array in the original particle order (getPositionBuffer /
+// getVelocityBuffer, MPMEngine.cpp:165-166): the particles are put back in
+// that order first (a step reorders them again, so query after each step).
+// Writes through the pointer are seen by the next step.
+float* MPMEngine::devicePointer(int field) {
+  if (field < 0 || field > 7) throw Error(NEBULA_MPM_ERR_INVALID, "field index out of range");
+  prepareHostAccess(true);
+  ++stateVersion_;  // the caller may write through the pointer
+  return reinterpret_cast<float*>(statePtrs(cur_).f[field]);
 }
 
 uint32_t MPMEngine::appendParticles(const float* pos4, const float* vel4, uint32_t n) {
@@ -988,6 +1023,15 @@ int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count) {
 }
 int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t count) {
   return guarded([&] { E(e).downloadState(host, count); });
+}
+int nebula_mpm_device_ptr(nebula_mpm* e, int field, float** out) {
+  return guarded([&] {
+    if (!out) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    *out = E(e).devicePointer(field);
+  });
+}
+int nebula_mpm_set_gravity(nebula_mpm* e, float gx, float gy, float gz) {
+  return guarded([&] { E(e).setGravity(gx, gy, gz); });
 }
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream) {
   return guarded([&] { E(e).step(dt, static_cast<cudaStream_t>(stream)); });

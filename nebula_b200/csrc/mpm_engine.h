@@ -115,6 +115,8 @@ class MPMEngine {
   void uploadState(const float* const f[8], uint32_t n);
   void download(int field, float* host, uint64_t count);
   void downloadState(float* const host[8], uint64_t count);
+  float* devicePointer(int field);
+  void setGravity(float gx, float gy, float gz);
   StatePtrs originalOrder();
   void step(float dt, cudaStream_t s);
   uint32_t liveCount() const { return live_; }
@@ -209,6 +211,7 @@ class MPMEngine {
   uint64_t emitEvents_ = 0;  // emissions since create / reset: the counter of the sampling hash
   static constexpr uint64_t kEmitSeed = 12345;
   uint32_t forceCount_ = 0;
+  std::vector<Force> hostForces_;  // the table last uploaded (setGravity edits it)
   bool hasSdf_ = false;
 
   uint64_t substeps_ = 0;

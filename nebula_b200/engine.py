@@ -224,6 +224,22 @@ class MPMEngine:
         call("nebula_mpm_download", self._h, FIELD_INDEX[field], _ptr(out), out.size)
         return out
 
+    def device_ptr(self, field: str) -> int:
+        """Device address of `field` (4 * live floats, original particle order);
+        valid until the next step or particle change."""
+        p = C.c_void_p()
+        call("nebula_mpm_device_ptr", self._h, FIELD_INDEX[field], C.byref(p))
+        return int(p.value or 0)
+
+    def setGravity(self, gx: float, gy: float, gz: float):
+        """nebula_mpm_set_gravity on the table this binding keeps: every gravity
+        entry replaced by one vector (none for (0, 0, 0)), other forces kept."""
+        from .scenes import FORCE_GRAVITY, gravity
+        fs = [f for f in self._forces if int(f["type"]) != FORCE_GRAVITY]
+        if gx or gy or gz:
+            fs.append(gravity((gx, gy, gz)))
+        self.setForces(fs)
+
     def state(self) -> dict:
         """All 8 fields (one unpermute, one synchronisation)."""
         n = self.liveParticleCount()
