@@ -54,12 +54,9 @@ def parse():
 
 
 def make_scene(name):
+    """The workload from nebula_b200/configs.json: slope = cfg3, elastic = cfg1, multimaterial = cfg2."""
     from nebula_b200 import scenes as S
-    if name == "slope":
-        return S.slope_flow()
-    if name == "elastic":
-        return S.elastic_block()
-    return S.multimaterial()
+    return S.load_config({"slope": "cfg3", "elastic": "cfg1", "multimaterial": "cfg2"}[name])
 
 
 def peaks():

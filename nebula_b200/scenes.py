@@ -522,3 +522,17 @@ def diff_block(seed=5, n=50000, res=64, substeps=200, dt=1e-4, side=37, y0_cells
     sc = Scene("diff_block_50k_64", params, make_state(pos, np.float32(sp) ** 3, vel=vel), substeps)
     sc.extra = {"E": E, "nu": 0.3, "rho0": 1000.0, "target": target, "checkpoint_every": 20}
     return sc
+
+# ----------------------------------------------------------------------------- named configurations
+CONFIGS_JSON = __import__("pathlib").Path(__file__).with_name("configs.json")
+
+
+def load_config(key: str):
+    """The scene (or, for the batched mix, the list of scenes) of configuration
+    `key` in configs.json, built with the seeds and sizes stored there."""
+    import json
+    cfg = json.loads(CONFIGS_JSON.read_text())["configs"][key]
+    args = dict(cfg["args"])
+    if "n_side" in args and isinstance(args["n_side"], list):
+        args["n_side"] = tuple(args["n_side"])
+    return globals()[cfg["generator"]](**args)
