@@ -13,6 +13,8 @@
 #include "mpm_scan.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 namespace nebula {
 namespace {
@@ -856,24 +858,30 @@ template <class K> int bigSmemCtasPerSm(K kernel, int threads, size_t smem) {
   return ctasPerSm(kernel, threads, smem);
 }
 
-// Most CTAs per SM of every kernel variant, resolved once (kernel attributes
-// and occupancy queries stay outside stream capture).
+// Most CTAs per SM of every kernel variant, resolved once per device (kernel
+// attributes are per device; the queries stay outside stream capture).
 struct LaunchShapes {
-  bool ready = false;
+  std::atomic<bool> ready{false};
   int p2g[2] = {0, 0};                          // [BATCH]
   int grid[2] = {0, 0};                         // [gridBatch == 4]
   int gridBatch = 0;                            // batched grid kernel
   int fused[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};  // [FLIP][BATCH][CHUNK == 256]
 };
-LaunchShapes g_shapes;
+constexpr int kShapeSlots = 64;  // device ordinals beyond this share slots modulo 64
+LaunchShapes g_shapes[kShapeSlots];
+std::mutex g_shapesMutex;
 
 template <bool FLIP, bool BATCH, int CHUNK> void setupFused(LaunchShapes& L) {
   L.fused[FLIP][BATCH][CHUNK == 256] = bigSmemCtasPerSm(k_g2p2g<FLIP, BATCH, CHUNK>, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>));
 }
 
 const LaunchShapes& shapes() {
-  if (g_shapes.ready) return g_shapes;
-  LaunchShapes& L = g_shapes;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  LaunchShapes& L = g_shapes[dev % kShapeSlots];
+  if (L.ready.load(std::memory_order_acquire)) return L;
+  std::lock_guard<std::mutex> lock(g_shapesMutex);
+  if (L.ready.load(std::memory_order_relaxed)) return L;
   L.p2g[0] = bigSmemCtasPerSm(k_p2g_bricks<false>, kThreads, sizeof(P2GSmem));
   L.p2g[1] = bigSmemCtasPerSm(k_p2g_bricks<true>, kThreads, sizeof(P2GSmem));
   L.grid[0] = ctasPerSm(k_grid_bricks<2>, kThreads);
@@ -887,7 +895,7 @@ const LaunchShapes& shapes() {
   setupFused<true, false, 256>(L);
   setupFused<true, true, 128>(L);
   setupFused<true, true, 256>(L);
-  L.ready = true;
+  L.ready.store(true, std::memory_order_release);
   return L;
 }
 
