@@ -217,7 +217,12 @@ int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t coun
  * by the next step. */
 int nebula_mpm_device_ptr(nebula_mpm* e, int field, float** out);
 /* MPMEngine::step (MPMEngine.cpp:404-474): numSubsteps substeps of dt/numSubsteps,
- * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * A step may be captured into a CUDA graph on a non-NULL stream and replayed
+ * when numSubsteps is even (the ping-pong state buffers then end each step in
+ * the parity the graph was captured with), after one uncaptured step, and
+ * with no emitter due and no setter called between replays (those act on the
+ * host side of a step, which a replay does not run). */
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream);
 /* MPMEngine::liveParticleCount (MPMEngine.h:67). */
 int nebula_mpm_live_count(const nebula_mpm* e, uint32_t* n);
