@@ -164,7 +164,11 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- algorithmic bytes
 def algorithmic_bytes(phase: str, n: int, active: int, nc: int, flip: bool, sdf: bool) -> float:
-    """Minimal DRAM bytes one launch of each phase must move (documented in DESIGN.md)."""
+    """Minimal DRAM bytes one launch of each phase must move: per particle its
+    state read and written once (x, v, F, B: 96 B written, those plus the
+    volume and material id: 104 B read) and 8 B of bin key and rank; per active
+    node 16 B accumulated by P2G, 16 B read and 16 B written by the grid update
+    and 16 B read by G2P; FLIP and the particle SDF check add their reads."""
     a = active
     if phase == "g2p":
         b = n * (80 + 128) + a * 20
