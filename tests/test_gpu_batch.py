@@ -194,3 +194,19 @@ def test_batch_ragged_with_empty_and_single_particle_scenes():
         assert rel_l2(got["P"][:, :3], want["P"][:, :3]) < 1e-5, sc.name
     assert b.stats()["error_flags"] == 0
     b.cleanup()
+
+
+def test_batch_with_flip_and_pic_scenes():
+    """FLIP (0.95), PIC (0) and APIC scenes in one batch (the batch then runs
+    the FLIP instantiation and keeps a pre-force velocity grid): each scene
+    equals its single-scene run."""
+    scenes = small_mix(3)
+    for sc, fr in zip(scenes, (0.95, 0.0, -1.0)):
+        sc.params.flip_ratio = fr
+    b, ids = batch_run(scenes, 30)
+    for sc, s in zip(scenes, ids):
+        got = b.state(s)
+        want = plain_run(sc, 30)
+        assert rel_l2(got["P"][:, :3], want["P"][:, :3]) < 1e-5, sc.params.flip_ratio
+        assert rel_l2(got["v"][:, :3], want["v"][:, :3]) < 1e-3, sc.params.flip_ratio
+    b.cleanup()
