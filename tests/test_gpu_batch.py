@@ -210,3 +210,26 @@ def test_batch_with_flip_and_pic_scenes():
         assert rel_l2(got["P"][:, :3], want["P"][:, :3]) < 1e-5, sc.params.flip_ratio
         assert rel_l2(got["v"][:, :3], want["v"][:, :3]) < 1e-3, sc.params.flip_ratio
     b.cleanup()
+
+
+def test_batch_plastic_models_and_sdf_colliders():
+    """Drucker-Prager, granular powder, viscoplastic mud and fluid scenes in one
+    batch (the float64 return maps inside the batched kernel), two of them with
+    a dense terrain SDF of their own grid: each equals its single-scene run."""
+    base = small_mix(4, nmax=8000)
+    mats = [S.material(S.MAT_DRUCKER_PRAGER, 3.5e5, 0.3, 1600.0, M_friction=0.6), S.preset_powder(), S.preset_mud(), S.preset_water()]
+    scenes = []
+    for k, (sc, m) in enumerate(zip(base, mats)):
+        sc.params.materials = [m]
+        sc.params.rho0 = float(m["rho0"])
+        if k % 2 == 0:
+            res = sc.params.grid_res[0]
+            sc.sdf, _ = S.terrain_sdf(k + 11, res, sc.params.cell_size)
+        scenes.append(sc)
+    b, ids = batch_run(scenes, 25)
+    for sc, s in zip(scenes, ids):
+        got = b.state(s)
+        want = plain_run(sc, 25)
+        assert rel_l2(got["P"][:, :3], want["P"][:, :3]) < 1e-5, sc.name
+        assert rel_l2(got["v"][:, :3], want["v"][:, :3]) < 1e-3, sc.name
+    b.cleanup()
