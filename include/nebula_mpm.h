@@ -279,6 +279,12 @@ int nebula_mpm_get_launch_config(nebula_mpm* e, nebula_mpm_launch_config* c);
  * fused_ctas_per_sm[fused_threads == 256], grid_ctas_per_sm[grid_batch == 4];
  * flip / batch select the fused kernel's FLIP and batched instantiations. */
 int nebula_mpm_launch_limits(int flip, int batch, uint32_t fused_ctas_per_sm[2], uint32_t grid_ctas_per_sm[2]);
+/* Self-test of the failure path of the kernels' waits: one warp of the brick
+ * scan's decoupled look-back waits on a predecessor tile that never publishes.
+ * The wait is bounded (about a second), so the kernel gives up, sets the
+ * scan-timeout bit (1) in *error_bits and returns; the CUDA context stays
+ * usable.  No counterpart in the reference. */
+int nebula_mpm_probe_wait_expiry(uint32_t* error_bits);
 /* The engine's own brick binning of the current positions (FUSED pipeline):
  * *numBricks listed bricks (brick id = cell Morton code >> 6) with the first
  * sorted slot of each (brickStarts has *numBricks + 1 entries, the last = live

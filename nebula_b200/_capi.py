@@ -117,6 +117,7 @@ _SIGS = {
     "nebula_mpm_set_gravity": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "nebula_mpm_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_launch_limits": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_probe_wait_expiry": (C.c_int, [C.c_void_p]),
     "nebula_mpm_export_brick_bins": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "nebula_mpm_export_grid": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]),

@@ -181,6 +181,11 @@ __device__ uint32_t lookBackWarp(unsigned long long* st, uint32_t tile, uint32_t
   return prefix;
 }
 
+// One warp waits as tile 1 on a tile 0 that never publishes: the bounded
+// look-back must give up after kBrickScanSpinLimit polls (a second or two),
+// set kErrScanTimeout and return.
+__global__ void k_wait_expiry_probe(unsigned long long* st, uint32_t* err) { (void)lookBackWarp(st, 1u, 0u, 0ull, err); }
+
 // Tickets from the monotone counter number every tile of every launch: tile =
 // ticket % tiles, launch = ticket / tiles.  Launches are stream-ordered, so one
 // launch's tickets are contiguous, and no host-side value changes between
@@ -915,6 +920,23 @@ LaunchLimits launchLimits(bool flip, bool batch) {
   out.gridCtasPerSm[0] = uint32_t(L.grid[0]);
   out.gridCtasPerSm[1] = uint32_t(L.grid[1]);
   return out;
+}
+
+cudaError_t probeWaitExpiry(uint32_t* errorBits) {
+  unsigned long long* st = nullptr;
+  uint32_t* err = nullptr;
+  cudaError_t e = cudaMalloc(&st, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&err, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(st, 0, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(err, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    k_wait_expiry_probe<<<1, 32>>>(st, err);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(errorBits, err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  cudaFree(st);
+  cudaFree(err);
+  return e;
 }
 
 void prepareBrickKernels(int numSMs) {

@@ -104,6 +104,10 @@ cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const B
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                              const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches);
+// Run the brick scan's bounded look-back against a predecessor that never
+// publishes; *errorBits receives the device error word (kErrScanTimeout set
+// when the wait gave up as designed).
+cudaError_t probeWaitExpiry(uint32_t* errorBits);
 // Resolve every launcher's one-time set-up (shared-memory limits, persistent
 // block counts) outside any stream capture.
 void prepareBrickKernels(int numSMs);

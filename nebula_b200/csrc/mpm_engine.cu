@@ -1030,6 +1030,12 @@ int nebula_mpm_device_ptr(nebula_mpm* e, int field, float** out) {
     *out = E(e).devicePointer(field);
   });
 }
+int nebula_mpm_probe_wait_expiry(uint32_t* error_bits) {
+  return guarded([&] {
+    if (!error_bits) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    nebula::check(nebula::probeWaitExpiry(error_bits), "wait-expiry probe");
+  });
+}
 int nebula_mpm_set_gravity(nebula_mpm* e, float gx, float gy, float gz) {
   return guarded([&] { E(e).setGravity(gx, gy, gz); });
 }
