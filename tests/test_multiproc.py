@@ -72,3 +72,37 @@ def test_two_ranks_gloo(tmp_path):
         assert r["n_sum"] == sum(sizes)
     cover = sorted(i for p in res[0]["everyone"] for i in p)
     assert cover == list(range(len(sizes)))
+
+
+def _rank_leaves(rank, world, port, out_dir):
+    """Rank 1 leaves between steps (after the first collective, none in
+    flight); rank 0's next collective must end with an error within the
+    process group's short timeout instead of hanging."""
+    import time
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    shard.max_over_ranks(1.0, dist)
+    if rank == 1:
+        os._exit(0)  # leaves without destroying the group
+    t0 = time.time()
+    failed = False
+    try:
+        shard.max_over_ranks(2.0, dist)
+    except Exception:
+        failed = True
+    torch.save({"failed": failed, "waited": time.time() - t0}, os.path.join(out_dir, "leave.pt"))
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_is_detected(tmp_path):
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_leaves, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        if p.is_alive():
+            p.kill()
+    r = torch.load(tmp_path / "leave.pt")
+    assert r["failed"] and r["waited"] < 60
