@@ -113,6 +113,7 @@ typedef struct nebula_mpm_stats {
   uint64_t kernel_launches;   /* kernels this engine has launched */
   uint32_t overflow_particles;/* particles whose P2G stencil left their block tile (slow path) */
   uint32_t error_flags;       /* device error bits seen at the last check */
+  uint64_t graph_launches;    /* steps replayed from a CUDA graph */
 } nebula_mpm_stats;
 
 typedef struct nebula_mpm nebula_mpm;
@@ -218,12 +219,22 @@ int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t coun
 int nebula_mpm_device_ptr(nebula_mpm* e, int field, float** out);
 /* MPMEngine::step (MPMEngine.cpp:404-474): numSubsteps substeps of dt/numSubsteps,
  * stream-ordered on `stream` (a cudaStream_t, NULL = legacy default stream).
- * A step may be captured into a CUDA graph on a non-NULL stream and replayed
- * when numSubsteps is even (the ping-pong state buffers then end each step in
- * the parity the graph was captured with), after one uncaptured step, and
- * with no emitter due and no setter called between replays (those act on the
- * host side of a step, which a replay does not run). */
+ * The engine replays the substep loop from CUDA graphs of its own: the second
+ * step in a row with the same kernel arguments (substep parameters, buffers,
+ * live count, substep count, launch shape) is captured, later ones replay it;
+ * a replay launches exactly what the uncaptured loop would.  Emitters and
+ * setters run on the host before the loop and change the key where they
+ * change an argument.  Off while phase profiling and while `stream` is being
+ * captured by the caller.
+ * A caller may also capture a step into a graph of its own on a non-NULL
+ * stream and replay it when numSubsteps is even (the ping-pong state buffers
+ * then end each step in the parity the graph was captured with), after one
+ * uncaptured step, and with no emitter due and no setter called between
+ * replays (those act on the host side of a step, which a replay does not run). */
 int nebula_mpm_step(nebula_mpm* e, float dt, void* stream);
+/* Engine-owned graph replays of nebula_mpm_step on (enable != 0, the default)
+ * or off (drops the captured graphs). */
+int nebula_mpm_set_graphs(nebula_mpm* e, int enable);
 /* MPMEngine::liveParticleCount (MPMEngine.h:67). */
 int nebula_mpm_live_count(const nebula_mpm* e, uint32_t* n);
 int nebula_mpm_get_stats(nebula_mpm* e, nebula_mpm_stats* s);

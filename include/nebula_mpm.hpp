@@ -89,6 +89,8 @@ class MPMEngine {
     ok(nebula_mpm_step(e_, dt, stream));
   }
   void sync() { ok(nebula_mpm_sync(e_)); }
+  // replays of the substep loop from the engine's own CUDA graphs (on by default)
+  void setGraphs(bool enable) { ok(nebula_mpm_set_graphs(e_, enable ? 1 : 0)); }
   uint32_t liveParticleCount() const {
     uint32_t n = 0;
     ok(nebula_mpm_live_count(e_, &n));

@@ -33,7 +33,7 @@ class Params(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("substeps", C.c_uint64), ("live_particles", C.c_uint32), ("active_bricks", C.c_uint32), ("particle_bricks", C.c_uint32),
                 ("grid_res", C.c_uint32 * 3), ("cube_res", C.c_uint32), ("hash_cells", C.c_uint32), ("kernel_launches", C.c_uint64),
-                ("overflow_particles", C.c_uint32), ("error_flags", C.c_uint32)]
+                ("overflow_particles", C.c_uint32), ("error_flags", C.c_uint32), ("graph_launches", C.c_uint64)]
 
 
 class Pass(C.Structure):
@@ -112,6 +112,7 @@ _SIGS = {
     "nebula_mpm_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_pipeline": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nebula_mpm_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_download_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nebula_mpm_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "nebula_mpm_set_gravity": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),

@@ -165,6 +165,8 @@ MPMEngine::~MPMEngine() {
   }
   for (auto ev : freeEvents_) cudaEventDestroy(ev);
   if (openEvent_) cudaEventDestroy(openEvent_);
+  clearGraphs();
+  if (captureStream_) cudaStreamDestroy(captureStream_);
 }
 
 // ------------------------------------------------------------------ phase timing
@@ -776,23 +778,146 @@ void MPMEngine::step(float dt, cudaStream_t s) {
   const float subDt = dt / float(n);  // MPMEngine.cpp:413
   const SubstepParams P = buildParams(subDt);
   if (params_.numSubsteps <= 0 || live_ == 0) return;
-  // substep k reads collider set min(k, trackLen - 1) of the track
-  auto atSubstep = [&](int k) {
-    SubstepParams Pk = P;
-    Pk.colliders += size_t(std::min(uint32_t(k), colliderTrackLen_ - 1)) * colliderCount_;
-    return Pk;
-  };
   if (pipeline_ == NEBULA_MPM_PIPELINE_DENSE) {
     normalizeOrder(s);
     discardPending(s);
-    for (int k = 0; k < params_.numSubsteps; ++k) substepDense(atSubstep(k), s);
+    for (int k = 0; k < params_.numSubsteps; ++k) substepDense(atSubstep(P, k), s);
     return;
   }
   if (!pendingMatches(subDt)) {
     discardPending(s);
     buildPending(P, s);
   }
-  for (int k = 0; k < params_.numSubsteps; ++k) substepFused(atSubstep(k), s);
+  runFused(P, s);
+}
+
+// substep k reads collider set min(k, trackLen - 1) of the track
+SubstepParams MPMEngine::atSubstep(const SubstepParams& P, int k) const {
+  SubstepParams Pk = P;
+  Pk.colliders += size_t(std::min(uint32_t(k), colliderTrackLen_ - 1)) * colliderCount_;
+  return Pk;
+}
+
+namespace {
+template <class T>
+void putKey(std::vector<unsigned char>& k, const T& v) {
+  const auto* p = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), p, p + sizeof(T));
+}
+}  // namespace
+// graph keys compare these records as bytes, so none of them may have padding
+static_assert(sizeof(SubstepParams) == 24 * 4 + 4 * sizeof(void*), "SubstepParams has padding");
+static_assert(sizeof(BrickBuffers) == 2 * 4 + 12 * sizeof(void*), "BrickBuffers has padding");
+static_assert(sizeof(StatePtrs) == 8 * sizeof(void*), "StatePtrs has padding");
+static_assert(sizeof(GridBuffers) == 3 * sizeof(void*), "GridBuffers has padding");
+static_assert(sizeof(LaunchConfig) == 4 * 4, "LaunchConfig has padding");
+
+std::vector<unsigned char> MPMEngine::graphKey(const SubstepParams& P) {
+  std::vector<unsigned char> k;
+  k.reserve(512);
+  putKey(k, P);
+  putKey(k, colliderTrackLen_);
+  putKey(k, params_.numSubsteps);
+  putKey(k, live_);
+  putKey(k, cur_);
+  putKey(k, statePtrs(0));
+  putKey(k, statePtrs(1));
+  putKey(k, pid_[0].ptr);
+  putKey(k, pid_[1].ptr);
+  putKey(k, brickBuffers());
+  putKey(k, gridBuffers());
+  putKey(k, err_.ptr);
+  putKey(k, launchCfg_);
+  putKey(k, numSMs_);
+  return k;
+}
+
+bool MPMEngine::graphsUsable(cudaStream_t s) const {
+  if (!useGraphs_ || profile_) return false;
+  // inside a capture of the caller's the launches go into the caller's graph
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return st == cudaStreamCaptureStatusNone;
+}
+
+void MPMEngine::clearGraphs() {
+  for (auto& g : graphs_) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);  // an in-flight replay completes first
+    g = StepGraph{};
+  }
+}
+
+void MPMEngine::setGraphs(bool on) {
+  bindDevice();
+  if (!on) clearGraphs();
+  useGraphs_ = on;
+}
+
+// The fused substep loop of one step, uncaptured or replayed from a graph.
+// Graphs are captured on an engine-owned stream (capture only records) and
+// launched on `s`, which may be the legacy default stream.
+void MPMEngine::runFused(const SubstepParams& P, cudaStream_t s) {
+  const int n = params_.numSubsteps;
+  auto loop = [&](cudaStream_t q) {
+    for (int k = 0; k < n; ++k) substepFused(atSubstep(P, k), q);
+  };
+  if (!graphsUsable(s)) {
+    loop(s);
+    return;
+  }
+  StepGraph& g = graphs_[cur_];
+  std::vector<unsigned char> key = graphKey(P);
+  if (g.key != key) {
+    // not what the last step of this parity ran: run it uncaptured, remember it
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = StepGraph{};
+    g.key = std::move(key);
+    loop(s);
+    return;
+  }
+  if (!g.exec) {
+    if (!captureStream_) check(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    // the host-side counters advance during the capture as for one run; they
+    // are put back and advanced below as for every replay
+    const int cur0 = cur_;
+    const bool perm0 = permuted_;
+    const uint64_t sub0 = substeps_, l0 = launches_;
+    auto restore = [&] {
+      cur_ = cur0;
+      permuted_ = perm0;
+      substeps_ = sub0;
+      launches_ = l0;
+    };
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(captureStream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+      loop(captureStream_);
+    } catch (...) {
+      cudaStreamEndCapture(captureStream_, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      restore();
+      throw;
+    }
+    const cudaError_t ec = cudaStreamEndCapture(captureStream_, &graph);
+    const uint64_t launched = launches_ - l0;
+    restore();
+    check(ec, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    check(ei, "cudaGraphInstantiate");
+    g.exec = exec;
+    g.launches = launched;
+  }
+  check(cudaGraphLaunch(g.exec, s), "cudaGraphLaunch");
+  ++graphLaunches_;
+  launches_ += g.launches;
+  substeps_ += uint64_t(n);
+  if (n & 1) cur_ ^= 1;
+  permuted_ = true;
 }
 
 void MPMEngine::exportBins(uint32_t* cnt, uint32_t* off, uint32_t* srt) {
@@ -888,6 +1013,7 @@ void MPMEngine::stats(nebula_mpm_stats* s) {
   s->kernel_launches = launches_;
   s->overflow_particles = overflow_;
   s->error_flags = errorFlags_;
+  s->graph_launches = graphLaunches_;
 }
 
 }  // namespace nebula
@@ -1081,6 +1207,9 @@ int nebula_mpm_set_launch_config(nebula_mpm* e, const nebula_mpm_launch_config* 
     if (!c) throw Error(NEBULA_MPM_ERR_INVALID, "null launch config");
     E(e).setLaunchConfig(nebula::fromAbi(*c));
   });
+}
+int nebula_mpm_set_graphs(nebula_mpm* e, int enable) {
+  return guarded([&] { E(e).setGraphs(enable != 0); });
 }
 int nebula_mpm_get_launch_config(nebula_mpm* e, nebula_mpm_launch_config* c) {
   return guarded([&] {

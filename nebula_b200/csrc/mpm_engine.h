@@ -130,6 +130,8 @@ class MPMEngine {
   int pipeline() const { return pipeline_; }
   void setLaunchConfig(const LaunchConfig& c);
   const LaunchConfig& launchConfig() const { return launchCfg_; }
+  // Replays of the fused substep loop from CUDA graphs (on by default).
+  void setGraphs(bool on);
   void exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_t* brickStarts, uint32_t* sortedPids);
 
  private:
@@ -164,6 +166,26 @@ class MPMEngine {
   void discardPending(cudaStream_t s);
   void buildPending(const SubstepParams& P, cudaStream_t s);
   void substepFused(const SubstepParams& P, cudaStream_t s);
+  void runFused(const SubstepParams& P, cudaStream_t s);
+  SubstepParams atSubstep(const SubstepParams& P, int k) const;
+  // Fused substep loops replayed from CUDA graphs.  A graph holds the kernels
+  // of one step with their arguments, so it is keyed by every argument the
+  // launches take (the substep parameters, buffer pointers, live count,
+  // substep count, buffer parity and launch shape): a replay under an equal
+  // key launches exactly what the uncaptured loop would.  One slot per buffer
+  // parity; a key is captured the second step in a row that its slot sees it.
+  struct StepGraph {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+  };
+  bool graphsUsable(cudaStream_t s) const;
+  std::vector<unsigned char> graphKey(const SubstepParams& P);
+  void clearGraphs();
+  bool useGraphs_ = true;
+  StepGraph graphs_[2];
+  cudaStream_t captureStream_ = nullptr;
+  uint64_t graphLaunches_ = 0;
   void prepareHostAccess(bool modifiesParticles);
   bool pendingMatches(float subDt) const;
   bool emitFromEmitters(float dt, cudaStream_t s);

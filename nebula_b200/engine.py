@@ -271,6 +271,11 @@ class MPMEngine:
         return {k: (list(getattr(s, k)) if k == "grid_res" else getattr(s, k)) for k, _ in s._fields_}
 
     # ------------------------------------------------------------ pipeline
+    def set_graphs(self, enable: bool):
+        """Replays of the substep loop from the engine's own CUDA graphs (on by
+        default); off drops the captured graphs."""
+        call("nebula_mpm_set_graphs", self._h, int(bool(enable)))
+
     def set_launch_config(self, cfg):
         """Launch shape of the fused and grid kernels (autotune.LaunchShape or a
         dict with its fields)."""
