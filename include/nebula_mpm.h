@@ -275,7 +275,10 @@ int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
  * fused G2P/P2G kernel = particles per P2G chunk (128 or 256);
  * fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the fused
  * and grid-update kernels (0 = as many as fit; larger values are capped at
- * that); grid_batch: grid nodes per thread per round (2 or 4).  Every shape
+ * that); grid_batch: grid nodes per thread per round (2 or 4); fused_split:
+ * work items per particle brick of the fused kernel (1-4, 0 = the default 4):
+ * 1 keeps a brick's chunks in one CTA, k > 1 deals them over k CTAs (more
+ * parallel items for scenes with few bricks, one tile flush per item).  Every shape
  * computes the same substep (float sums may associate differently).  No
  * counterpart in the reference (its dispatch sizes are fixed in the shaders). */
 typedef struct nebula_mpm_launch_config {
@@ -283,6 +286,7 @@ typedef struct nebula_mpm_launch_config {
   uint32_t fused_ctas_per_sm;
   uint32_t grid_ctas_per_sm;
   uint32_t grid_batch;
+  uint32_t fused_split;
 } nebula_mpm_launch_config;
 int nebula_mpm_set_launch_config(nebula_mpm* e, const nebula_mpm_launch_config* c);
 int nebula_mpm_get_launch_config(nebula_mpm* e, nebula_mpm_launch_config* c);

@@ -49,7 +49,8 @@ class Particles(C.Structure):
 
 
 class LaunchConfig(C.Structure):
-    _fields_ = [("fused_threads", C.c_uint32), ("fused_ctas_per_sm", C.c_uint32), ("grid_ctas_per_sm", C.c_uint32), ("grid_batch", C.c_uint32)]
+    _fields_ = [("fused_threads", C.c_uint32), ("fused_ctas_per_sm", C.c_uint32), ("grid_ctas_per_sm", C.c_uint32), ("grid_batch", C.c_uint32),
+                ("fused_split", C.c_uint32)]
 
 
 class BatchConfig(C.Structure):

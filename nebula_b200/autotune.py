@@ -3,12 +3,14 @@
 The fused G2P/P2G kernel and the grid update take their launch shape from a
 ``nebula_mpm_launch_config``: the fused kernel's CTA size (= particles per P2G
 chunk, 128 or 256), how many persistent CTAs each of the two kernels keeps per
-SM, and the grid kernel's nodes per thread per round (2 or 4).  Which shape is
+SM, the grid kernel's nodes per thread per round (2 or 4), and how many work
+items the fused kernel deals per particle brick (1-4).  Which shape is
 fastest depends on the GPU and on the workload (particles per brick, scene
 sizes, FLIP or APIC, the material mix), so ``tune`` times candidate shapes on
 the caller's own workload with CUDA events and keeps the fastest, by
-coordinate descent in two rounds (the fused kernel's shape, then the grid
-update's), and stores the result in a JSON cache keyed by the GPU and a
+coordinate descent in three rounds (the fused kernel's CTA shape, its items
+per brick, then the grid update's shape), and stores the result in a JSON
+cache keyed by the GPU and a
 workload key; a later run on the same GPU and workload reuses the entry
 without timing anything.  Every shape computes the same substep (float sums
 may associate differently), so tuning changes speed, not results.
@@ -33,7 +35,7 @@ from typing import Callable, Iterable
 from . import _capi
 
 CACHE_ENV = "NEBULA_B200_TUNE_CACHE"
-CACHE_VERSION = 1
+CACHE_VERSION = 2  # 2: shapes carry fused_split
 
 
 @dataclass(frozen=True)
@@ -42,13 +44,15 @@ class LaunchShape:
     fused_ctas_per_sm: int = 0  # 0 = as many as fit
     grid_ctas_per_sm: int = 0
     grid_batch: int = 4
+    fused_split: int = 4  # fused-kernel items per particle brick
 
     def to_c(self) -> _capi.LaunchConfig:
-        return _capi.LaunchConfig(int(self.fused_threads), int(self.fused_ctas_per_sm), int(self.grid_ctas_per_sm), int(self.grid_batch))
+        return _capi.LaunchConfig(int(self.fused_threads), int(self.fused_ctas_per_sm), int(self.grid_ctas_per_sm), int(self.grid_batch),
+                                  int(self.fused_split))
 
     @staticmethod
     def from_c(c) -> "LaunchShape":
-        return LaunchShape(c.fused_threads, c.fused_ctas_per_sm, c.grid_ctas_per_sm, c.grid_batch)
+        return LaunchShape(c.fused_threads, c.fused_ctas_per_sm, c.grid_ctas_per_sm, c.grid_batch, c.fused_split)
 
     @staticmethod
     def coerce(x) -> "LaunchShape":
@@ -94,6 +98,10 @@ def fused_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:
         for k in _ctas_options(most, (most - 1, most // 2)):
             c.append(replace(base, fused_threads=threads, fused_ctas_per_sm=k))
     return c
+
+
+def split_candidates(base: LaunchShape) -> list[LaunchShape]:
+    return [replace(base, fused_split=k) for k in (1, 2, 3, 4)]
 
 
 def grid_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:
@@ -167,6 +175,7 @@ def tune(measure: Callable[[LaunchShape], float], key: str, limits: Limits, path
 
     t_base = timed(base)
     best = min(fused_candidates(base, limits), key=timed)
+    best = min(split_candidates(best), key=timed)
     best = min(grid_candidates(best, limits), key=timed)
     entry = {"shape": asdict(best), "ms_per_substep": seen[best], "default_ms_per_substep": t_base,
              "tried": [[asdict(s), t] for s, t in tried], "when": time.strftime("%Y-%m-%dT%H:%M:%S")}

@@ -365,6 +365,7 @@ struct P2GSmemT {
   uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
   uint32_t markMask;           // grid-active marks of the item brick's 3^3 neighbour bricks
   uint32_t item;
+  uint32_t items[2];           // fused kernel: claimed items by iteration parity
 };
 using P2GSmem = P2GSmemT<kThreads>;
 
@@ -713,15 +714,16 @@ __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridB
 }
 
 // ------------------------------------------------------------------ fused G2P -> update -> P2G
-// One particle brick: G2P of the particles in sorted slots [start, end) of
-// brick `b` (the scene's own brick id) from the staged grid, particle update,
-// binning count under the global brick key brickBase + (Morton >> 6), and P2G
-// of the updated particles.
+// One item of a particle brick: G2P of the particles in the chunks of sorted
+// slots [start, end) of brick `b` (the scene's own brick id) that begin at
+// start, start + stride, ... (stride = CHUNK times the items per brick), from
+// the staged grid; particle update, binning count under the global brick key
+// brickBase + (Morton >> 6), and P2G of the updated particles.
 template <bool FLIP, int CHUNK>
 __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP, CHUNK>& S, uint32_t b, uint32_t start, uint32_t end,
-                                          uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
-                                          uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B, const GridBuffers& G,
-                                          float dtStress, uint32_t* err) {
+                                          uint32_t stride, uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur,
+                                          StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B,
+                                          const GridBuffers& G, float dtStress, uint32_t* err) {
   constexpr int kChunk = CHUNK;
   auto& sm = S.p2g;
   int bx, by, bz;
@@ -742,7 +744,7 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
   const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
   const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
   uint32_t par = 0;
-  for (uint32_t base = start; base < end; base += kChunk, par ^= 1u) {
+  for (uint32_t base = start; base < end; base += stride, par ^= 1u) {
     const uint32_t t = base + threadIdx.x;
     const bool act = t < end;
     const uint32_t mask = __ballot_sync(0xffffffffu, act);
@@ -797,21 +799,33 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
 // spills to L1-cached local memory beat 2 CTAs of 256 at 128 registers
 // (measured on the 1M-particle slope: Drucker-Prager -3%, Von Mises -6%,
 // ELASTIC -9% per launch); shared memory is 54 KB per 256-thread CTA.
+// The queue deals `split` items per particle brick: item i is part
+// i / numPB of brick i % numPB and takes the brick's chunks part, part +
+// split, ...; parts beyond a brick's last chunk are skipped.  split = 1 keeps
+// a brick in one CTA (one staging and one tile flush per brick); more items
+// per brick shorten the longest item, which bounds small scenes.
 template <bool FLIP, bool BATCH, int CHUNK>
 __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
                                                     StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G,
-                                                    float dtStress, uint32_t* err) {
+                                                    float dtStress, uint32_t* err, uint32_t split) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   G2P2GSmem<FLIP, CHUNK>& S = *reinterpret_cast<G2P2GSmem<FLIP, CHUNK>*>(smem_raw);
   auto& sm = S.p2g;
   const uint32_t numPB = B.counters[kCntNumPB];
-  for (;;) {
-    if (threadIdx.x == 0) sm.item = atomicAdd(B.counters + kCntQueueFused, 1u);
+  const uint32_t numItems = numPB * split;
+  // the claim alternates between two slots: a thread may claim the next item
+  // while others still read this one, never two ahead (one barrier per claim)
+  for (uint32_t it = 0;; it ^= 1u) {
+    if (threadIdx.x == 0) sm.items[it] = atomicAdd(B.counters + kCntQueueFused, 1u);
+    __syncthreads();
+    const uint32_t i = sm.items[it];
+    if (i >= numItems) break;
+    const uint32_t part = i / numPB, bi = i - part * numPB;
+    const uint32_t b = B.pbBrick[bi], end = min(B.pbStart[bi + 1], n), first = min(B.pbStart[bi], end) + part * uint32_t(CHUNK);
+    if (first >= end) continue;  // the brick has no chunk for this part
+    const uint32_t start = first, stride = split * uint32_t(CHUNK);
     p2gZeroTiles(sm);
     __syncthreads();
-    const uint32_t i = sm.item;
-    if (i >= numPB) break;
-    const uint32_t b = B.pbBrick[i], end = min(B.pbStart[i + 1], n), start = min(B.pbStart[i], end);
     if constexpr (BATCH) {
       __shared__ SubstepParams sP;
       __shared__ uint32_t sBase;
@@ -822,9 +836,9 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
       }
       __syncthreads();
       const uint32_t base = sBase;
-      g2p2gItem<FLIP, CHUNK>(sP, S, b - base, start, end, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
+      g2p2gItem<FLIP, CHUNK>(sP, S, b - base, start, end, stride, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
     } else {
-      g2p2gItem<FLIP, CHUNK>(P0, S, b, start, end, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
+      g2p2gItem<FLIP, CHUNK>(P0, S, b, start, end, stride, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
     }
     __syncthreads();
   }
@@ -1015,22 +1029,24 @@ namespace {
 
 template <bool FLIP, bool BATCH, int CHUNK>
 void launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                 const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, int numSMs, cudaStream_t s) {
+                 const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, uint32_t split, int numSMs,
+                 cudaStream_t s) {
   const int blocks = persistentGrid(ctasPerSm, shapes().fused[FLIP][BATCH][CHUNK == 256], numSMs);
-  k_g2p2g<FLIP, BATCH, CHUNK><<<blocks, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>), s>>>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err);
+  k_g2p2g<FLIP, BATCH, CHUNK><<<blocks, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>), s>>>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err,
+                                                                                   split);
 }
 
 template <bool BATCH>
 void launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur,
                     StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs,
                     cudaStream_t s) {
-  const uint32_t k = lc.fusedCtasPerSm;
+  const uint32_t k = lc.fusedCtasPerSm, sp = std::max(lc.fusedSplit, 1u);
   if (flip) {
-    if (lc.fusedThreads == 128) launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
-    else launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
+    if (lc.fusedThreads == 128) launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    else launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
   } else {
-    if (lc.fusedThreads == 128) launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
-    else launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, numSMs, s);
+    if (lc.fusedThreads == 128) launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    else launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
   }
 }
 

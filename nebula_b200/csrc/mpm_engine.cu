@@ -236,6 +236,7 @@ void validateLaunchConfig(const LaunchConfig& c) {
   if (c.fusedThreads != 128 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 128 or 256");
   if (c.gridBatch != 2 && c.gridBatch != 4) throw Error(NEBULA_MPM_ERR_INVALID, "grid_batch must be 2 or 4");
   if (c.fusedCtasPerSm > 64 || c.gridCtasPerSm > 64) throw Error(NEBULA_MPM_ERR_INVALID, "CTAs per SM must be <= 64 (0 = as many as fit)");
+  if (c.fusedSplit < 1 || c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 1-4 (0 = 4)");
 }
 
 LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
@@ -244,6 +245,7 @@ LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
   l.fusedCtasPerSm = c.fused_ctas_per_sm;
   l.gridCtasPerSm = c.grid_ctas_per_sm;
   l.gridBatch = c.grid_batch;
+  l.fusedSplit = c.fused_split == 0 ? 4u : c.fused_split;
   return l;
 }
 
@@ -253,6 +255,7 @@ nebula_mpm_launch_config toAbi(const LaunchConfig& l) {
   c.fused_ctas_per_sm = l.fusedCtasPerSm;
   c.grid_ctas_per_sm = l.gridCtasPerSm;
   c.grid_batch = l.gridBatch;
+  c.fused_split = l.fusedSplit;
   return c;
 }
 
@@ -810,7 +813,7 @@ static_assert(sizeof(SubstepParams) == 24 * 4 + 4 * sizeof(void*), "SubstepParam
 static_assert(sizeof(BrickBuffers) == 2 * 4 + 12 * sizeof(void*), "BrickBuffers has padding");
 static_assert(sizeof(StatePtrs) == 8 * sizeof(void*), "StatePtrs has padding");
 static_assert(sizeof(GridBuffers) == 3 * sizeof(void*), "GridBuffers has padding");
-static_assert(sizeof(LaunchConfig) == 4 * 4, "LaunchConfig has padding");
+static_assert(sizeof(LaunchConfig) == 5 * 4, "LaunchConfig has padding");
 
 std::vector<unsigned char> MPMEngine::graphKey(const SubstepParams& P) {
   std::vector<unsigned char> k;

@@ -18,17 +18,20 @@ def test_candidates_stay_within_occupancy():
     g = A.grid_candidates(A.LaunchShape(fused_threads=128), LIM)
     assert all(s.fused_threads == 128 for s in g)
     assert {(s.grid_batch, s.grid_ctas_per_sm) for s in g} == {(4, 0), (4, 4), (4, 2), (2, 0), (2, 4), (2, 2)}
+    sp = A.split_candidates(A.LaunchShape(fused_threads=128, fused_ctas_per_sm=5))
+    assert [s.fused_split for s in sp] == [1, 2, 3, 4] and all(s.fused_ctas_per_sm == 5 for s in sp)
     one = A.Limits(fused=(1, 1), grid=(1, 1))
     assert len(A.fused_candidates(A.LaunchShape(), one)) == 2 and len(A.grid_candidates(A.LaunchShape(), one)) == 2
 
 
 def cost(s):
-    """Fastest at 128 threads, 5 CTAs/SM, grid batch 2 with 4 CTAs/SM."""
+    """Fastest at 128 threads, 5 CTAs/SM, 3 items per brick, grid batch 2 with 4 CTAs/SM."""
     c = 10.0
     c += 0.0 if s.fused_threads == 128 else 1.0
     c += {0: 0.5, 5: 0.0, 3: 0.8, 2: 0.3, 1: 2.0}[s.fused_ctas_per_sm]
     c += 0.0 if s.grid_batch == 2 else 0.1
     c += {0: 0.2, 4: 0.0, 2: 0.05, 8: 0.3}[s.grid_ctas_per_sm]
+    c += {1: 0.4, 2: 0.1, 3: 0.0, 4: 0.05}[s.fused_split]
     return c
 
 
@@ -41,19 +44,21 @@ def test_descent_finds_the_cheapest_shape_and_caches_it(tmp_path):
 
     path = tmp_path / "shapes.json"
     best, rep = A.tune(measure, "gpu|k", LIM, path, repeats=2)
-    assert best == A.LaunchShape(128, 5, 4, 2)
+    assert best == A.LaunchShape(128, 5, 4, 2, 3)
     assert rep["source"] == "measured" and rep["ms_per_substep"] == cost(best)
     assert rep["default_ms_per_substep"] == cost(A.LaunchShape())
     assert len(calls) == 2 * len({s for s in calls})  # every distinct shape timed `repeats` times
     d = json.loads(path.read_text())
-    assert d["entries"]["gpu|k"]["shape"] == {"fused_threads": 128, "fused_ctas_per_sm": 5, "grid_ctas_per_sm": 4, "grid_batch": 2}
+    assert d["entries"]["gpu|k"]["shape"] == {"fused_threads": 128, "fused_ctas_per_sm": 5, "grid_ctas_per_sm": 4, "grid_batch": 2,
+                                              "fused_split": 3}
     calls.clear()
     best2, rep2 = A.tune(measure, "gpu|k", LIM, path)
     assert best2 == best and rep2["source"] == "cache" and not calls
     A.tune(lambda s: 1.0 if s == A.LaunchShape() else 2.0, "gpu|other", LIM, path)
     d = json.loads(path.read_text())
     assert set(d["entries"]) == {"gpu|k", "gpu|other"}
-    assert d["entries"]["gpu|other"]["shape"] == {"fused_threads": 256, "fused_ctas_per_sm": 0, "grid_ctas_per_sm": 0, "grid_batch": 4}
+    assert d["entries"]["gpu|other"]["shape"] == {"fused_threads": 256, "fused_ctas_per_sm": 0, "grid_ctas_per_sm": 0, "grid_batch": 4,
+                                                  "fused_split": 4}
     best3, rep3 = A.tune(lambda s: 1.0 if s == A.LaunchShape() else 2.0, "gpu|k", LIM, path, force=True)
     assert best3 == A.LaunchShape() and rep3["source"] == "measured"
 
@@ -69,8 +74,9 @@ def test_keys_and_shape_conversions(tmp_path, monkeypatch):
     k = A.workload_key("batch", 3_140_220, 128, False, [2, 0, 2], 64)
     assert k == "batch|n2^22|cube128|pic-apic|models0-2|scenes64"
     assert A.workload_key("engine", 1_000_000, 256, True, [2]) == "engine|n2^20|cube256|flip|models2|scenes1"
-    s = A.LaunchShape(128, 4, 2, 2)
+    s = A.LaunchShape(128, 4, 2, 2, 3)
     assert A.LaunchShape.from_c(s.to_c()) == s
-    assert A.LaunchShape.coerce({"fused_threads": 128, "fused_ctas_per_sm": 4, "grid_ctas_per_sm": 2, "grid_batch": 2}) == s
+    assert A.LaunchShape.coerce({"fused_threads": 128, "fused_ctas_per_sm": 4, "grid_ctas_per_sm": 2, "grid_batch": 2, "fused_split": 3}) == s
+    assert A.LaunchShape.coerce({"fused_threads": 128}).fused_split == 4
     monkeypatch.setenv(A.CACHE_ENV, str(tmp_path / "x.json"))
     assert A.cache_path() == tmp_path / "x.json"

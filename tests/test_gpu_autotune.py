@@ -12,7 +12,8 @@ from nebula_b200.engine import engine_for_scene
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [A.LaunchShape(), A.LaunchShape(128, 0, 0, 4), A.LaunchShape(256, 1, 2, 2), A.LaunchShape(128, 3, 4, 2), A.LaunchShape(256, 2, 8, 4)]
+SHAPES = [A.LaunchShape(), A.LaunchShape(128, 0, 0, 4), A.LaunchShape(256, 1, 2, 2), A.LaunchShape(128, 3, 4, 2), A.LaunchShape(256, 2, 8, 4),
+          A.LaunchShape(256, 0, 0, 4, 1), A.LaunchShape(256, 0, 0, 4, 2), A.LaunchShape(128, 0, 0, 4, 3)]
 
 
 def rel(a, b):
@@ -40,7 +41,7 @@ def test_every_shape_computes_the_same_substeps(flip):
 
 def test_bad_shapes_are_rejected():
     e = engine_for_scene(S.shear_block())
-    for bad in (A.LaunchShape(64, 0, 0, 4), A.LaunchShape(256, 0, 0, 3), A.LaunchShape(256, 65, 0, 4)):
+    for bad in (A.LaunchShape(64, 0, 0, 4), A.LaunchShape(256, 0, 0, 3), A.LaunchShape(256, 65, 0, 4), A.LaunchShape(256, 0, 0, 4, 5)):
         with pytest.raises(_capi.NebulaError):
             e.set_launch_config(bad)
     assert e.launch_config() == A.LaunchShape()
@@ -51,15 +52,16 @@ def test_bad_shapes_are_rejected():
 def test_batch_shapes_agree_and_tune_batch_caches(tmp_path):
     scenes = S.batch_mix(only={0, 1, 2, 3})
     out = []
-    for shape in (A.LaunchShape(), A.LaunchShape(128, 0, 4, 2)):
+    for shape in (A.LaunchShape(), A.LaunchShape(128, 0, 4, 2), A.LaunchShape(256, 0, 0, 4, 1)):
         b, ids = batch_for_scenes(scenes)
         b.set_launch_config(shape)
         assert b.launch_config() == shape
         b.step(scenes[0].params.dt * 20, 20)
         out.append([b.download(s, "P")[:, :3] for s in ids])
         b.cleanup()
-    for a, c in zip(*out):
-        assert rel(a, c) < 1e-6
+    for other in out[1:]:
+        for a, c in zip(other, out[0]):
+            assert rel(a, c) < 1e-6
     b, ids = batch_for_scenes(scenes)
     path = tmp_path / "shapes.json"
     shape, rep = A.tune_batch(b, scenes, ids, substeps=5, path=path, repeats=1)
