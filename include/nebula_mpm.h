@@ -49,7 +49,10 @@ typedef struct nebula_mpm_config {
 
 /* MaterialParams (src/core/MaterialParams.h:16-38), 64 bytes. model:
  * 0 ELASTIC (Hencky), 1 VON_MISES, 2 DRUCKER_PRAGER, 3 GRANULAR_POWDER,
- * 4 FLUID, 5 VISCOPLASTIC_MUD. */
+ * 4 FLUID, 5 VISCOPLASTIC_MUD; and 6 FIXED_COROTATED, which the reference
+ * names (README.md:78) but does not implement: Kirchhoff stress
+ * 2 mu (F - R) F^T + lambda (J - 1) J I, R the rotation of F's polar
+ * decomposition.  Other values act as ELASTIC. */
 typedef struct nebula_mpm_material {
   float mu, lambda, rho0;
   uint32_t model;
@@ -210,6 +213,25 @@ int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count);
 /* All 8 fields at once (P, v, F0, F1, F2, B0, B1, B2), original particle order,
  * count = 4 * live floats per field; one unpermute and one synchronisation. */
 int nebula_mpm_download_state(nebula_mpm* e, float* const host[8], uint64_t count);
+/* Streaming state exchange, stream-ordered on `stream` and overlapped with
+ * the steps queued before it: the copies run on two engine-owned copy
+ * streams through device staging buffers (2 x 128 B per particle of
+ * capacity, allocated on first use), one per direction, so a loop of
+ *   step(k); download_state_async(k); upload_state_async(k + 1)
+ * moves step k's result to the host and step k + 1's input to the device
+ * while step k computes.
+ * upload_state_async: replaces the state of particles [0, n) like
+ * nebula_mpm_upload_state (live count n, original particle order) at this
+ * point of `stream`; the host arrays (pinned for the copy to be
+ * asynchronous) must stay unchanged until the stream has passed it.
+ * download_state_async: copies the state as of this point of `stream` (all 8
+ * fields, original order, count = 4 * live floats per field) to the host
+ * arrays; they hold it after nebula_mpm_sync, or once `stream` has passed a
+ * later nebula_mpm_wait_downloads.
+ * wait_downloads: makes `stream` wait for every download queued so far. */
+int nebula_mpm_upload_state_async(nebula_mpm* e, const float* const fields[8], uint32_t n, void* stream);
+int nebula_mpm_download_state_async(nebula_mpm* e, float* const host[8], uint64_t count, void* stream);
+int nebula_mpm_wait_downloads(nebula_mpm* e, void* stream);
 /* getPositionBuffer / getVelocityBuffer (MPMEngine.cpp:165-166) for any field:
  * the device array of field `f` (4 * live floats) in the original particle
  * order.  The engine reorders particles during a step, so the pointer is valid

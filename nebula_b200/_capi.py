@@ -115,6 +115,9 @@ _SIGS = {
     "nebula_mpm_set_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_download_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_upload_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "nebula_mpm_download_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "nebula_mpm_wait_downloads": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "nebula_mpm_set_gravity": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "nebula_mpm_get_launch_config": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -38,7 +38,10 @@ static_assert(sizeof(Material) == 64, "Material");
 static_assert(sizeof(Collider) == 64, "Collider");
 static_assert(sizeof(Force) == 32, "Force");
 
-enum : uint32_t { MAT_ELASTIC = 0, MAT_VON_MISES = 1, MAT_DRUCKER_PRAGER = 2, MAT_GRANULAR_POWDER = 3, MAT_FLUID = 4, MAT_VISCOPLASTIC_MUD = 5 };
+enum : uint32_t {
+  MAT_ELASTIC = 0, MAT_VON_MISES = 1, MAT_DRUCKER_PRAGER = 2, MAT_GRANULAR_POWDER = 3, MAT_FLUID = 4, MAT_VISCOPLASTIC_MUD = 5,
+  MAT_FIXED_COROTATED = 6  // not in the reference's shaders: see fixedCorotatedStress
+};
 enum : uint32_t { COLL_PLANE = 0, COLL_SPHERE = 1, COLL_BOX = 2, COLL_CAPSULE = 3 };
 enum : uint32_t { FORCE_GRAVITY = 0, FORCE_CONSTANT_WIND = 1 };
 
@@ -427,6 +430,30 @@ template <class T> __device__ __forceinline__ m3<T> henckyStress(const m3<T>& F,
   svd3(F, U, s, V);
   henckyPrincipal(s, mu, lam, k);
   return stressUDUt(U, k);
+}
+
+// Fixed-corotated elasticity (Stomakhin et al. 2012), the model the
+// reference's README names beside Hencky for ELASTIC (README.md:78) without
+// implementing it; here model 6.  tau = 2 mu (F - R) F^T + lam (J - 1) J I
+// with R = U V^T a rotation; for F = U S V^T with det U = det V = +1 (S
+// signed) that is U diag(2 mu s_i (s_i - 1) + lam J (J - 1)) U^T, J = s0 s1 s2
+// = det F.  svd3's sign fix makes det U = +1 but its eigenvector sort can
+// leave det V = -1, with s2 of the wrong sign: flipping V's last column with
+// s2 leaves U S V^T and U unchanged.  Same float svd3 as ELASTIC.  svd3 keeps
+// the singular vectors in the rows of its matrices (the reference's layout,
+// which its own models multiply as columns); this model is not the
+// reference's, so its stress is the textbook sum of k_i u_i u_i^T:
+// tau[c][r] = sum_i k_i U[r][i] U[c][i], the index pattern of stressRebuilt.
+template <class T> __device__ __forceinline__ m3<T> fixedCorotatedStress(const m3<T>& F, T mu, T lam) {
+  m3<T> U, V;
+  T s[3], k[3];
+  svd3(F, U, s, V);
+  if (s[0] * s[1] * s[2] * m3det(F) < T(0)) s[2] = -s[2];
+  const T J = s[0] * s[1] * s[2];
+  const T c = lam * J * (J - T(1));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) k[i] = T(2) * mu * s[i] * (s[i] - T(1)) + c;
+  return stressRebuilt(U, k);
 }
 
 // Plastic return map + Kirchhoff stress with ONE decomposition (double).

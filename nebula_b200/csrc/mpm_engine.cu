@@ -167,6 +167,13 @@ MPMEngine::~MPMEngine() {
   if (openEvent_) cudaEventDestroy(openEvent_);
   clearGraphs();
   if (captureStream_) cudaStreamDestroy(captureStream_);
+  if (copyIn_) {
+    cudaStreamSynchronize(copyIn_);
+    cudaStreamSynchronize(copyOut_);
+    cudaStreamDestroy(copyIn_);
+    cudaStreamDestroy(copyOut_);
+    for (cudaEvent_t ev : {inReady_, inFree_, outReady_, outFree_}) cudaEventDestroy(ev);
+  }
 }
 
 // ------------------------------------------------------------------ phase timing
@@ -225,6 +232,94 @@ void MPMEngine::bindDevice() const { check(cudaSetDevice(device_), "cudaSetDevic
 void MPMEngine::quiesce() {
   bindDevice();
   check(lastStream_ ? cudaStreamSynchronize(lastStream_) : cudaDeviceSynchronize(), "synchronize");
+  if (copyIn_) check(cudaStreamSynchronize(copyIn_), "synchronize uploads");
+  if (copyOut_) check(cudaStreamSynchronize(copyOut_), "synchronize downloads");
+}
+
+void MPMEngine::switchStream(cudaStream_t s) {
+  if (s != lastStream_) {
+    quiesce();  // work queued on the previous stream must finish first
+    lastStream_ = s;
+  }
+}
+
+void MPMEngine::ensureStaging() {
+  const size_t bytes = size_t(8) * std::max<uint32_t>(capacity_, 1u) * sizeof(float4);
+  if (inStage_.bytes < bytes) {
+    inStage_.alloc(bytes);
+    outStage_.alloc(bytes);
+  }
+  if (!copyIn_) {
+    check(cudaStreamCreateWithFlags(&copyIn_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&copyOut_, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* ev : {&inReady_, &inFree_, &outReady_, &outFree_}) check(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "cudaEventCreate");
+  }
+}
+
+// H2D of the new state into the input staging buffer on the upload stream
+// (after the previous upload's staging copy was consumed); then, in `s`'s
+// order, the staged state becomes the current one (device copy, identity
+// particle order, no pending P2G).  The transfer runs while earlier work on
+// `s` (a step) still computes.
+void MPMEngine::uploadStateAsync(const float* const f[8], uint32_t n, cudaStream_t s) {
+  if (n > capacity_) throw Error(NEBULA_MPM_ERR_INVALID, "more particles than capacity");
+  for (int k = 0; k < 8; ++k)
+    if (n && !f[k]) throw Error(NEBULA_MPM_ERR_INVALID, "null field");
+  bindDevice();
+  switchStream(s);
+  ensureStaging();
+  float4* stage = static_cast<float4*>(inStage_.ptr);
+  const size_t cap = capacity_;
+  check(cudaStreamWaitEvent(copyIn_, inFree_, 0), "cudaStreamWaitEvent");
+  for (int k = 0; k < 8 && n; ++k)
+    check(cudaMemcpyAsync(stage + k * cap, f[k], size_t(n) * sizeof(float4), cudaMemcpyHostToDevice, copyIn_), "upload state");
+  check(cudaEventRecord(inReady_, copyIn_), "cudaEventRecord");
+  check(cudaStreamWaitEvent(s, inReady_, 0), "cudaStreamWaitEvent");
+  discardPending(s);
+  const StatePtrs st = statePtrs(cur_);
+  for (int k = 0; k < 8 && n; ++k)
+    check(cudaMemcpyAsync(st.f[k], stage + k * cap, size_t(n) * sizeof(float4), cudaMemcpyDeviceToDevice, s), "stage state");
+  check(cudaEventRecord(inFree_, s), "cudaEventRecord");
+  check(launchIota(static_cast<uint32_t*>(pid_[cur_].ptr), capacity_, s, &launches_), "iota");
+  permuted_ = false;
+  live_ = n;
+  ++stateVersion_;
+}
+
+// In `s`'s order the current state goes, in original particle order, to the
+// output staging buffer (after the previous download's transfer left it); the
+// D2H then runs on the download stream while later work on `s` computes.
+void MPMEngine::downloadStateAsync(float* const host[8], uint64_t count, cudaStream_t s) {
+  if (count != uint64_t(live_) * 4) throw Error(NEBULA_MPM_ERR_INVALID, "count must be 4 * live particles");
+  for (int k = 0; k < 8; ++k)
+    if (count && (!host || !host[k])) throw Error(NEBULA_MPM_ERR_INVALID, "null host buffer");
+  bindDevice();
+  switchStream(s);
+  ensureStaging();
+  float4* stage = static_cast<float4*>(outStage_.ptr);
+  const size_t cap = capacity_;
+  StatePtrs out;
+  for (int k = 0; k < 8; ++k) out.f[k] = stage + k * cap;
+  check(cudaStreamWaitEvent(s, outFree_, 0), "cudaStreamWaitEvent");
+  if (live_) {
+    if (permuted_) {
+      check(launchUnpermute(statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), out, live_, s, &launches_), "unpermute");
+    } else {
+      const StatePtrs st = statePtrs(cur_);
+      for (int k = 0; k < 8; ++k)
+        check(cudaMemcpyAsync(out.f[k], st.f[k], size_t(live_) * sizeof(float4), cudaMemcpyDeviceToDevice, s), "stage state");
+    }
+  }
+  check(cudaEventRecord(outReady_, s), "cudaEventRecord");
+  check(cudaStreamWaitEvent(copyOut_, outReady_, 0), "cudaStreamWaitEvent");
+  for (int k = 0; k < 8 && count; ++k)
+    check(cudaMemcpyAsync(host[k], out.f[k], count * sizeof(float), cudaMemcpyDeviceToHost, copyOut_), "download state");
+  check(cudaEventRecord(outFree_, copyOut_), "cudaEventRecord");
+}
+
+void MPMEngine::waitDownloads(cudaStream_t s) {
+  bindDevice();
+  if (outFree_) check(cudaStreamWaitEvent(s, outFree_, 0), "cudaStreamWaitEvent");
 }
 
 void MPMEngine::setParams(const nebula_mpm_params& p) {
@@ -1146,6 +1241,18 @@ int nebula_mpm_upload_state(nebula_mpm* e, const float* const fields[8], uint32_
     if (!fields) throw Error(NEBULA_MPM_ERR_INVALID, "null fields");
     E(e).uploadState(fields, n);
   });
+}
+int nebula_mpm_upload_state_async(nebula_mpm* e, const float* const fields[8], uint32_t n, void* stream) {
+  return guarded([&] {
+    if (!fields) throw Error(NEBULA_MPM_ERR_INVALID, "null fields");
+    E(e).uploadStateAsync(fields, n, static_cast<cudaStream_t>(stream));
+  });
+}
+int nebula_mpm_download_state_async(nebula_mpm* e, float* const host[8], uint64_t count, void* stream) {
+  return guarded([&] { E(e).downloadStateAsync(host, count, static_cast<cudaStream_t>(stream)); });
+}
+int nebula_mpm_wait_downloads(nebula_mpm* e, void* stream) {
+  return guarded([&] { E(e).waitDownloads(static_cast<cudaStream_t>(stream)); });
 }
 int nebula_mpm_download(nebula_mpm* e, int field, float* host, uint64_t count) {
   return guarded([&] { E(e).download(field, host, count); });

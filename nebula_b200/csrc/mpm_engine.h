@@ -115,6 +115,11 @@ class MPMEngine {
   void uploadState(const float* const f[8], uint32_t n);
   void download(int field, float* host, uint64_t count);
   void downloadState(float* const host[8], uint64_t count);
+  // Stream-ordered state exchange through device staging buffers and
+  // engine-owned copy streams (overlaps the transfers with the steps).
+  void uploadStateAsync(const float* const f[8], uint32_t n, cudaStream_t s);
+  void downloadStateAsync(float* const host[8], uint64_t count, cudaStream_t s);
+  void waitDownloads(cudaStream_t s);
   float* devicePointer(int field);
   void setGravity(float gx, float gy, float gz);
   StatePtrs originalOrder();
@@ -186,6 +191,13 @@ class MPMEngine {
   StepGraph graphs_[2];
   cudaStream_t captureStream_ = nullptr;
   uint64_t graphLaunches_ = 0;
+  // asynchronous state exchange: staging buffers (8 fields x capacity float4
+  // each), one copy stream per direction, and the events ordering their reuse
+  void ensureStaging();
+  void switchStream(cudaStream_t s);
+  DevBuf inStage_, outStage_;
+  cudaStream_t copyIn_ = nullptr, copyOut_ = nullptr;
+  cudaEvent_t inReady_ = nullptr, inFree_ = nullptr, outReady_ = nullptr, outFree_ = nullptr;
   void prepareHostAccess(bool modifiesParticles);
   bool pendingMatches(float subDt) const;
   bool emitFromEmitters(float dt, cudaStream_t s);

@@ -348,6 +348,8 @@ __device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s,
 #pragma unroll
         for (int b = 0; b < 3; ++b) tau.m[a][b] += (2.0f * mat.visc) * (D[a][b] - (a == b ? trD / 3.0f : 0.f));
     }
+  } else if (mat.model == MAT_FIXED_COROTATED) {
+    tau = fixedCorotatedStress<float>(Fn, mat.mu, mat.lam);
   } else {
     tau = henckyStress<float>(Fn, mat.mu, mat.lam);
   }

@@ -213,6 +213,31 @@ class MPMEngine:
         ptrs = (C.c_void_p * 8)(*[a.ctypes.data for a in arrs])
         call("nebula_mpm_upload_state", self._h, ptrs, n)
 
+    def upload_state_async(self, state: dict, stream=None):
+        """nebula_mpm_upload_state_async: `state` holds 8 C-contiguous (n, 4)
+        float32 arrays (pinned host memory for an asynchronous copy), which the
+        caller keeps unchanged until `stream` has passed this point."""
+        arrs = [state[f] for f in FIELDS]
+        for a in arrs:
+            if a.dtype != np.float32 or not a.flags.c_contiguous or a.ndim != 2 or a.shape[1] != 4:
+                raise ValueError("upload_state_async wants C-contiguous (n, 4) float32 arrays")
+        ptrs = (C.c_void_p * 8)(*[a.ctypes.data for a in arrs])
+        call("nebula_mpm_upload_state_async", self._h, ptrs, arrs[0].shape[0], _stream_handle(stream))
+
+    def download_state_async(self, out: dict, stream=None):
+        """nebula_mpm_download_state_async into 8 C-contiguous (live, 4) float32
+        arrays, valid after sync() or once `stream` passed wait_downloads()."""
+        arrs = [out[f] for f in FIELDS]
+        n = self.liveParticleCount()
+        for a in arrs:
+            if a.dtype != np.float32 or not a.flags.c_contiguous or a.shape != (n, 4):
+                raise ValueError("download_state_async wants C-contiguous (live, 4) float32 arrays")
+        ptrs = (C.c_void_p * 8)(*[a.ctypes.data for a in arrs])
+        call("nebula_mpm_download_state_async", self._h, ptrs, 4 * n, _stream_handle(stream))
+
+    def wait_downloads(self, stream=None):
+        call("nebula_mpm_wait_downloads", self._h, _stream_handle(stream))
+
     def liveParticleCount(self) -> int:
         n = C.c_uint32()
         call("nebula_mpm_live_count", self._h, C.byref(n))

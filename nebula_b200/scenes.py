@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-MAT_ELASTIC, MAT_VON_MISES, MAT_DRUCKER_PRAGER, MAT_GRANULAR_POWDER, MAT_FLUID, MAT_VISCOPLASTIC_MUD = range(6)
+MAT_ELASTIC, MAT_VON_MISES, MAT_DRUCKER_PRAGER, MAT_GRANULAR_POWDER, MAT_FLUID, MAT_VISCOPLASTIC_MUD, MAT_FIXED_COROTATED = range(7)
 COLL_PLANE, COLL_SPHERE, COLL_BOX, COLL_CAPSULE = range(4)
 FORCE_GRAVITY, FORCE_CONSTANT_WIND = 0, 1
 
@@ -337,7 +337,8 @@ def shear_block(model=MAT_ELASTIC, seed=1, gamma=20.0, substeps=100, dt=1e-4, fl
     float32 and float64 alike), and an initial shear velocity v_x = gamma (y - 0.7)
     so that F develops distinct singular values.  model: ELASTIC (E=1e4),
     VON_MISES (E=1e4, q_max=200), DRUCKER_PRAGER (E=3.5e5, rho 1600, 30 deg),
-    or the reference's presets for GRANULAR_POWDER, FLUID and VISCOPLASTIC_MUD."""
+    or the reference's presets for GRANULAR_POWDER, FLUID and VISCOPLASTIC_MUD,
+    or FIXED_COROTATED (E=1e4)."""
     sc = elastic_block(seed=seed, substeps=substeps, dt=dt, flip_ratio=flip_ratio)
     if model == MAT_DRUCKER_PRAGER:
         m = material(model, 3.5e5, 0.3, 1600.0, M_friction=math.tan(math.radians(30.0)))
@@ -349,13 +350,15 @@ def shear_block(model=MAT_ELASTIC, seed=1, gamma=20.0, substeps=100, dt=1e-4, fl
         m = preset_water()
     elif model == MAT_VISCOPLASTIC_MUD:
         m = preset_mud()
+    elif model == MAT_FIXED_COROTATED:
+        m = material(MAT_FIXED_COROTATED, 1e4, 0.3, 1000.0)
     else:
         m = material(MAT_ELASTIC, 1e4, 0.3, 1000.0)
     sc.params.materials = [m]
     sc.params.rho0 = float(m["rho0"])
     P = sc.state["P"]
     sc.state["v"][:, 0] = (gamma * (P[:, 1].astype(np.float64) - 0.7)).astype(np.float32)
-    sc.name = "shear_block_%s_8k_64" % ("elastic", "vonmises", "druckerprager", "powder", "fluid", "mud")[model]
+    sc.name = "shear_block_%s_8k_64" % ("elastic", "vonmises", "druckerprager", "powder", "fluid", "mud", "corotated")[model]
     return sc
 
 

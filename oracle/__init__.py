@@ -102,6 +102,7 @@ def lib():
             ("orc_set_num_threads", [C.c_int]),
             ("orc_morton_decode", [C.c_uint32, vp]),
             ("orc_hencky", [vp, C.c_float, C.c_float, vp, C.c_int]),
+            ("orc_fixed_corotated", [vp, C.c_float, C.c_float, vp, C.c_int]),
             ("orc_svd3", [vp, vp, vp, vp]),
             ("orc_project", [vp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, vp]),
         ]:
@@ -292,6 +293,14 @@ def hencky(F_glsl: np.ndarray, mu: float, lam: float, fp64: bool = False) -> np.
     f = np.ascontiguousarray(F_glsl, dtype=np.float32).reshape(9)
     t = np.empty(9, np.float32)
     lib().orc_hencky(_ptr(f), mu, lam, _ptr(t), int(fp64))
+    return t.reshape(3, 3)
+
+
+def fixed_corotated(F_glsl: np.ndarray, mu: float, lam: float, fp64: bool = False) -> np.ndarray:
+    """Fixed-corotated Kirchhoff stress (model 6) of a 3x3 F in GLSL layout (F[c][r])."""
+    f = np.ascontiguousarray(F_glsl, dtype=np.float32).reshape(9)
+    t = np.empty(9, np.float32)
+    lib().orc_fixed_corotated(_ptr(f), mu, lam, _ptr(t), int(fp64))
     return t.reshape(3, 3)
 
 

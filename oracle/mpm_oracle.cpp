@@ -151,7 +151,8 @@ struct Force {
 };
 static_assert(sizeof(Force) == 32, "force record");
 
-enum { MAT_ELASTIC = 0, MAT_VON_MISES = 1, MAT_DRUCKER_PRAGER = 2, MAT_GRANULAR_POWDER = 3, MAT_FLUID = 4, MAT_VISCOPLASTIC_MUD = 5 };
+enum { MAT_ELASTIC = 0, MAT_VON_MISES = 1, MAT_DRUCKER_PRAGER = 2, MAT_GRANULAR_POWDER = 3, MAT_FLUID = 4, MAT_VISCOPLASTIC_MUD = 5,
+       MAT_FIXED_COROTATED = 6 };
 enum { COLL_PLANE = 0, COLL_SPHERE = 1, COLL_BOX = 2, COLL_CAPSULE = 3 };
 
 }  // namespace
@@ -288,6 +289,32 @@ template <class T> M3<T> henckyStress(const M3<T>& F, T mu, T lam) {
   V3<T> kp = lam * trEps * mk(T(1), T(1), T(1)) + T(2) * mu * eps;
   M3<T> dg = mdiag(kp[0], kp[1], kp[2]);
   return mmul(mmul(U, dg), mtrans(U));
+}
+
+// Fixed-corotated elasticity (Stomakhin et al. 2012, "Energetically consistent
+// invertible elasticity"): the model the reference's README names beside
+// Hencky for ELASTIC (README.md:78; MaterialParams.h:6) but does not
+// implement, added as its own model number 6.  Kirchhoff stress
+//   tau = 2 mu (F - R) F^T + lam (J - 1) J I,  R = U V^T a rotation,
+// and with F = U S V^T, det U = det V = +1 (S signed):
+//   tau = U diag(2 mu s_i (s_i - 1) + lam J (J - 1)) U^T,  J = s0 s1 s2 = det F.
+// svd3's sign fix makes det U = +1, but its sort of the eigenvectors can
+// leave det V = -1; then s2 carries the wrong sign, and flipping V's last
+// column with s2 (which leaves U S V^T and U unchanged) restores det V = +1.
+// svd3 stores the singular vectors as the rows of its GLSL matrices (the
+// reference's layout, kept for its own models); this model is not the
+// reference's, so its stress is the textbook sum of k_i u_i u_i^T, which in
+// that storage is transpose(U) * diag(k) * U.
+template <class T> M3<T> fixedCorotatedStress(const M3<T>& F, T mu, T lam) {
+  M3<T> U, V;
+  V3<T> s;
+  svd3(F, U, s, V);
+  const T detF = mdet(F);
+  if (s[0] * s[1] * s[2] * detF < T(0)) s[2] = -s[2];
+  T J = s[0] * s[1] * s[2];
+  T c = lam * J * (J - T(1));
+  M3<T> dg = mdiag(T(2) * mu * s[0] * (s[0] - T(1)) + c, T(2) * mu * s[1] * (s[1] - T(1)) + c, T(2) * mu * s[2] * (s[2] - T(1)) + c);
+  return mmul(mmul(mtrans(U), dg), U);
 }
 
 template <class T> M3<T> fluidStressJ(T J, T bulkK) { return mscale(bulkK * (J - T(1)), mident<T>()); }
@@ -777,6 +804,8 @@ template <class R, class RP> struct Sim final : SimBase {
         R trD = D[0][0] + D[1][1] + D[2][2];
         M3<R> devD = madd(D, mscale(-(trD / R(3)), mident<R>()));
         tau_new = madd(tau_new, mscale(R(2) * visc, devD));
+      } else if (model == MAT_FIXED_COROTATED) {
+        tau_new = fixedCorotatedStress(F_new, mu, lam);
       } else {
         tau_new = henckyStress(F_new, mu, lam);
       }
@@ -939,6 +968,19 @@ void orc_hencky(const float* F, float mu, float lam, float* tau, int fp64) {
     M3<float> f;
     for (int i = 0; i < 9; ++i) f.m[i / 3][i % 3] = F[i];
     M3<float> t = henckyStress(f, mu, lam);
+    for (int i = 0; i < 9; ++i) tau[i] = t.m[i / 3][i % 3];
+  }
+}
+void orc_fixed_corotated(const float* F, float mu, float lam, float* tau, int fp64) {
+  if (fp64) {
+    M3<double> f;
+    for (int i = 0; i < 9; ++i) f.m[i / 3][i % 3] = F[i];
+    M3<double> t = fixedCorotatedStress(f, double(mu), double(lam));
+    for (int i = 0; i < 9; ++i) tau[i] = float(t.m[i / 3][i % 3]);
+  } else {
+    M3<float> f;
+    for (int i = 0; i < 9; ++i) f.m[i / 3][i % 3] = F[i];
+    M3<float> t = fixedCorotatedStress(f, mu, lam);
     for (int i = 0; i < 9; ++i) tau[i] = t.m[i / 3][i % 3];
   }
 }

@@ -302,6 +302,23 @@ def test_trajectory_fluid_100_substeps():
     assert ex <= 1e-4 and eF <= 1e-4
 
 
+def test_trajectory_fixed_corotated_100_substeps():
+    """FIXED_COROTATED (model 6, not in the reference's shaders): the same float
+    svd3 as ELASTIC with the corotated principal stresses; x and F carry the
+    1e-4 bar against the float32 oracle."""
+    sc = S.shear_block(S.MAT_FIXED_COROTATED)
+    gs, r = run_pair(sc, 100, ["ref32", "fp64"])
+    ex, eF = rel_l2(gs["P"][:, :3], r["ref32"]["P"][:, :3]), rel_l2(state_F(gs), state_F(r["ref32"]))
+    es = rel_l2(stress6(gs), stress6(r["ref32"]))
+    print("fixed-corotated shear 100 substeps: x %.3e F %.3e stress %.3e vs ref32; x %.3e F %.3e vs fp64" %
+          (ex, eF, es, rel_l2(gs["P"][:, :3], r["fp64"]["P"][:, :3]), rel_l2(state_F(gs), state_F(r["fp64"]))))
+    assert ex <= 1e-4 and eF <= 1e-4 and es <= 1e-3
+    # the model is not the Hencky one: the same scene as ELASTIC ends elsewhere
+    he = S.shear_block()
+    gh, _ = run_pair(he, 100, [])
+    assert rel_l2(stress6(gs), stress6(gh)) > 1e-3
+
+
 def test_trajectory_sdf_terrain_small():
     """Drucker-Prager slab on a terrain SDF (64^3 version of the slope scene)."""
     sc = S.slope_flow(res=64, n_side=(50, 6, 50), dt=1e-4)

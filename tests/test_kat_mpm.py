@@ -85,6 +85,49 @@ def test_hencky_uniform_compression(fp64):
     assert abs(t[0, 0] - exp) < abs(exp) * 0.01
 
 
+def _fixed_corotated_np(F, mu, lam):
+    """tau = 2 mu (F - R) F^T + lam (J - 1) J I in float64, R the rotation of
+    F's polar decomposition (det R = +1 also for an inverted F), written from
+    numpy's SVD independently of the oracle's Jacobi svd3."""
+    U, s, Vt = np.linalg.svd(F)
+    if np.linalg.det(U) < 0:
+        U[:, 2] *= -1
+        s[2] *= -1
+    if np.linalg.det(Vt) < 0:
+        Vt[2, :] *= -1
+        s[2] *= -1
+    R = U @ Vt
+    J = np.linalg.det(F)
+    return 2 * mu * (F - R) @ F.T + lam * (J - 1) * J * np.eye(3)
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_fixed_corotated_stress_matches_polar_formula(fp64):
+    """Model 6: the oracle's stress (svd3 + diagonal form) against the polar
+    formula, for random stretches, rotations and an inverted F; zero at F = I
+    and at any pure rotation."""
+    import oracle
+    mu, lam = 3846.15, 5769.23
+    rng = np.random.default_rng(11)
+    for k in range(40):
+        F = np.eye(3) + 0.3 * rng.standard_normal((3, 3))
+        if k == 39:
+            F = np.diag([1.05, 0.95, -0.9]) @ F  # inverted
+        if abs(np.linalg.det(F)) < 0.2:
+            continue
+        want = _fixed_corotated_np(F, mu, lam)
+        got = oracle.fixed_corotated(F.T, mu, lam, fp64=fp64).T  # GLSL layout is column-major
+        assert np.allclose(got, want, rtol=0, atol=(1e-6 if fp64 else 2e-2) * max(1.0, np.abs(want).max())), k
+    assert np.all(np.abs(oracle.fixed_corotated(np.eye(3), mu, lam)) < 1e-3)
+    c, s = np.cos(0.7), np.sin(0.7)
+    Rz = np.array([[c, -s, 0], [s, c, 0], [0, 0, 1]])
+    assert np.all(np.abs(oracle.fixed_corotated(Rz.T, mu, lam, fp64=True)) < 1e-3)
+    # small axis-aligned strains: both models linearise to lam tr(e) I + 2 mu e
+    F = np.diag([1.001, 0.999, 1.0005])
+    fc, he = oracle.fixed_corotated(F, mu, lam, fp64=True), oracle.hencky(F, mu, lam, fp64=True)
+    assert np.allclose(fc, he, rtol=3e-3, atol=1e-3)
+
+
 # ----------------------------------------------------------------------------- domain (test_domain.cpp:8-50)
 def test_domain_grid_res():
     assert S.grid_res((10.0, 10.0, 10.0), 10.0 / 64.0) == (64, 64, 64)
