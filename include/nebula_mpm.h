@@ -170,6 +170,30 @@ int nebula_mpm_set_gravity(nebula_mpm* e, float gx, float gy, float gz);
  * vel4=(v, id bits); F=I, B=0, stress=0; truncated at capacity.  *appended
  * (may be NULL) receives the count actually added. */
 int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* vel4, uint32_t n, uint32_t* appended);
+/* Seeded particle placement of the measurement configurations (no
+ * counterpart in the reference, whose init places an unjittered lattice,
+ * MPMEngine.cpp:86-137): counts[0] x counts[1] x counts[2] points, x fastest,
+ * then z, then y, at origin + index * spacing, each coordinate offset by
+ * U(-jitter, +jitter) drawn from the counter-based SplitMix64 stream
+ * (seed, stream) in that order (x, y, z of point 0, then of point 1, ...);
+ * computed in double, stored as float.  P.w = particleVolume, v = vel,
+ * v.w = materialId bits. */
+typedef struct nebula_mpm_lattice {
+  uint32_t counts[3];
+  uint32_t materialId;
+  double spacing;
+  double origin[3];
+  double jitter;
+  uint64_t seed;
+  uint64_t stream;
+  float particleVolume;
+  float vel[3];
+} nebula_mpm_lattice;
+/* The lattice's points on the host: pos4 and vel4 hold 4 * n floats,
+ * n = counts[0] * counts[1] * counts[2]. */
+int nebula_mpm_lattice_points(const nebula_mpm_lattice* L, float* pos4, float* vel4, uint64_t n);
+/* nebula_mpm_append_particles of the lattice's points (truncated at capacity). */
+int nebula_mpm_append_lattice(nebula_mpm* e, const nebula_mpm_lattice* L, uint32_t* appended);
 /* MPMEngine::resetParticles (MPMEngine.cpp:281-287); also rewinds the emitters. */
 int nebula_mpm_reset_particles(nebula_mpm* e);
 

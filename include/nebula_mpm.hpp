@@ -140,6 +140,12 @@ class MPMEngine {
     return appended;
   }
   void resetParticles() { ok(nebula_mpm_reset_particles(e_)); }
+  // the seeded jittered lattice of the measurement configurations
+  uint32_t appendLattice(const nebula_mpm_lattice& L) {
+    uint32_t appended = 0;
+    ok(nebula_mpm_append_lattice(e_, &L, &appended));
+    return appended;
+  }
   uint32_t addEmitter(const nebula_mpm_emitter& em) {
     uint32_t index = 0;
     ok(nebula_mpm_add_emitter(e_, &em, &index));

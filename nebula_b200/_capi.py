@@ -30,6 +30,12 @@ class Params(C.Structure):
                 ("q_max", C.c_float), ("M_friction", C.c_float), ("q_cohesion", C.c_float), ("flip_ratio", C.c_float)]
 
 
+class Lattice(C.Structure):
+    _fields_ = [("counts", C.c_uint32 * 3), ("materialId", C.c_uint32), ("spacing", C.c_double), ("origin", C.c_double * 3),
+                ("jitter", C.c_double), ("seed", C.c_uint64), ("stream", C.c_uint64), ("particleVolume", C.c_float),
+                ("vel", C.c_float * 3)]
+
+
 class Stats(C.Structure):
     _fields_ = [("substeps", C.c_uint64), ("live_particles", C.c_uint32), ("active_bricks", C.c_uint32), ("particle_bricks", C.c_uint32),
                 ("grid_res", C.c_uint32 * 3), ("cube_res", C.c_uint32), ("hash_cells", C.c_uint32), ("kernel_launches", C.c_uint64),
@@ -116,6 +122,8 @@ _SIGS = {
     "nebula_mpm_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "nebula_mpm_download_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nebula_mpm_upload_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "nebula_mpm_lattice_points": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nebula_mpm_append_lattice": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "nebula_mpm_download_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "nebula_mpm_wait_downloads": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nebula_mpm_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),

@@ -1217,6 +1217,64 @@ int nebula_mpm_append_particles(nebula_mpm* e, const float* pos4, const float* v
     if (appended) *appended = k;
   });
 }
+namespace {
+// SplitMix64 at counter i (1-based) of the stream (seed, stream): the base
+// seed * 0x100000001B3 + stream * 0xD1B54A32D192ED03 plus i golden-ratio
+// increments, then the SplitMix64 finaliser (Steele, Lea, Flood 2014).
+uint64_t splitmix64At(uint64_t base, uint64_t i) {
+  uint64_t z = base + i * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+uint64_t latticeCount(const nebula_mpm_lattice& L) { return uint64_t(L.counts[0]) * L.counts[1] * L.counts[2]; }
+
+void latticePoints(const nebula_mpm_lattice& L, float* pos4, float* vel4) {
+  const uint64_t base = L.seed * 0x100000001B3ull + L.stream * 0xD1B54A32D192ED03ull;
+  const uint32_t nx = L.counts[0], ny = L.counts[1], nz = L.counts[2];
+  float idBits;
+  std::memcpy(&idBits, &L.materialId, 4);
+  uint64_t p = 0;
+  for (uint32_t iy = 0; iy < ny; ++iy)
+    for (uint32_t iz = 0; iz < nz; ++iz)
+      for (uint32_t ix = 0; ix < nx; ++ix, ++p) {
+        const uint32_t idx[3] = {ix, iy, iz};
+        for (int a = 0; a < 3; ++a) {
+          // top 53 bits as a double in [0, 1), then lo + (hi - lo) * u; the
+          // products are kept apart from the sums (no fused multiply-add), so
+          // the points are the same on every host
+          const double u = double(splitmix64At(base, 3 * p + a + 1) >> 11) * (1.0 / 9007199254740992.0);
+          const volatile double ju = (2.0 * L.jitter) * u;
+          const volatile double at = double(idx[a]) * L.spacing;
+          pos4[4 * p + a] = float((at + L.origin[a]) + (-L.jitter + ju));
+          vel4[4 * p + a] = L.vel[a];
+        }
+        pos4[4 * p + 3] = L.particleVolume;
+        vel4[4 * p + 3] = idBits;
+      }
+}
+}  // namespace
+
+int nebula_mpm_lattice_points(const nebula_mpm_lattice* L, float* pos4, float* vel4, uint64_t n) {
+  return guarded([&] {
+    if (!L) throw Error(NEBULA_MPM_ERR_INVALID, "null lattice");
+    if (n != latticeCount(*L)) throw Error(NEBULA_MPM_ERR_INVALID, "n must be counts[0] * counts[1] * counts[2]");
+    if (n && (!pos4 || !vel4)) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    latticePoints(*L, pos4, vel4);
+  });
+}
+int nebula_mpm_append_lattice(nebula_mpm* e, const nebula_mpm_lattice* L, uint32_t* appended) {
+  return guarded([&] {
+    if (!L) throw Error(NEBULA_MPM_ERR_INVALID, "null lattice");
+    const uint64_t n = latticeCount(*L);
+    if (n > 0xFFFFFFFFull) throw Error(NEBULA_MPM_ERR_INVALID, "lattice larger than 2^32 points");
+    std::vector<float> pos(4 * n), vel(4 * n);
+    latticePoints(*L, pos.data(), vel.data());
+    const uint32_t k = E(e).appendParticles(pos.data(), vel.data(), uint32_t(n));
+    if (appended) *appended = k;
+  });
+}
 int nebula_mpm_add_emitter(nebula_mpm* e, const nebula_mpm_emitter* em, uint32_t* index) {
   return guarded([&] {
     if (!em) throw Error(NEBULA_MPM_ERR_INVALID, "null emitter");

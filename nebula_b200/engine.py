@@ -64,6 +64,30 @@ def _stream_handle(stream):
 _PARAM_NAMES = ("restitution", "wall_friction", "numSubsteps", "plasticModel", "q_max", "M_friction", "q_cohesion", "flip_ratio")
 
 
+
+def lattice_record(counts, spacing, origin, jitter, seed, stream=0, particle_volume=0.0, vel=(0.0, 0.0, 0.0), material_id=0):
+    """A nebula_mpm_lattice: the seeded jittered lattice of scenes.jittered_lattice."""
+    L = _capi.Lattice()
+    L.counts[:] = [int(c) for c in counts]
+    L.materialId = int(material_id)
+    L.spacing = float(spacing)
+    L.origin[:] = [float(o) for o in origin]
+    L.jitter = float(jitter)
+    L.seed = int(seed)
+    L.stream = int(stream)
+    L.particleVolume = float(particle_volume)
+    L.vel[:] = [float(v) for v in vel]
+    return L
+
+
+def lattice_points(L) -> tuple[np.ndarray, np.ndarray]:
+    """(pos4, vel4) of a lattice record, computed on the host by the library."""
+    n = int(L.counts[0]) * int(L.counts[1]) * int(L.counts[2])
+    pos = np.empty((n, 4), np.float32)
+    vel = np.empty((n, 4), np.float32)
+    call("nebula_mpm_lattice_points", C.byref(L), _ptr(pos), _ptr(vel), n)
+    return pos, vel
+
 class MPMEngine:
     """One MPM scene on the GPU."""
 
@@ -185,6 +209,12 @@ class MPMEngine:
             raise ValueError("pos and vel must have the same shape")
         k = C.c_uint32()
         call("nebula_mpm_append_particles", self._h, _ptr(p), _ptr(v), p.shape[0], C.byref(k))
+        return k.value
+
+    def append_lattice(self, L) -> int:
+        """nebula_mpm_append_lattice: the seeded lattice record `L` appended."""
+        k = C.c_uint32()
+        call("nebula_mpm_append_lattice", self._h, C.byref(L), C.byref(k))
         return k.value
 
     def resetParticles(self):

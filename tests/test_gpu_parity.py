@@ -331,6 +331,30 @@ def test_trajectory_sdf_terrain_small():
 
 
 # ----------------------------------------------------------------------------- engine surface
+def test_append_lattice_places_the_seeded_block():
+    """nebula_mpm_append_lattice into an empty engine gives the 8,000-particle
+    block of the Python scene generator exactly, and it then steps like it."""
+    from nebula_b200.engine import MPMConfig, MPMEngine, engine_for_scene, lattice_record
+    sc = S.elastic_block()
+    sp = sc.params
+    h = 1.0 / 64
+    half = 0.5 * h * 19 / 2.0
+    L = lattice_record((20, 20, 20), 0.5 * h, (0.5 - half, 0.7 - half, 0.5 - half), 0.25 * h, seed=1,
+                       particle_volume=float(np.float32(0.5 * h) ** 3))
+    eng = MPMEngine(MPMConfig(nx=0, ny=0, nz=0, domainSize=tuple(sp.domain_size), cellSize=sp.cell_size, maxParticles=sc.n,
+                              E=1e4, nu=0.3, rho0=sp.rho0))
+    assert eng.append_lattice(L) == sc.n
+    assert np.array_equal(eng.download("P"), sc.state["P"])
+    assert np.array_equal(eng.download("F1"), sc.state["F1"])
+    ref = engine_for_scene(sc)
+    for e in (eng, ref):
+        e.setMaterials(sp.materials_array()[: len(sp.materials)])
+        e.setForces(list(sp.forces))
+        e.flip_ratio = sp.flip_ratio
+        e.run_substeps(sp.dt, 10)
+    assert rel_l2(eng.download("P")[:, :3], ref.download("P")[:, :3]) < 1e-6
+
+
 def test_engine_default_lattice_and_append():
     from nebula_b200.engine import MPMConfig, MPMEngine
     eng = MPMEngine(MPMConfig(nx=4, ny=3, nz=2, domainSize=(10, 10, 10), cellSize=10 / 64, maxParticles=30))
