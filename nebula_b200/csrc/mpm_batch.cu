@@ -454,12 +454,14 @@ void BatchEngine::substep(uint32_t k, cudaStream_t st) {
   BrickBuffers B = brickBuffers();
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
-  check(launchGridBricksBatch(T, k, B, G, launchCfg_, numSMs_, st, &launches_), "grid bricks");
+  const bool fold = live_ < kFoldScatterMax;
+  check(launchGridBricksBatch(T, k, B, G, fold ? live_ : 0u, err, launchCfg_, numSMs_, st, &launches_), "grid bricks");
   check(launchG2P2GBatch(T, G.vold != nullptr, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
                          static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, err, launchCfg_, numSMs_, st, &launches_),
         "g2p2g");
   check(launchBrickScan(B, err, st, &launches_), "brick scan");
-  check(launchPermScatter(B, live_, err, st, &launches_), "perm scatter");
+  // the permutation of this binning: here, or by the next grid launch
+  if (!fold) check(launchPermScatter(B, live_, err, st, &launches_), "perm scatter");
   cur_ ^= 1;
   permuted_ = true;
 }

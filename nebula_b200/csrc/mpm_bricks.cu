@@ -323,12 +323,40 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint32_t n, uint32_t* err) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+// Sorted slot of buffer index t: the start of its brick plus its rank.
+__device__ __forceinline__ void permScatterOne(const BrickBuffers& B, uint32_t n, uint32_t* err, uint32_t t) {
   const uint32_t slot = B.brickStart[B.binKey[t]] + B.binRank[t];
   if (slot < n) B.perm[slot] = t;
   else atomicOr(err, kErrBinRange);
+}
+
+// Scatter of buffer indices t0, t0 + stride, ... < n, four per round with
+// the loads of a round issued before their dependent loads and stores.
+__device__ __forceinline__ void permScatterStrided(const BrickBuffers& B, uint32_t n, uint32_t* err, uint64_t t0, uint64_t stride) {
+  for (uint64_t base = t0; base < n; base += 4 * stride) {
+    uint32_t key[4], rank[4], start[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t t = base + uint64_t(k) * stride;
+      key[k] = t < n ? B.binKey[t] : 0u;
+      rank[k] = t < n ? B.binRank[t] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) start[k] = base + uint64_t(k) * stride < n ? B.brickStart[key[k]] : 0u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint64_t t = base + uint64_t(k) * stride;
+      if (t >= n) continue;
+      const uint32_t slot = start[k] + rank[k];
+      if (slot < n) B.perm[slot] = uint32_t(t);
+      else atomicOr(err, kErrBinRange);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint32_t n, uint32_t* err) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) permScatterOne(B, n, err, t);
 }
 
 // ------------------------------------------------------------------ shared-memory P2G
@@ -636,10 +664,16 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P0, Scene
 // configuration): their brick ids, then their accumulators (and an L1
 // prefetch of their SDF samples) are loaded before any node is updated, so
 // one round costs about the memory round trips of one node.
+// The kernel also scatters the permutation of the binning that precedes it
+// (the scan's brick starts, the fused kernel's keys and ranks) when n > 0:
+// the grid update does not read it and the next fused kernel does, so the
+// scatter needs no launch of its own.  Scattering the same binning twice
+// writes the same values.
 template <int kGridBatch>
-__global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, BrickBuffers B, GridBuffers G) {
+__global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, BrickBuffers B, GridBuffers G, uint32_t n, uint32_t* err) {
   const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  permScatterStrided(B, n, err, uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, stride);
   for (uint64_t g0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g0 < total; g0 += stride * kGridBatch) {
     uint32_t code[kGridBatch];
     bool live[kGridBatch];
@@ -673,8 +707,11 @@ __global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, Brick
 
 // Batched grid update: one warp per listed grid brick, two nodes per lane, the
 // brick's scene parameters in a warp-private shared copy.
-__global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, uint32_t substep, BrickBuffers B, GridBuffers G) {
+// Also scatters the permutation of the preceding binning (as k_grid_bricks).
+__global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, uint32_t substep, BrickBuffers B, GridBuffers G, uint32_t n,
+                                                                uint32_t* err) {
   __shared__ SubstepParams sP[kThreads / 32];
+  permScatterStrided(B, n, err, uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, uint64_t(gridDim.x) * blockDim.x);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t numGB = B.counters[kCntNumGB];
   for (uint32_t gb = blockIdx.x * (kThreads / 32) + warp; gb < numGB; gb += gridDim.x * (kThreads / 32)) {
@@ -1001,20 +1038,20 @@ cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n,
   return cudaGetLastError();
 }
 
-cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs, cudaStream_t s,
-                             uint64_t* launches) {
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err, const LaunchConfig& lc,
+                             int numSMs, cudaStream_t s, uint64_t* launches) {
   const LaunchShapes& L = shapes();
   if (lc.gridBatch == 2)
-    k_grid_bricks<2><<<persistentGrid(lc.gridCtasPerSm, L.grid[0], numSMs), kThreads, 0, s>>>(P, b, g);
+    k_grid_bricks<2><<<persistentGrid(lc.gridCtasPerSm, L.grid[0], numSMs), kThreads, 0, s>>>(P, b, g, n, err);
   else
-    k_grid_bricks<4><<<persistentGrid(lc.gridCtasPerSm, L.grid[1], numSMs), kThreads, 0, s>>>(P, b, g);
+    k_grid_bricks<4><<<persistentGrid(lc.gridCtasPerSm, L.grid[1], numSMs), kThreads, 0, s>>>(P, b, g, n, err);
   ++*launches;
   return cudaGetLastError();
 }
 
-cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs,
-                                  cudaStream_t s, uint64_t* launches) {
-  k_grid_bricks_batch<<<persistentGrid(lc.gridCtasPerSm, shapes().gridBatch, numSMs), kThreads, 0, s>>>(T, substep, b, g);
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err,
+                                  const LaunchConfig& lc, int numSMs, cudaStream_t s, uint64_t* launches) {
+  k_grid_bricks_batch<<<persistentGrid(lc.gridCtasPerSm, shapes().gridBatch, numSMs), kThreads, 0, s>>>(T, substep, b, g, n, err);
   ++*launches;
   return cudaGetLastError();
 }

@@ -86,8 +86,16 @@ cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, 
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
                             int numSMs, cudaStream_t s, uint64_t* launches);
 // Sparse grid update over the listed grid bricks; clears acc as it reads.
-cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs, cudaStream_t s,
-                             uint64_t* launches);
+// Also scatters the permutation (sorted slot -> buffer index of the n
+// particles) of the binning before it, which the next fused kernel reads
+// (n = 0: none).  Below kFoldScatterMax particles the scatter rides on the
+// grid launch (one launch fewer per substep: -3.4% per substep at 8,000
+// particles, -1.4% at 80,000); above it the separate k_perm_scatter launch,
+// all of whose threads issue their loads at once, is faster (+0.3% folded
+// at 1M).
+constexpr uint32_t kFoldScatterMax = 1u << 19;
+cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err, const LaunchConfig& lc,
+                             int numSMs, cudaStream_t s, uint64_t* launches);
 // Zero acc over the listed grid bricks (discarding a pending P2G).
 cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
 // The fused G2P -> particle update -> P2G + binning count.
@@ -100,8 +108,8 @@ cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* p
 cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32_t n, const BrickBuffers& b, cudaStream_t s, uint64_t* launches);
 cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, int numSMs,
                                  cudaStream_t s, uint64_t* launches);
-cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, const LaunchConfig& lc, int numSMs,
-                                  cudaStream_t s, uint64_t* launches);
+cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err,
+                                  const LaunchConfig& lc, int numSMs, cudaStream_t s, uint64_t* launches);
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                              const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches);

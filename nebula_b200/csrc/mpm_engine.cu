@@ -816,7 +816,8 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   uint64_t l0 = launches_;
   phaseBegin(kPhaseGrid, s);
-  check(launchGridBricks(P, B, G, launchCfg_, numSMs_, s, &launches_), "grid bricks");
+  const bool fold = live_ < kFoldScatterMax;
+  check(launchGridBricks(P, B, G, fold ? live_ : 0u, err, launchCfg_, numSMs_, s, &launches_), "grid bricks");
   phaseEnd(kPhaseGrid, s, l0);
   l0 = launches_;
   phaseBegin(kPhaseFused, s);
@@ -827,7 +828,8 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   l0 = launches_;
   phaseBegin(kPhaseBin, s);
   check(launchBrickScan(B, err, s, &launches_), "brick scan");
-  check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
+  // the permutation of this binning: here, or by the next grid launch
+  if (!fold) check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
   phaseEnd(kPhaseBin, s, l0);
   cur_ ^= 1;
   permuted_ = true;
@@ -1036,7 +1038,13 @@ void MPMEngine::exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_
   cudaStream_t s = lastStream_;
   // binning does not depend on dt; a grid built here is rebuilt by a step with dt != 0
   if (!pending_) buildPending(buildParams(0.f), s);
-  uint32_t* tmp = static_cast<uint32_t*>(binKey_.ptr);  // free between substeps
+  // after a step the last binning's permutation waits for the next grid
+  // launch, which reads the bin keys again: scatter it here (the same
+  // values) and keep the keys intact
+  check(launchPermScatter(brickBuffers(), live_, static_cast<uint32_t*>(err_.ptr), s, &launches_), "perm scatter");
+  DevBuf sortedTmp;
+  sortedTmp.alloc(size_t(std::max<uint32_t>(live_, 1u)) * sizeof(uint32_t));
+  uint32_t* tmp = static_cast<uint32_t*>(sortedTmp.ptr);
   check(launchSortedPid(static_cast<const uint32_t*>(perm_.ptr), static_cast<const uint32_t*>(pid_[cur_].ptr), tmp, live_, s, &launches_),
         "sorted pid");
   quiesce();
@@ -1047,7 +1055,7 @@ void MPMEngine::exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_
   check(cudaMemcpy(brickIds, pbBrick_.ptr, size_t(cnt[kCntNumPB]) * 4, cudaMemcpyDeviceToHost), "download bricks");
   check(cudaMemcpy(brickStarts, pbStart_.ptr, size_t(cnt[kCntNumPB] + 1) * 4, cudaMemcpyDeviceToHost), "download bricks");
   if (live_) check(cudaMemcpy(sortedPids, tmp, size_t(live_) * 4, cudaMemcpyDeviceToHost), "download bricks");
-  // binKey is rebuilt by the next binning; the pending grid stays valid
+  // the bin keys and the pending grid stay valid for the next step
 }
 
 void MPMEngine::exportGrid(float dt, float* mom, float* mass) {
