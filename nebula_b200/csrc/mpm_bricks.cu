@@ -29,6 +29,30 @@ inline uint32_t blocksFor(uint64_t n, int t = kThreads) { return uint32_t((n + t
 
 __device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
 
+// Programmatic dependent launch: the per-substep kernels are launched with
+// programmatic stream serialization, so a kernel's CTAs may be scheduled as
+// soon as the previous kernel's CTAs have all exited (no kernel triggers
+// earlier), hiding the launch latency between them.  Every such kernel waits
+// here, before its first memory access, until the previous grid has
+// completed and its writes are visible; without the launch attribute the
+// wait returns at once.
+__device__ __forceinline__ void waitForPredecessorGrid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+cudaError_t launchSerialized(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Lanes in `mask` holding the same key take consecutive slots of counter[key].
 __device__ __forceinline__ uint32_t warpAggInc(uint32_t mask, uint32_t* counter, uint32_t key) {
   const uint32_t peers = __match_any_sync(mask, key);
@@ -194,6 +218,7 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   __shared__ unsigned long long s_ticket;
   __shared__ uint32_t s_warp[3][kBrickScanThreads / 32];
   __shared__ uint32_t s_prefix[3];
+  waitForPredecessorGrid();
   if (threadIdx.x == 0) s_ticket = atomicAdd(B.scanTile, 1ull);
   __syncthreads();
   const uint32_t tile = uint32_t(s_ticket % B.tiles);
@@ -355,6 +380,7 @@ __device__ __forceinline__ void permScatterStrided(const BrickBuffers& B, uint32
 }
 
 __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint32_t n, uint32_t* err) {
+  waitForPredecessorGrid();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) permScatterOne(B, n, err, t);
 }
@@ -671,6 +697,7 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P0, Scene
 // writes the same values.
 template <int kGridBatch>
 __global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, BrickBuffers B, GridBuffers G, uint32_t n, uint32_t* err) {
+  waitForPredecessorGrid();
   const uint64_t total = uint64_t(B.counters[kCntNumGB]) * 64u;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   permScatterStrided(B, n, err, uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, stride);
@@ -711,6 +738,7 @@ __global__ void __launch_bounds__(kThreads) k_grid_bricks(SubstepParams P, Brick
 __global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, uint32_t substep, BrickBuffers B, GridBuffers G, uint32_t n,
                                                                 uint32_t* err) {
   __shared__ SubstepParams sP[kThreads / 32];
+  waitForPredecessorGrid();
   permScatterStrided(B, n, err, uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, uint64_t(gridDim.x) * blockDim.x);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t numGB = B.counters[kCntNumGB];
@@ -848,6 +876,7 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   G2P2GSmem<FLIP, CHUNK>& S = *reinterpret_cast<G2P2GSmem<FLIP, CHUNK>*>(smem_raw);
   auto& sm = S.p2g;
+  waitForPredecessorGrid();
   const uint32_t numPB = B.counters[kCntNumPB];
   const uint32_t numItems = numPB * split;
   // the claim alternates between two slots: a thread may claim the next item
@@ -1012,16 +1041,16 @@ cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32
 }
 
 cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches) {
-  k_brick_scan<<<b.tiles, kBrickScanThreads, 0, s>>>(b, err);
+  const cudaError_t e = launchSerialized(k_brick_scan, dim3(b.tiles), dim3(kBrickScanThreads), 0, s, b, err);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches) {
   if (n == 0) return cudaSuccess;
-  k_perm_scatter<<<blocksFor(n), kThreads, 0, s>>>(b, n, err);
+  const cudaError_t e = launchSerialized(k_perm_scatter, dim3(blocksFor(n)), dim3(kThreads), 0, s, b, n, err);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchP2GBricks(const SubstepParams& P, StatePtrs cur, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
@@ -1041,19 +1070,21 @@ cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n,
 cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err, const LaunchConfig& lc,
                              int numSMs, cudaStream_t s, uint64_t* launches) {
   const LaunchShapes& L = shapes();
-  if (lc.gridBatch == 2)
-    k_grid_bricks<2><<<persistentGrid(lc.gridCtasPerSm, L.grid[0], numSMs), kThreads, 0, s>>>(P, b, g, n, err);
-  else
-    k_grid_bricks<4><<<persistentGrid(lc.gridCtasPerSm, L.grid[1], numSMs), kThreads, 0, s>>>(P, b, g, n, err);
+  const cudaError_t e = lc.gridBatch == 2
+                            ? launchSerialized(k_grid_bricks<2>, dim3(persistentGrid(lc.gridCtasPerSm, L.grid[0], numSMs)), dim3(kThreads), 0, s,
+                                               P, b, g, n, err)
+                            : launchSerialized(k_grid_bricks<4>, dim3(persistentGrid(lc.gridCtasPerSm, L.grid[1], numSMs)), dim3(kThreads), 0, s,
+                                               P, b, g, n, err);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err,
                                   const LaunchConfig& lc, int numSMs, cudaStream_t s, uint64_t* launches) {
-  k_grid_bricks_batch<<<persistentGrid(lc.gridCtasPerSm, shapes().gridBatch, numSMs), kThreads, 0, s>>>(T, substep, b, g, n, err);
+  const cudaError_t e = launchSerialized(k_grid_bricks_batch, dim3(persistentGrid(lc.gridCtasPerSm, shapes().gridBatch, numSMs)), dim3(kThreads), 0,
+                                         s, T, substep, b, g, n, err);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches) {
@@ -1065,26 +1096,25 @@ cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, 
 namespace {
 
 template <bool FLIP, bool BATCH, int CHUNK>
-void launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                 const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, uint32_t split, int numSMs,
-                 cudaStream_t s) {
+cudaError_t launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt,
+                        uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, uint32_t split,
+                        int numSMs, cudaStream_t s) {
   const int blocks = persistentGrid(ctasPerSm, shapes().fused[FLIP][BATCH][CHUNK == 256], numSMs);
-  k_g2p2g<FLIP, BATCH, CHUNK><<<blocks, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>), s>>>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err,
-                                                                                   split);
+  return launchSerialized(k_g2p2g<FLIP, BATCH, CHUNK>, dim3(blocks), dim3(CHUNK), sizeof(G2P2GSmem<FLIP, CHUNK>), s, P, T, cur, pidCur, nxt,
+                          pidNxt, n, b, g, dtStress, err, split);
 }
 
 template <bool BATCH>
-void launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur,
-                    StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, int numSMs,
-                    cudaStream_t s) {
+cudaError_t launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur,
+                           StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err,
+                           int numSMs, cudaStream_t s) {
   const uint32_t k = lc.fusedCtasPerSm, sp = std::max(lc.fusedSplit, 1u);
   if (flip) {
-    if (lc.fusedThreads == 128) launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-    else launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-  } else {
-    if (lc.fusedThreads == 128) launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-    else launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    if (lc.fusedThreads == 128) return launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    return launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
   }
+  if (lc.fusedThreads == 128) return launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+  return launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
 }
 
 }  // namespace
@@ -1092,17 +1122,17 @@ void launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, c
 cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                         const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                         uint64_t* launches) {
-  launchFusedFor<false>(P.flip_ratio > 0.01f, lc, P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
+  const cudaError_t e = launchFusedFor<false>(P.flip_ratio > 0.01f, lc, P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                              const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches) {
-  launchFusedFor<true>(flip, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
+  const cudaError_t e = launchFusedFor<true>(flip, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
   ++*launches;
-  return cudaGetLastError();
+  return e;
 }
 
 cudaError_t launchUnpermute(StatePtrs in, const uint32_t* pid, StatePtrs out, uint32_t n, cudaStream_t s, uint64_t* launches) {
