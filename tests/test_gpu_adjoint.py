@@ -172,8 +172,9 @@ def test_full_rollout_against_float64_fixture():
     The rollout's grid sums are float atomics whose order changes from run to
     run, and on this floor-contact scene that moves the projections by 1-2%
     between GPU runs (measured over five runs: 1.0e-2 to 1.8e-2 apart; each
-    run 1.3e-2 to 2.8e-2 from the oracle, once 5.4e-2).  The bars therefore
-    hold the mean of three runs, and each run more loosely."""
+    run 1.3e-2 to 2.8e-2 from the oracle, once 5.4e-2; the mean of five runs
+    1.4e-2).  The bars therefore hold the mean of three runs at 4e-2, room for
+    one outlying run, and each run at 8e-2."""
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_adjoint_golden", GOLDEN.parent / "make_adjoint_golden.py")
     gen = importlib.util.module_from_spec(spec)
@@ -191,7 +192,7 @@ def test_full_rollout_against_float64_fixture():
         assert rel(proj[8:], fx["proj_adjoint"][8:]) < 8e-2 and rel(proj[8:], fx["proj_fd"][8:]) < 8e-2
         runs.append(proj)
     proj = np.mean(runs, axis=0)
-    assert rel(proj[8:], fx["proj_adjoint"][8:]) < 3e-2 and rel(proj[8:], fx["proj_fd"][8:]) < 3e-2
+    assert rel(proj[8:], fx["proj_adjoint"][8:]) < 4e-2 and rel(proj[8:], fx["proj_fd"][8:]) < 4e-2
     # v0 directions: contact-conditioned (see test_contact_gradient_matches_float64_adjoint) and the
     # loss is rough at finite-difference scale in v0 here, so only the oracle's adjoint is the reference
     assert rel(proj[:8], fx["proj_adjoint"][:8]) < 5e-2
