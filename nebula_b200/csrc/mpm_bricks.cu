@@ -561,7 +561,9 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_
   if (threadIdx.x == 0) sm.numCells[par] = 0u;  // reused two chunks later, after another barrier
 }
 
-// Sum the tile copies and add every non-zero node to the global grid.
+// Sum the tile copies, add every non-zero node to the global grid and leave
+// the tile zeroed (each node is read and cleared by the one thread that owns
+// it) for the CTA's next item.
 template <class SM>
 __device__ __forceinline__ void p2gFlush(const SubstepParams& P, SM& sm, int tx, int ty, int tz, float4* acc) {
   const int cr = int(P.cubeRes);
@@ -569,11 +571,15 @@ __device__ __forceinline__ void p2gFlush(const SubstepParams& P, SM& sm, int tx,
     float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
     for (int w = 0; w < kTileCopies; ++w) {
-      const float* t = sm.tiles + w * 4 * kTileNodes;
+      float* t = sm.tiles + w * 4 * kTileNodes;
       m += t[q];
       mx += t[kTileNodes + q];
       my += t[2 * kTileNodes + q];
       mz += t[3 * kTileNodes + q];
+      t[q] = 0.f;
+      t[kTileNodes + q] = 0.f;
+      t[2 * kTileNodes + q] = 0.f;
+      t[3 * kTileNodes + q] = 0.f;
     }
     if (m == 0.f && mx == 0.f && my == 0.f && mz == 0.f) continue;
     const int nx = tx + (q & 7), ny = ty + ((q >> 3) & 7), nz = tz + (q >> 6);
@@ -879,6 +885,10 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
   waitForPredecessorGrid();
   const uint32_t numPB = B.counters[kCntNumPB];
   const uint32_t numItems = numPB * split;
+  // The tile, cell lists and counters start zeroed here and are left so by
+  // every item (the flush clears the tile, the list walk the cell heads, each
+  // chunk its cell count, thread 0 the marks after the item's last barrier).
+  p2gZeroTiles(sm);
   // the claim alternates between two slots: a thread may claim the next item
   // while others still read this one, never two ahead (one barrier per claim)
   for (uint32_t it = 0;; it ^= 1u) {
@@ -890,8 +900,6 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
     const uint32_t b = B.pbBrick[bi], end = min(B.pbStart[bi + 1], n), first = min(B.pbStart[bi], end) + part * uint32_t(CHUNK);
     if (first >= end) continue;  // the brick has no chunk for this part
     const uint32_t start = first, stride = split * uint32_t(CHUNK);
-    p2gZeroTiles(sm);
-    __syncthreads();
     if constexpr (BATCH) {
       __shared__ SubstepParams sP;
       __shared__ uint32_t sBase;
@@ -907,6 +915,7 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
       g2p2gItem<FLIP, CHUNK>(P0, S, b, start, end, stride, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
     }
     __syncthreads();
+    if (threadIdx.x == 0) sm.markMask = 0u;  // read before the barrier, set again after the next claim's
   }
 }
 
