@@ -92,3 +92,15 @@ def test_create_without_device_reports_error(lib):
     rc = lib.nebula_mpm_create(C.byref(MPMConfig(nx=2, ny=2, nz=2).to_c()), C.byref(h))
     assert rc in (_capi.ERR_CUDA, _capi.ERR_OOM)
     assert _capi.last_error()
+
+
+def test_header_is_plain_c():
+    """The boundary header compiles as C99 on its own (no C++ types cross the ABI)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    r = subprocess.run([cc, "-x", "c", "-std=c99", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", str(ROOT / "include" / "nebula_mpm.h")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
