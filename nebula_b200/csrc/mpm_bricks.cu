@@ -748,15 +748,26 @@ __global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, ui
   permScatterStrided(B, n, err, uint64_t(blockIdx.x) * blockDim.x + threadIdx.x, uint64_t(gridDim.x) * blockDim.x);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t numGB = B.counters[kCntNumGB];
-  for (uint32_t gb = blockIdx.x * (kThreads / 32) + warp; gb < numGB; gb += gridDim.x * (kThreads / 32)) {
+  // Each warp takes a contiguous run of the (ascending) grid-brick list, so
+  // consecutive bricks mostly share a scene: the scene is searched once and
+  // then advanced, and its parameters are copied only when it changes.
+  const uint32_t warps = gridDim.x * (kThreads / 32), gw = blockIdx.x * (kThreads / 32) + warp;
+  const uint32_t per = (numGB + warps - 1) / warps;
+  const uint32_t g0 = min(gw * per, numGB), g1 = min(g0 + per, numGB);
+  uint32_t sc = g0 < g1 ? findScene(T.brickBase, T.count, B.gbBrick[g0]) : 0u;
+  uint32_t loaded = 0xFFFFFFFFu;
+  for (uint32_t gb = g0; gb < g1; ++gb) {
     const uint32_t bg = B.gbBrick[gb];
-    const uint32_t sc = findScene(T.brickBase, T.count, bg);
+    while (sc + 1u < T.count && T.brickBase[sc + 1u] <= bg) ++sc;
     const uint32_t base = T.brickBase[sc];
-    __syncwarp();
-    copyParams(&sP[warp], T.params + sc, lane, 32);
-    __syncwarp();
-    if (lane == 0) sP[warp].colliders += size_t(substep) * sP[warp].colliderCount;
-    __syncwarp();
+    if (sc != loaded) {
+      __syncwarp();
+      copyParams(&sP[warp], T.params + sc, lane, 32);
+      __syncwarp();
+      if (lane == 0) sP[warp].colliders += size_t(substep) * sP[warp].colliderCount;
+      __syncwarp();
+      loaded = sc;
+    }
     const SubstepParams& P = sP[warp];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
