@@ -535,21 +535,51 @@ typedef struct nebula_mpm_particles {
 size_t nebula_mpm_bin_workspace_size(uint32_t hashCells, uint32_t particleCount);
 int nebula_mpm_bin(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSorted,
                    void* dWorkspace, size_t workspaceBytes, void* stream);
-/* Same outputs as nebula_mpm_bin, for callers that cannot provide or allocate a
- * workspace: the scratch is a fixed file-scope device array inside the library
- * (hashCells <= nebula_mpm_bin_noalloc_max_cells() = 2^21, i.e. 128^3, and
- * particleCount <= nebula_mpm_bin_noalloc_max_particles() = 2^18; larger
- * sizes return NEBULA_MPM_ERR_INVALID).  No device memory is allocated.  The
- * first call on each device (with that device current) looks up the array's
- * address; make it before any stream capture.  Every call clears what it
- * needs on the stream.  Calls on one device share the scratch, so calls that
- * can overlap in time must be ordered by the caller.  This entry point has no
- * counterpart in the reference: its binning (mpm_hash_count.comp,
- * hash_scan_*.comp, mpm_hash_sort.comp) runs on engine-owned buffers only. */
+/* Error word of the last nebula_mpm_bin (or nebula_hash_bin) that used this
+ * workspace, read on `stream` (the call synchronizes it): *errorBits = 0 and
+ * NEBULA_MPM_OK when the binning ran clean; otherwise the bits (1: a bounded
+ * look-back wait of the scan expired, 8: a binning index fell outside the
+ * particle range, which follows an expired wait) and NEBULA_MPM_ERR_DEVICE.
+ * hashCells / particleCount are those of the binning call.  The bits stay in
+ * the workspace until the next binning call clears them.  The reference
+ * reports nothing from its binning dispatches (MPMEngine.cpp:423-456). */
+int nebula_mpm_bin_status(const void* dWorkspace, size_t workspaceBytes, uint32_t hashCells, uint32_t particleCount, uint32_t* errorBits,
+                          void* stream);
+/* Self-test of that failure path on a caller workspace: one CTA of the
+ * binning scan runs as tile 1 against a tile 0 that never publishes, so its
+ * bounded look-back (about a second) gives up and sets bit 1 in the
+ * workspace's error word, which nebula_mpm_bin_status then returns.  Reads
+ * dCellCount[0, hashCells) and writes only workspace words; needs hashCells
+ * >= 4096.  No counterpart in the reference. */
+int nebula_mpm_bin_probe_wait_expiry(const nebula_mpm_pass* pass, const uint32_t* dCellCount, void* dWorkspace, size_t workspaceBytes,
+                                     void* stream);
+/* Same outputs as nebula_mpm_bin, for callers that cannot allocate device
+ * memory or hand over a workspace: a foreign-function binding that holds only
+ * the three output arrays, or a frame loop that must not call cudaMalloc
+ * (which may synchronize the whole device) between frames.  The scratch is a
+ * fixed file-scope device array inside the library, held by every GPU that
+ * loads it until the process exits: hashCells <=
+ * nebula_mpm_bin_noalloc_max_cells() = 2^21 (128^3) and particleCount <=
+ * nebula_mpm_bin_noalloc_max_particles() = 2^18; larger sizes return
+ * NEBULA_MPM_ERR_INVALID.  No device memory is allocated.  The first call in
+ * each CUDA context (with its device current) looks up the array's address;
+ * make it before any stream capture.  Every call clears what it needs on the
+ * stream.  Calls on one device share the scratch, so calls that can overlap
+ * in time race and must be ordered by the caller.  No counterpart in the
+ * reference. */
 size_t nebula_mpm_bin_noalloc_max_cells(void);
 size_t nebula_mpm_bin_noalloc_max_particles(void);
 int nebula_mpm_bin_noalloc(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dCellCount, uint32_t* dCellOffset, uint32_t* dSorted,
                            void* stream);
+/* Error word of the last nebula_mpm_bin_noalloc on the current device, read
+ * on `stream` (synchronized): the bits and status codes of
+ * nebula_mpm_bin_status.  Allocates nothing.  No counterpart in the reference. */
+int nebula_mpm_bin_noalloc_status(uint32_t* errorBits, void* stream);
+/* nebula_mpm_bin_probe_wait_expiry on the library-held scratch (hashCells >=
+ * 4096 and within the limits above); read the result with
+ * nebula_mpm_bin_noalloc_status.  Allocates nothing.  No counterpart in the
+ * reference. */
+int nebula_mpm_bin_noalloc_probe_wait_expiry(const nebula_mpm_pass* pass, const uint32_t* dCellCount, void* stream);
 /* mpm_zero_grid.comp + mpm_p2g.comp: writes gridMom[0, hashCells) (w = 0) and
  * gridMass; clears gridMom[hashCells, 2 hashCells). */
 int nebula_mpm_p2g(const nebula_mpm_pass* pass, const nebula_mpm_particles* parts, const uint32_t* dCellCount, const uint32_t* dCellOffset,

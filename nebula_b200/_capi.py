@@ -176,6 +176,10 @@ _SIGS = {
     "nebula_mpm_bin_noalloc_max_cells": (C.c_size_t, []),
     "nebula_mpm_bin_noalloc_max_particles": (C.c_size_t, []),
     "nebula_mpm_bin_noalloc": (C.c_int, [C.POINTER(Pass), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_bin_status": (C.c_int, [C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), C.c_void_p]),
+    "nebula_mpm_bin_probe_wait_expiry": (C.c_int, [C.POINTER(Pass), C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "nebula_mpm_bin_noalloc_status": (C.c_int, [C.POINTER(C.c_uint32), C.c_void_p]),
+    "nebula_mpm_bin_noalloc_probe_wait_expiry": (C.c_int, [C.POINTER(Pass), C.c_void_p, C.c_void_p]),
     "nebula_mpm_p2g": (C.c_int, [C.POINTER(Pass), C.POINTER(Particles), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p]),
     "nebula_mpm_grid_update": (C.c_int, [C.POINTER(Pass), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

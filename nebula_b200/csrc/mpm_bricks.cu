@@ -758,6 +758,10 @@ __global__ void __launch_bounds__(kThreads) k_grid_bricks_batch(SceneTable T, ui
   uint32_t loaded = 0xFFFFFFFFu;
   for (uint32_t gb = g0; gb < g1; ++gb) {
     const uint32_t bg = B.gbBrick[gb];
+    // k_brick_scan lists grid bricks in ascending order, so the scene only
+    // moves forward; a brick below the current scene's base (a list built
+    // otherwise) is searched for again instead of taking the wrong scene
+    if (bg < T.brickBase[sc]) sc = findScene(T.brickBase, T.count, bg);
     while (sc + 1u < T.count && T.brickBase[sc + 1u] <= bg) ++sc;
     const uint32_t base = T.brickBase[sc];
     if (sc != loaded) {

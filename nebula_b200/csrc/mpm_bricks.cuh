@@ -33,7 +33,7 @@ struct BrickBuffers {
   uint32_t* brickStart;       // [nb] first sorted slot of each brick
   uint32_t* pbBrick;          // [nb] particle-brick list
   uint32_t* pbStart;          // [nb + 1] first slot of each listed brick; pbStart[numPB] = total
-  uint32_t* gbBrick;          // [nb] grid-brick list
+  uint32_t* gbBrick;          // [nb] grid-brick list, ascending (k_brick_scan writes it in brick order)
   uint32_t* counters;         // [kCntSlots]
   unsigned long long* scanState;  // [3 * tiles] status words (epoch-tagged)
   unsigned long long* scanTile;   // monotone tile counter

@@ -6,6 +6,7 @@
 // buildHashGridCPU, tests/helpers/MPMHarness.cpp:132-178, 260-282), plus the
 // PBF engine's spatial hash on the same counting sort (nebula_hash_bin).
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "mpm_engine.h"
@@ -83,6 +84,31 @@ BinWorkspaceLayout binLayout(uint32_t nc, uint32_t n) {
   return L;
 }
 
+// The counting sort's buffers inside a caller workspace laid out by binLayout.
+BinBuffers workspaceBins(const BinWorkspaceLayout& L, void* dWorkspace, uint32_t hashCells) {
+  char* ws = static_cast<char*>(dWorkspace);
+  BinBuffers b{};
+  b.cellStart = reinterpret_cast<uint32_t*>(ws + L.cellStart);
+  b.key = reinterpret_cast<uint32_t*>(ws + L.key);
+  b.rank = reinterpret_cast<uint32_t*>(ws + L.rank);
+  b.sortedTmp = reinterpret_cast<uint32_t*>(ws + L.sortedTmp);
+  b.tileState = reinterpret_cast<unsigned long long*>(ws + L.tiles);
+  b.tileCounter = reinterpret_cast<uint32_t*>(b.tileState + scanTiles(hashCells));
+  b.err = reinterpret_cast<uint32_t*>(ws + L.err);
+  return b;
+}
+
+}  // namespace
+
+void throwBinErrors(uint32_t bits) {
+  if (!bits) return;
+  char buf[192];
+  std::snprintf(buf, sizeof(buf), "binning error bits 0x%x (1: a scan look-back wait expired, 8: a binning index fell outside [0, n))", bits);
+  throw Error(NEBULA_MPM_ERR_DEVICE, buf);
+}
+
+namespace {
+
 template <class F> int guarded(F&& f) {
   try {
     f();
@@ -114,22 +140,46 @@ int nebula_mpm_bin(const nebula_mpm_pass* pass, const float* dPos4, uint32_t* dC
     if (!dWorkspace || workspaceBytes < L.total) throw Error(NEBULA_MPM_ERR_INVALID, "bin workspace too small");
     if (!dCellCount || !dCellOffset || (n && (!dPos4 || !dSorted))) throw Error(NEBULA_MPM_ERR_INVALID, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    char* ws = static_cast<char*>(dWorkspace);
-    BinBuffers b;
+    BinBuffers b = workspaceBins(L, dWorkspace, pass->hashCells);
     b.cellCount = dCellCount;
-    b.cellStart = reinterpret_cast<uint32_t*>(ws + L.cellStart);
     b.cellEnd = dCellOffset;
-    b.key = reinterpret_cast<uint32_t*>(ws + L.key);
-    b.rank = reinterpret_cast<uint32_t*>(ws + L.rank);
-    b.sortedTmp = reinterpret_cast<uint32_t*>(ws + L.sortedTmp);
     b.sorted = dSorted;
-    b.tileState = reinterpret_cast<unsigned long long*>(ws + L.tiles);
-    b.tileCounter = reinterpret_cast<uint32_t*>(b.tileState + scanTiles(pass->hashCells));
-    b.err = reinterpret_cast<uint32_t*>(ws + L.err);
     check(cudaMemsetAsync(b.err, 0, 4, s), "memset");
     uint64_t launches = 0;
     SubstepParams P = fromPass(*pass, nullptr, nullptr, nullptr, nullptr);
     check(launchBin(P, reinterpret_cast<const float4*>(dPos4), n, b, s, &launches), "bin");
+  });
+}
+
+int nebula_mpm_bin_status(const void* dWorkspace, size_t workspaceBytes, uint32_t hashCells, uint32_t particleCount, uint32_t* errorBits,
+                          void* stream) {
+  return guarded([&] {
+    if (!errorBits) throw Error(NEBULA_MPM_ERR_INVALID, "null output");
+    *errorBits = 0;
+    const BinWorkspaceLayout L = binLayout(hashCells, particleCount);
+    if (!dWorkspace || workspaceBytes < L.total) throw Error(NEBULA_MPM_ERR_INVALID, "bin workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t bits = 0;
+    check(cudaMemcpyAsync(&bits, static_cast<const char*>(dWorkspace) + L.err, sizeof(bits), cudaMemcpyDeviceToHost, s), "read error word");
+    check(cudaStreamSynchronize(s), "stream synchronize");
+    *errorBits = bits;
+    throwBinErrors(bits);
+  });
+}
+
+int nebula_mpm_bin_probe_wait_expiry(const nebula_mpm_pass* pass, const uint32_t* dCellCount, void* dWorkspace, size_t workspaceBytes,
+                                     void* stream) {
+  return guarded([&] {
+    validate(pass);
+    if (pass->hashCells < 2u * uint32_t(kScanTile)) throw Error(NEBULA_MPM_ERR_INVALID, "the probe needs hashCells >= 4096");
+    const BinWorkspaceLayout L = binLayout(pass->hashCells, pass->particleCount);
+    if (!dWorkspace || workspaceBytes < L.total) throw Error(NEBULA_MPM_ERR_INVALID, "bin workspace too small");
+    if (!dCellCount) throw Error(NEBULA_MPM_ERR_INVALID, "null buffer");
+    BinBuffers b = workspaceBins(L, dWorkspace, pass->hashCells);
+    b.cellCount = const_cast<uint32_t*>(dCellCount);
+    uint64_t launches = 0;
+    SubstepParams P = fromPass(*pass, nullptr, nullptr, nullptr, nullptr);
+    check(launchBinScanExpiryProbe(P, b, static_cast<cudaStream_t>(stream), &launches), "bin scan probe");
   });
 }
 
@@ -152,18 +202,10 @@ int nebula_hash_bin(const nebula_hash_grid* grid, const float* dPredP4, const ui
     if (!dWorkspace || workspaceBytes < L.total) throw Error(NEBULA_MPM_ERR_INVALID, "hash workspace too small");
     if (!dCellCount || !dCellOffset || (n && (!dPredP4 || !dSortedIdx))) throw Error(NEBULA_MPM_ERR_INVALID, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    char* ws = static_cast<char*>(dWorkspace);
-    BinBuffers b;
+    BinBuffers b = workspaceBins(L, dWorkspace, grid->hashCells);
     b.cellCount = dCellCount;
-    b.cellStart = reinterpret_cast<uint32_t*>(ws + L.cellStart);
     b.cellEnd = dCellOffset;
-    b.key = reinterpret_cast<uint32_t*>(ws + L.key);
-    b.rank = reinterpret_cast<uint32_t*>(ws + L.rank);
-    b.sortedTmp = reinterpret_cast<uint32_t*>(ws + L.sortedTmp);
     b.sorted = dSortedIdx;
-    b.tileState = reinterpret_cast<unsigned long long*>(ws + L.tiles);
-    b.tileCounter = reinterpret_cast<uint32_t*>(b.tileState + scanTiles(grid->hashCells));
-    b.err = reinterpret_cast<uint32_t*>(ws + L.err);
     b.typeFlag = dTypeFlag;
     check(cudaMemsetAsync(b.err, 0, 4, s), "memset");
     SubstepParams P{};

@@ -26,6 +26,8 @@ struct Error : std::runtime_error {
 };
 void check(cudaError_t e, const char* what);
 extern thread_local std::string g_last_error;
+// Throws NEBULA_MPM_ERR_DEVICE naming the error bits of a single-pass binning call (none: returns).
+void throwBinErrors(uint32_t bits);
 
 // Rigid pose applied to a mesh on the device (transformTriangles, MeshSDF.h:134-141):
 // v -> q * v + t, n -> q * n; q a unit quaternion (w, x, y, z).

@@ -42,6 +42,13 @@ size_t scanWorkspaceBytes(uint64_t n);
 // Counting sort of particles by Morton cell: counts, exclusive scan, scatter,
 // then in-cell ordering by ascending particle index.  `launches` counts kernels.
 cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, const BinBuffers& b, cudaStream_t s, uint64_t* launches);
+// Failure-path self-test of launchBin's scan on the same buffers: one CTA of
+// the cell scan runs as tile 1 against a tile 0 that never publishes, so its
+// bounded look-back gives up, sets kErrScanTimeout in *b.err and returns
+// (about a second).  Reads cellCount[0, hashCells), writes only workspace
+// words (cellStart of tile 1, the status words, the ticket, the error word).
+// Needs hashCells >= 2 scan tiles (4,096 cells).
+cudaError_t launchBinScanExpiryProbe(const SubstepParams& P, const BinBuffers& b, cudaStream_t s, uint64_t* launches);
 // Particle-major P2G into the reference's dense grid layout (grid must be zeroed).
 cudaError_t launchP2GDense(const SubstepParams& P, StatePtrs st, const uint32_t* sorted, uint32_t n, float4* gridMom, float* gridMass,
                            cudaStream_t s, uint64_t* launches);

@@ -202,6 +202,21 @@ cudaError_t launchBin(const SubstepParams& P, const float4* pos, uint32_t n, con
   return cudaGetLastError();
 }
 
+cudaError_t launchBinScanExpiryProbe(const SubstepParams& P, const BinBuffers& b, cudaStream_t s, uint64_t* launches) {
+  const uint64_t nc = P.hashCells;
+  const uint32_t tiles = scanTiles(nc);
+  if (tiles < 2) return cudaErrorInvalidValue;
+  // every status word unpublished and the tile ticket at 1: the single CTA
+  // below becomes tile 1 and waits on a tile 0 that never runs
+  cudaError_t e = cudaMemsetAsync(b.tileState, 0, (size_t(tiles) + 1) * sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.err, 0, sizeof(uint32_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b.tileCounter, 1, 1, s);  // little-endian u32 = 1
+  if (e != cudaSuccess) return e;
+  k_scan_exclusive<<<1, kScanThreads, 0, s>>>(b.cellCount, b.cellStart, nullptr, nc, b.tileState, b.tileCounter, b.err, nullptr);
+  ++*launches;
+  return cudaGetLastError();
+}
+
 cudaError_t launchP2GDense(const SubstepParams& P, StatePtrs st, const uint32_t* sorted, uint32_t n, float4* gridMom, float* gridMass,
                            cudaStream_t s, uint64_t* launches) {
   if (n == 0) return cudaSuccess;

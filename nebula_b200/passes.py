@@ -106,6 +106,19 @@ class PassRunner:
         call("nebula_mpm_bin", C.byref(p), _vp(self.state[0]), _vp(self.cell_count), _vp(self.cell_offset), _vp(self.sorted),
              _vp(self.ws), self.ws.numel(), self._stream())
 
+    def bin_status(self) -> tuple[int, int]:
+        """(status code, error bits) of the last bin() on this workspace
+        (nebula_mpm_bin_status; synchronizes the stream)."""
+        bits = C.c_uint32(0)
+        rc = _capi.lib().nebula_mpm_bin_status(_vp(self.ws), self.ws.numel(), self.nc, self.n, C.byref(bits), self._stream())
+        return int(rc), int(bits.value)
+
+    def probe_bin_wait_expiry(self):
+        """Make the binning scan's bounded look-back expire on this workspace
+        (nebula_mpm_bin_probe_wait_expiry); bin_status() then reports bit 1."""
+        p = make_pass(self.sp, self.n)
+        call("nebula_mpm_bin_probe_wait_expiry", C.byref(p), _vp(self.cell_count), _vp(self.ws), self.ws.numel(), self._stream())
+
     def p2g(self):
         p = make_pass(self.sp, self.n)
         parts = self._parts()

@@ -60,3 +60,29 @@ def test_noalloc_matches_workspace_bin_two_calls(cuda_lib):
         for a, b in zip(g, want):
             assert np.array_equal(a, b)
         assert int(g[0].sum()) == r.n
+
+
+@pytest.mark.gpu
+def test_noalloc_status_reports_an_expired_wait(cuda_lib):
+    """The error word of the library-held scratch reaches the caller through
+    nebula_mpm_bin_noalloc_status: clean after a call, the scan-timeout bit
+    after the probe has made the scan's bounded look-back expire, clean again
+    after the next call, whose bins equal nebula_mpm_bin's."""
+    lib = _capi.lib()
+    sc = S.elastic_block()
+    r = PassRunner(sc.params, sc.n)
+    r.upload_particles(sc.state)
+    stream = C.c_void_p(torch.cuda.current_stream(r.dev).cuda_stream)
+    bits = C.c_uint32(7)
+    first = _noalloc_bins(r)
+    assert lib.nebula_mpm_bin_noalloc_status(C.byref(bits), stream) == _capi.OK and bits.value == 0
+    p = make_pass(r.sp, r.n)
+    counts = torch.zeros(r.nc, dtype=torch.int32, device=r.dev)  # the probe reads hashCells counts
+    _capi.call("nebula_mpm_bin_noalloc_probe_wait_expiry", C.byref(p), C.c_void_p(counts.data_ptr()), stream)
+    assert lib.nebula_mpm_bin_noalloc_status(C.byref(bits), stream) == _capi.ERR_DEVICE
+    assert bits.value & 1, bits.value
+    again = _noalloc_bins(r)
+    assert lib.nebula_mpm_bin_noalloc_status(C.byref(bits), stream) == _capi.OK and bits.value == 0
+    r.bin()
+    for a, b, c in zip(again, first, r.read_bins()):
+        assert np.array_equal(a, b) and np.array_equal(a, c)
