@@ -40,12 +40,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nebula", choices=["nebula", "reference"])
     ap.add_argument("--workload", default="slope", choices=["slope", "elastic", "multimaterial"])
-    ap.add_argument("--substeps", type=int, default=10, help="substeps per step() call")
+    ap.add_argument("--substeps", type=int, default=25,
+                    help="substeps per step() call; the timed steps run substeps 1 .. steps * substeps of the workload "
+                         "(default 20 x 25 = the 500 substeps of the slope scene)")
     ap.add_argument("--pipeline", default="fused", choices=["fused", "dense"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-substeps", type=int, default=0, help="oracle substeps timed for cpu_baseline (0 = auto)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain measurement on the 64-scene mix")
-    ap.add_argument("--batch-steps", type=int, default=5, help="timed steps of the batched / plain comparison")
+    ap.add_argument("--batch-steps", type=int, default=10,
+                    help="timed steps of 20 substeps of the batched / plain comparison (10 = the mix's 200 substeps)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-vs-forward measurement")
     ap.add_argument("--no-mesh-sdf", action="store_true", help="skip the mesh -> SDF build measurement")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner's")
@@ -257,19 +260,23 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None, tune: bool 
     scenes = S.batch_mix(only=set(mine))
     n_all = sum(sizes)
     dt = scenes[0].params.dt
-    frames = warmup + steps
+    frames = max(warmup, steps)
     tracks = [[S.collider_track(sc, substeps, k * substeps) for k in range(frames)] for sc in scenes]
     stream = torch.cuda.Stream()
 
-    def timed(step_fn):
+    def timed(step_fn, restart):
+        # warm-up steps from the initial states, then the initial states again:
+        # the timed steps cover substeps 1 .. steps * substeps of the mix
         for k in range(warmup):
             step_fn(k)
+        torch.cuda.synchronize()
+        restart()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for k in range(warmup, frames):
+        for k in range(steps):
             step_fn(k)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -290,8 +297,12 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None, tune: bool 
             b.set_collider_track(s, tracks[i][k])
         b.step(dt * substeps, substeps, stream)
 
+    def batch_restart():
+        for i, s in enumerate(ids):
+            b.upload_state(s, scenes[i].state)
+
     st0 = b.stats()
-    ms_b = timed(batch_step)
+    ms_b = timed(batch_step, batch_restart)
     b.sync()
     st1 = b.stats()
     launches_b = int(st1["kernel_launches"] - st0["kernel_launches"])
@@ -306,8 +317,12 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None, tune: bool 
             e.setColliderTrack(tracks[i][k])
             e.step(dt * substeps, stream)
 
+    def plain_restart():
+        for i, e in enumerate(engines):
+            e.upload_state(scenes[i].state)
+
     l0 = sum(e.stats()["kernel_launches"] for e in engines)
-    ms_p = timed(plain_step)
+    ms_p = timed(plain_step, plain_restart)
     for e in engines:
         e.sync()
     launches_p = int(sum(e.stats()["kernel_launches"] for e in engines) - l0)
@@ -315,6 +330,7 @@ def measure_batch(steps: int, warmup: int, substeps: int, dist=None, tune: bool 
         e.cleanup()
     ps = float(n_all) * substeps * steps
     return {"workload": "batch_mix_64", "scenes": len(sizes), "particles": n_all, "substeps_per_step": substeps, "steps": steps,
+            "substep_range": [1, steps * substeps],
             "warmup": warmup, "dt": dt, "value": ps / (ms_b * 1e-3), "ms_per_step": ms_b / steps, "plain_value": ps / (ms_p * 1e-3),
             "plain_ms_per_step": ms_p / steps, "speedup": ms_p / ms_b, "unit": UNIT, "gpu_launches": launches_b,
             "plain_gpu_launches": launches_p, "n_gpus": world, "scaling": "strong" if world > 1 else "single",
@@ -578,8 +594,12 @@ def main():
         tuned = {"shape": rep["shape"], "source": rep["source"], "ms_per_substep": rep["ms_per_substep"],
                  "default_ms_per_substep": rep["default_ms_per_substep"], "shapes_tried": len(rep["tried"]), "key": rep["key"]}
 
+    # warm-up steps from the initial state, then the initial state again: the
+    # timed steps cover substeps 1 .. steps * substeps of the workload
     for _ in range(args.warmup):
         eng.step(dt_frame, stream)
+    eng.sync()
+    eng.upload_state(sc.state)
     eng.sync()
 
     # ---- L2: inputs larger than L2, or a flush written between the timed steps
@@ -612,6 +632,9 @@ def main():
     eng.upload_state(sc.state)
     for _ in range(args.warmup):
         eng.step(dt_frame, stream)
+    eng.sync()
+    eng.upload_state(sc.state)
+    eng.sync()
     eng.profile(True)
     eng.profile_read(reset=True)
     for _ in range(prof_steps):
@@ -703,6 +726,7 @@ def main():
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
         "config": {"workload": sc.name, "particles": n, "grid": list(sp.grid_res), "substeps_per_step": S, "dt": sp.dt,
+                   "substep_range": [1, args.steps * S], "workload_substeps": sc.substeps,
                    "transfer": "APIC" if sp.flip_ratio < -0.5 else ("FLIP" if flip else "PIC"), "parallelism": "replicas" if world > 1 else "single", "pipeline": args.pipeline,
                    "l2": l2_note, "active_nodes": active},
         "roofline": roofline,

@@ -158,6 +158,16 @@ int nebula_mpm_set_collider_mesh(nebula_mpm* e, const float* tris, uint32_t n);
  * triangles of the last nebula_mpm_set_collider_mesh: no host transfer.
  * rotation_wxyz: unit quaternion (w, x, y, z). */
 int nebula_mpm_set_collider_mesh_pose(nebula_mpm* e, const float translation[3], const float rotation_wxyz[4]);
+/* Closest-point definition of the engine's mesh SDF builds, from the next
+ * nebula_mpm_set_collider_mesh / _pose on: NEBULA_MPM_CLOSEST_POINT_COMPLETE
+ * (default; the complete Voronoi-region test) or
+ * NEBULA_MPM_CLOSEST_POINT_REFERENCE (closestPtOnTriangle of MeshSDF.h:48-78
+ * step for step, without its edge-BC region, by brute force over the
+ * triangles as buildMeshSDF does: the reference's SDF exactly, including its
+ * wrong distances and signs where edge BC is closest). */
+#define NEBULA_MPM_CLOSEST_POINT_COMPLETE 0
+#define NEBULA_MPM_CLOSEST_POINT_REFERENCE 1
+int nebula_mpm_set_collider_mesh_closest_point(nebula_mpm* e, int mode);
 /* EngineBase::setForces / addForce / clearForces (EngineBase.cpp:22-40):
  * replaces the force table (n <= 16).  No shader is rebuilt: forces are a
  * kernel parameter table. */
@@ -501,6 +511,17 @@ int nebula_mpm_mesh_build_sdf(const nebula_mpm_mesh* m, const float translation[
  * the pose applied on the device; a null translation or rotation is the identity. */
 int nebula_mpm_mesh_sdf_posed(const float* dTris, uint32_t nTris, const float translation[3], const float rotation_wxyz[4],
                               const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream);
+/* buildMeshSDF (MeshSDF.h:98-132) with the reference's own closest point
+ * (closestPtOnTriangle, MeshSDF.h:48-78, no edge-BC region): every cell
+ * visits every triangle, O(cells x triangles), since that point can lie
+ * outside the triangle and no distance bound holds for it.  Same arguments
+ * and output as nebula_mpm_mesh_sdf_posed (null translation / rotation =
+ * identity); the _build_ form takes a prepared mesh, keeping the first-in-
+ * list rule for equal distances. */
+int nebula_mpm_mesh_sdf_reference(const float* dTris, uint32_t nTris, const float translation[3], const float rotation_wxyz[4],
+                                  const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream);
+int nebula_mpm_mesh_build_sdf_reference(const nebula_mpm_mesh* m, const float translation[3], const float rotation_wxyz[4],
+                                        const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream);
 
 /* ---------------------------------------------------------------- single passes
  * One reference dispatch each, on caller-owned DEVICE buffers in the reference

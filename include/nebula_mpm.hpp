@@ -112,6 +112,10 @@ class MPMEngine {
   void setColliderMeshPose(const float translation[3], const float rotationWxyz[4]) {
     ok(nebula_mpm_set_collider_mesh_pose(e_, translation, rotationWxyz));
   }
+  // true: later mesh builds take the reference's closestPtOnTriangle (its exact SDF)
+  void setColliderMeshClosestPoint(bool reference) {
+    ok(nebula_mpm_set_collider_mesh_closest_point(e_, reference ? NEBULA_MPM_CLOSEST_POINT_REFERENCE : NEBULA_MPM_CLOSEST_POINT_COMPLETE));
+  }
 
   // the force table of EngineBase (EngineBase.cpp:22-40)
   void addForce(const nebula_mpm_force& f) {

@@ -11,6 +11,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libnebula_mpm.so"
 
 OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_DEVICE, ERR_UNSUPPORTED = range(6)
+CLOSEST_POINT_COMPLETE, CLOSEST_POINT_REFERENCE = 0, 1
 PIPELINE_DENSE, PIPELINE_FUSED = 0, 1
 
 
@@ -103,6 +104,11 @@ _SIGS = {
     "nebula_mpm_mesh_sdf_posed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32 * 3, C.c_uint32, C.c_float,
                                             C.c_void_p, C.c_void_p]),
     "nebula_mpm_set_collider_mesh_pose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nebula_mpm_set_collider_mesh_closest_point": (C.c_int, [C.c_void_p, C.c_int]),
+    "nebula_mpm_mesh_sdf_reference": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32 * 3, C.c_uint32, C.c_float,
+                                               C.c_void_p, C.c_void_p]),
+    "nebula_mpm_mesh_build_sdf_reference": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32 * 3, C.c_uint32, C.c_float, C.c_void_p,
+                                                     C.c_void_p]),
     "nebula_mpm_set_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "nebula_mpm_append_particles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "nebula_mpm_reset_particles": (C.c_int, [C.c_void_p]),

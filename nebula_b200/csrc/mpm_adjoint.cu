@@ -185,7 +185,7 @@ __device__ __forceinline__ void henckyAdj(const double Fm[3][3], double mu, doub
 #pragma unroll
     for (int r = 0; r < 3; ++r) F.m[c][r] = Fm[r][c];
   double s[3];
-  svd3(F, Ug, s, Vg);
+  svd3F64(F, Ug, s, Vg);
   double tb[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -262,14 +262,14 @@ struct Stencil {
 };
 
 __device__ __forceinline__ void stencilAt(const SubstepParams& P, const float xp[3], const int base[3], Stencil& S) {
-  const float h = P.cellSize;
+  const float invH = 1.0f / P.cellSize;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     S.base[a] = base[a];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       S.xi[a][k] = nodeCentre(P, a, base[a] + k);
-      const float d = __fdiv_rn(xp[a] - S.xi[a][k], h);
+      const float d = (xp[a] - S.xi[a][k]) * invH;
       S.w[a][k] = bspline2(d);
       S.g[a][k] = bspline2g(d);
       S.hh[a][k] = bspline2h(d);
@@ -282,13 +282,13 @@ struct NodeTerms {
 };
 
 __device__ __forceinline__ void nodeTerms(const SubstepParams& P, const Stencil& S, const float xp[3], int ix, int iy, int iz, NodeTerms& t) {
-  const float h = P.cellSize, ih2 = 1.0f / (h * h);
+  const float h = P.cellSize, invH = 1.0f / h, ih2 = 1.0f / (h * h);
   const float wx = S.w[0][ix], wy = S.w[1][iy], wz = S.w[2][iz];
   const float gx = S.g[0][ix], gy = S.g[1][iy], gz = S.g[2][iz];
   t.w = wx * wy * wz;
-  t.dw[0] = __fdiv_rn(gx * wy * wz, h);
-  t.dw[1] = __fdiv_rn(wx * gy * wz, h);
-  t.dw[2] = __fdiv_rn(wx * wy * gz, h);
+  t.dw[0] = gx * wy * wz * invH;
+  t.dw[1] = wx * gy * wz * invH;
+  t.dw[2] = wx * wy * gz * invH;
   t.H[0][0] = S.hh[0][ix] * wy * wz * ih2;
   t.H[1][1] = wx * S.hh[1][iy] * wz * ih2;
   t.H[2][2] = wx * wy * S.hh[2][iz] * ih2;
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kT) k_adj_g2p(SubstepParams P, St st, const fl
                                                 AdjPtrs ob, AdjPtrs ib, float4* gadj, float* mub, float* lamb) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  const float dt = P.dt, h = P.cellSize;
+  const float dt = P.dt, h = P.cellSize, invH = 1.0f / h;
   const float4 P4 = st.f[0][p];
   const float xp[3] = {P4.x, P4.y, P4.z};
   float F[3][3];
@@ -349,8 +349,8 @@ __global__ void __launch_bounds__(kT) k_adj_g2p(SubstepParams P, St st, const fl
     if (vi.w < 1e-10f) continue;
     const float w = S.w[0][ix] * S.w[1][iy] * S.w[2][iz];
     if (w < 1e-12f) continue;
-    const float dw[3] = {__fdiv_rn(S.g[0][ix] * S.w[1][iy] * S.w[2][iz], h), __fdiv_rn(S.w[0][ix] * S.g[1][iy] * S.w[2][iz], h),
-                         __fdiv_rn(S.w[0][ix] * S.w[1][iy] * S.g[2][iz], h)};
+    const float dw[3] = {S.g[0][ix] * S.w[1][iy] * S.w[2][iz] * invH, S.w[0][ix] * S.g[1][iy] * S.w[2][iz] * invH,
+                         S.w[0][ix] * S.w[1][iy] * S.g[2][iz] * invH};
     const float v[3] = {vi.x, vi.y, vi.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a)

@@ -84,9 +84,15 @@ __device__ __forceinline__ bool stencilBrickMask(const SubstepParams& P, int cx,
   const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, cr) >> 2;
   const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, cr) >> 2;
   if (x0 < bx - 1 || x1 > bx + 1 || y0 < by - 1 || y1 > by + 1 || z0 < bz - 1 || z1 > bz + 1) return false;
-  for (int z = z0; z <= z1; ++z)
-    for (int y = y0; y <= y1; ++y)
-      for (int x = x0; x <= x1; ++x) mask |= 1u << ((z - bz + 1) * 9 + (y - by + 1) * 3 + (x - bx + 1));
+  // per axis the 3-bit set of touched neighbour offsets; their product set is
+  // the bits z*9 + y*3 + x: spreading y's bits to 0/3/6 and z's to 0/9/18
+  // makes it two multiplications (the partial products never overlap)
+  const uint32_t mx = ((2u << (x1 - x0)) - 1u) << (x0 - bx + 1);
+  const uint32_t my = ((2u << (y1 - y0)) - 1u) << (y0 - by + 1);
+  const uint32_t mz = ((2u << (z1 - z0)) - 1u) << (z0 - bz + 1);
+  const uint32_t ys = (my & 1u) | ((my & 2u) << 2) | ((my & 4u) << 4);
+  const uint32_t zs = (mz & 1u) | ((mz & 2u) << 8) | ((mz & 4u) << 16);
+  mask |= (mx * ys) * zs;
   return true;
 }
 
@@ -395,11 +401,12 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 // contributions in registers, then add them into the brick's 8^3 tile (see
 // kTileCopies).  Two barriers per chunk.  The brick ends with one vector
 // reduction per non-zero node of the tile.
-constexpr int kRow = 10;        // float4 per input row: 3 axes x 3 offsets of (A0, A1, A2, W), then (m, -, -, -)
+constexpr int kRow = 9;         // float4 per input row: 3 axes x 3 offsets (see p2gRow)
 constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
 
-constexpr uint32_t kNoRow = 0xFFFFu;  // end of a cell's list
+constexpr uint32_t kNoRow = 0x7FFFu;     // end of a cell's list
+constexpr uint32_t kExactRow = 0x8000u;  // next[] flag: this row is in the exact form (see p2gRow)
 // Copies of the brick's 8^3 accumulation tile: 1 = one tile shared by the
 // warps, updated with shared-memory float reductions (a warp owns one cell at
 // a time, so warps collide only on the nodes where neighbouring cells'
@@ -414,7 +421,8 @@ struct P2GSmemT {
   float4 rows[CHUNK * kRow];
   float tiles[kTileCopies * 4 * kTileNodes];
   uint32_t head[kCellSlots];   // first row of each cell's list (kNoRow: empty)
-  uint16_t next[CHUNK];        // next row of the same cell
+  uint16_t next[CHUNK];        // next row of the same cell, | kExactRow when the row is in the exact form
+  float mass[CHUNK];           // the particle mass of an exact-form row
   uint16_t cells[kCellSlots];  // the chunk's non-empty cells
   uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
   uint32_t markMask;           // grid-active marks of the item brick's 3^3 neighbour bricks
@@ -423,12 +431,17 @@ struct P2GSmemT {
 };
 using P2GSmem = P2GSmemT<kThreads>;
 
-// Push this thread's row onto the list of cell `key` (`par`: the chunk's parity).
+// A stencil-centre cell among the 6^3 around a brick: its coordinates
+// relative to the block origin packed as rx | ry << 3 | rz << 6 (the chunk's
+// cell list holds these), and its slot (rz * 6 + ry) * 6 + rx in head[].
+__device__ __forceinline__ uint32_t cellSlotOf(uint32_t packed) { return ((packed >> 6) * 6u + ((packed >> 3) & 7u)) * 6u + (packed & 7u); }
+
+// Push this thread's row onto the list of the packed cell (`par`: the chunk's parity).
 template <class SM>
-__device__ __forceinline__ void p2gRegister(SM& sm, int key, uint32_t par) {
-  const uint32_t prev = atomicExch(&sm.head[key], threadIdx.x);
-  sm.next[threadIdx.x] = uint16_t(prev);
-  if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(key);
+__device__ __forceinline__ void p2gRegister(SM& sm, uint32_t packed, uint32_t par, bool exact) {
+  const uint32_t prev = atomicExch(&sm.head[cellSlotOf(packed)], threadIdx.x);
+  sm.next[threadIdx.x] = uint16_t(prev | (exact ? kExactRow : 0u));
+  if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(packed);
 }
 
 template <bool FLIP, int CHUNK>
@@ -444,10 +457,23 @@ struct G2P2GSmem {
 //   W_y W_z A_x[dx] + W_x W_z A_y[dy] + W_x W_y A_z[dz]
 // with, per axis c and offset d (r_c = x_i,c - x_p,c, G = N'/h):
 //   A_c[d] = [c == x] m v W_c + (m 4/h^2 B)[:, c] W_c r_c - (dt Vp tau)[:, c] G_c
-// and the mass term is m W_x W_y W_z.  row[3c + d] = (A_c[d], W_c[d]); row[9].x = m.
-__device__ __forceinline__ void p2gRow(const SubstepParams& P, const PState& s, float dtStress, int cx, int cy, int cz, float4* row) {
+// and the mass term is m W_x W_y W_z.  The usual form folds the mass into the
+// x factors:
+//   row[d]     = (A_x[d],     m W_x[d])
+//   row[3 + d] = (A_y[d] / m, W_y[d])
+//   row[6 + d] = (A_z[d] / m, W_z[d])
+// so a node term is  wyz X.xyz + (X.w Z.w) Y.xyz + (X.w Y.w) Z.xyz  and its
+// mass X.w wyz: three vector loads, no per-particle scalar, and no weight
+// test.  The shader skips a node whose weight is below 1e-12
+// (mpm_p2g.comp:47); the smallest of the 27 weights is the product of the
+// three axis minima, so when that product is below 1e-12 (0.15% of the slope
+// scene's particles: near a cell face in all three axes, or very near one),
+// or the mass is not positive, the row is written in the exact form instead,
+// (A_c[d], W_c[d]) for every axis with the mass in `mass`, whose terms carry
+// the shader's test (p2gNodeTermExact).  Returns true for the exact form.
+__device__ __forceinline__ bool p2gRow(const SubstepParams& P, const PState& s, float dtStress, int cx, int cy, int cz, float4* row, float& m) {
   const float invH = 1.0f / P.cellSize;
-  const float m = fetchRho0(P, __float_as_uint(s.v.w)) * s.P.w;
+  m = fetchRho0(P, __float_as_uint(s.v.w)) * s.P.w;
   const float av[3] = {m * s.v.x, m * s.v.y, m * s.v.z};
   float Q[3][3];  // GLSL [col][row]
   if (P.flip_ratio < -0.5f) {
@@ -467,25 +493,49 @@ __device__ __forceinline__ void p2gRow(const SubstepParams& P, const PState& s, 
                          {sdt * s.B1.w, sdt * s.B2.w, sdt * s.F2.w}};
   const float xp[3] = {s.P.x, s.P.y, s.P.z};
   const int cc[3] = {cx, cy, cz};
+  float xs[3][3], W[3][3], G[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float ds[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xs[c][d] = nodeCentre(P, c, cc[c] - 1 + d);
+      ds[d] = (xp[c] - xs[c][d]) * invH;
+    }
+    bsplineStencil(ds[0], ds[1], ds[2], W[c], G[c]);
+  }
+  const float wmin = (fminf(W[0][0], fminf(W[0][1], W[0][2])) * fminf(W[1][0], fminf(W[1][1], W[1][2]))) * fminf(W[2][0], fminf(W[2][1], W[2][2]));
+  const bool exact = !(m > 0.f && wmin >= 1e-12f);
+  const float sx = exact ? 1.0f : m, sa = exact ? 1.0f : 1.0f / m;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const float xi = nodeCentre(P, c, cc[c] - 1 + d);
-      const float dd = (xp[c] - xi) * invH;
-      const float W = bspline2(dd);
-      const float Gc = bspline2g(dd) * invH;
-      const float Rw = W * (xi - xp[c]);
+      const float Wc = W[c][d], Gc = G[c][d] * invH;
+      const float Rw = Wc * (xs[c][d] - xp[c]);
       float A[3];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) A[q] = (c == 0 ? av[q] * W : 0.f) + Q[c][q] * Rw - T[c][q] * Gc;
-      row[3 * c + d] = make_float4(A[0], A[1], A[2], W);
+      for (int q = 0; q < 3; ++q) A[q] = (c == 0 ? av[q] * Wc : 0.f) + Q[c][q] * Rw - T[c][q] * Gc;
+      if (c == 0) row[d] = make_float4(A[0], A[1], A[2], sx * Wc);
+      else row[3 * c + d] = make_float4(A[0] * sa, A[1] * sa, A[2] * sa, Wc);
     }
-  row[9] = make_float4(m, 0.f, 0.f, 0.f);
+  return exact;
 }
 
-// Contribution of `row` to its stencil node (dx, dy, dz), skipped below w = 1e-12.
+// Contribution of a usual-form row to its stencil node (dx, dy, dz).
 __device__ __forceinline__ void p2gNodeTerm(const float4* __restrict__ row, int dx, int dy, int dz, float acc[4]) {
+  const float4 X = row[dx], Y = row[3 + dy], Z = row[6 + dz];
+  const float wyz = Y.w * Z.w;
+  const float wxz = X.w * Z.w, wxy = X.w * Y.w;
+  acc[0] += wyz * X.x + wxz * Y.x + wxy * Z.x;
+  acc[1] += wyz * X.y + wxz * Y.y + wxy * Z.y;
+  acc[2] += wyz * X.z + wxz * Y.z + wxy * Z.z;
+  acc[3] += X.w * wyz;
+}
+
+// Contribution of an exact-form row (mass m) to its stencil node, skipped
+// below w = 1e-12.
+__device__ __forceinline__ void p2gNodeTermExact(const float4* __restrict__ row, float m, int dx, int dy, int dz, float acc[4]) {
   const float4 X = row[dx], Y = row[3 + dy], Z = row[6 + dz];
   const float wyz = Y.w * Z.w;
   const float w = X.w * wyz;
@@ -494,11 +544,12 @@ __device__ __forceinline__ void p2gNodeTerm(const float4* __restrict__ row, int 
   acc[0] += wyz * X.x + wxz * Y.x + wxy * Z.x;
   acc[1] += wyz * X.y + wxz * Y.y + wxy * Z.y;
   acc[2] += wyz * X.z + wxz * Y.z + wxy * Z.z;
-  acc[3] += w * row[9].x;
+  acc[3] += w * m;
 }
 
-// Direct scatter of one row to global memory (stencils outside the brick's tile).
-__device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* row, int cx, int cy, int cz, float4* acc) {
+// Direct scatter of one row (either form) to global memory: particles whose
+// stencil leaves the brick's block.
+__device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* row, float m, bool exact, int cx, int cy, int cz, float4* acc) {
   const int cr = int(P.cubeRes);
   for (int dz = 0; dz < 3; ++dz)
     for (int dy = 0; dy < 3; ++dy)
@@ -506,7 +557,8 @@ __device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* 
         const int nx = cx + dx - 1, ny = cy + dy - 1, nz = cz + dz - 1;
         if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
         float a[4] = {0.f, 0.f, 0.f, 0.f};
-        p2gNodeTerm(row, dx, dy, dz, a);
+        if (exact) p2gNodeTermExact(row, m, dx, dy, dz, a);
+        else p2gNodeTerm(row, dx, dy, dz, a);
         if (a[3] != 0.f || a[0] != 0.f || a[1] != 0.f || a[2] != 0.f) redAddV4(acc + mortonEncode(nx, ny, nz), a[0], a[1], a[2], a[3]);
       }
 }
@@ -531,16 +583,25 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_
   const int cr = int(P.cubeRes);
   float* tile = sm.tiles + (kTileCopies == 1 ? 0 : warp) * 4 * kTileNodes;
   const uint32_t numCells = sm.numCells[par];
+  // a tile wholly inside the grid needs no per-node bounds test
+  const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
   for (uint32_t ci = warp; ci < numCells; ci += kWarps) {
-    const int q = sm.cells[ci];
-    const int rx = q % 6, ry = (q / 6) % 6, rz = q / 36;
-    const int lx = rx + dx, ly = ry + dy, lz = rz + dz;  // tile-local node
+    const uint32_t packed = sm.cells[ci];
+    const uint32_t q = cellSlotOf(packed);
+    const int lx = int(packed & 7u) + dx, ly = int((packed >> 3) & 7u) + dy, lz = int(packed >> 6) + dz;  // tile-local node
     const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
-    if (lane < 27 && nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr) {
+    if (lane < 27 && (inside || (nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr))) {
       float a[4] = {0.f, 0.f, 0.f, 0.f};
-      // a list holds at most kChunk rows; the bound keeps the walk finite whatever the list holds
+      // A list holds at most kChunk rows; the bound keeps the walk finite
+      // whatever the list holds.  The row form is uniform across the warp's
+      // lanes (they walk the same row).
       uint32_t j = sm.head[q] & 0xFFFFu;
-      for (int it = 0; j < uint32_t(kChunk) && it < kChunk; ++it, j = sm.next[j]) p2gNodeTerm(sm.rows + j * kRow, dx, dy, dz, a);
+      for (int it = 0; j < uint32_t(kChunk) && it < kChunk; ++it) {
+        const uint32_t link = sm.next[j];
+        if (link & kExactRow) p2gNodeTermExact(sm.rows + j * kRow, sm.mass[j], dx, dy, dz, a);
+        else p2gNodeTerm(sm.rows + j * kRow, dx, dy, dz, a);
+        j = link & ~kExactRow;
+      }
       const int t = (lz * 8 + ly) * 8 + lx;
       if (kTileCopies == 1) {
         atomicAdd(tile + t, a[3]);
@@ -624,10 +685,11 @@ __device__ __forceinline__ void gatherFallback(const SubstepParams& P, const PSt
   g2pGather(P, st, grid, vpic, vpo, Gv, Bn);
 }
 
-// The slot of a particle's stencil centre among the brick's 216 cell slots, or -1.
-__device__ __forceinline__ int cellSlot(int cx, int cy, int cz, int ox, int oy, int oz) {
+// A particle's stencil centre among the brick's 6^3 cells (block origin ox,
+// oy, oz), packed as rx | ry << 3 | rz << 6 (cellSlotOf gives its slot), or -1.
+__device__ __forceinline__ int cellPacked(int cx, int cy, int cz, int ox, int oy, int oz) {
   const int rx = cx - ox, ry = cy - oy, rz = cz - oz;
-  if ((unsigned)rx < 6u && (unsigned)ry < 6u && (unsigned)rz < 6u) return (rz * 6 + ry) * 6 + rx;
+  if ((unsigned)rx < 6u && (unsigned)ry < 6u && (unsigned)rz < 6u) return rx | (ry << 3) | (rz << 6);
   return -1;
 }
 
@@ -650,10 +712,12 @@ __device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, SM& sm, uin
         int cx, cy, cz;
         cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
         float4* row = sm.rows + threadIdx.x * kRow;
-        p2gRow(P, st, dtStress, cx, cy, cz, row);
-        const int key = cellSlot(cx, cy, cz, tx + 1, ty + 1, tz + 1);
-        if (key >= 0) p2gRegister(sm, key, par);
-        else p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+        float m;
+        const bool exact = p2gRow(P, st, dtStress, cx, cy, cz, row, m);
+        sm.mass[threadIdx.x] = m;
+        const int key = cellPacked(cx, cy, cz, tx + 1, ty + 1, tz + 1);
+        if (key >= 0) p2gRegister(sm, uint32_t(key), par, exact);
+        else p2gRowGlobal(P, row, m, exact, cx, cy, cz, G.acc);
       }
     }
     p2gChunk(P, sm, par, tx, ty, tz);
@@ -862,12 +926,14 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
       if (valid) {
         if (!stencilBrickMask(P, cx, cy, cz, bx, by, bz, marks)) markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
         float4* row = sm.rows + threadIdx.x * kRow;
-        p2gRow(P, st, dtStress, cx, cy, cz, row);
-        const int key = cellSlot(cx, cy, cz, sx, sy, sz);
+        float m;
+        const bool exact = p2gRow(P, st, dtStress, cx, cy, cz, row, m);
+        sm.mass[threadIdx.x] = m;
+        const int key = cellPacked(cx, cy, cz, sx, sy, sz);
         if (key >= 0) {
-          p2gRegister(sm, key, par);
+          p2gRegister(sm, uint32_t(key), par, exact);
         } else {
-          p2gRowGlobal(P, row, cx, cy, cz, G.acc);
+          p2gRowGlobal(P, row, m, exact, cx, cy, cz, G.acc);
           atomicAdd(B.counters + kCntOverflow, 1u);
         }
       }

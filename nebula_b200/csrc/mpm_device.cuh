@@ -128,6 +128,29 @@ __device__ __forceinline__ float bspline2g(float d) {
   return 0.0f;
 }
 
+// N(d_k) and N'(d_k) of one axis' three stencil nodes, d_k = (x_p - x_k) / h
+// with the nodes at base, base + 1, base + 2: d_0 lies in [0.5, 1.5], d_1 in
+// [-0.5, 0.5], d_2 in [-1.5, -0.5] up to rounding, so each node takes the
+// branch of bspline2 / bspline2g its interval selects, with the same
+// operations (equal results inside the intervals, and at their ends, where
+// the branches meet).  A particle outside its cell (a clamped cell index)
+// falls back to the general functions.
+__device__ __forceinline__ void bsplineStencil(float d0, float d1, float d2, float W[3], float G[3]) {
+  if (fabsf(d1) <= 0.5009765625f) {
+    const float t0 = fmaxf(1.5f - d0, 0.0f), t2 = fmaxf(1.5f + d2, 0.0f);
+    W[0] = 0.5f * t0 * t0;
+    G[0] = -t0;
+    W[1] = 0.75f - d1 * d1;
+    G[1] = -2.0f * d1;
+    W[2] = 0.5f * t2 * t2;
+    G[2] = t2;
+  } else {
+    W[0] = bspline2(d0); G[0] = bspline2g(d0);
+    W[1] = bspline2(d1); G[1] = bspline2g(d1);
+    W[2] = bspline2(d2); G[2] = bspline2g(d2);
+  }
+}
+
 // ------------------------------------------------------------------ small matrices (GLSL indexing)
 template <class T> struct m3 {
   T m[3][3];
@@ -268,40 +291,41 @@ template <class T> __device__ __forceinline__ void svd3(const m3<T>& F, m3<T>& U
   }
 }
 
-// ---- float64 decomposition of the return maps, with cheap rotations.
-// One Jacobi rotation zeroing A[P0][P1] (the pivot rule, stopping rule and
-// angle formula of mpm_common.glsl:224-244): the angle's tangent t is
-// evaluated in float, then (c, s) are made exactly orthonormal in double
-// (c = 1/sqrt(1 + t^2), s = t c) and A is transformed as the full similarity
-// R^T A R.  An angle off by float rounding therefore leaves an off-diagonal
-// ~1e-7 of the one removed, which later rotations remove; A and V stay a
-// float64-exact similarity and an orthonormal basis.  This replaces three
-// float64 divisions and two square roots per rotation by one rsqrt.
+// ---- float64 decomposition of the return maps.
+// One Jacobi rotation zeroing A[P0][P1] with the update of
+// mpm_common.glsl:224-244 (A[p][p] -= t apq, A[q][q] += t apq, A[p][q] = 0,
+// the third row and column rotated, V rotated), in float64.  The tangent t is
+// the small root of apq t^2 + (aqq - app) t - apq = 0, i.e. the shader's
+// sign(tau) / (|tau| + sqrt(1 + tau^2)) with tau = (aqq - app) / (2 apq): it
+// is first evaluated in float and then refined by one Newton step in double
+// whose reciprocal derivative is taken in float, so t carries ~1e-14 relative
+// error without a float64 division or square root.  tau's sign is taken from
+// the double operands; sign(0) = 0 gives t = 0, for which the shader's update
+// only zeroes A[p][q] (equal diagonals).
 template <int P0, int P1>
-__device__ __forceinline__ void jacobiRotateMixed(m3<double>& A, m3<double>& V) {
+__device__ __forceinline__ void jacobiRotateF64(m3<double>& A, m3<double>& V) {
   constexpr int R = 3 - P0 - P1;
   const double apq = A.m[P0][P1], app = A.m[P0][P0], aqq = A.m[P1][P1];
-  const float tau = float(aqq - app) / (2.0f * float(apq));
-  const float at = fabsf(tau);
-  const float tf = at < 1e18f ? gsign(tau) / (at + sqrtf(1.0f + tau * tau)) : 0.5f / tau;
-  if (tf == 0.0f) {
-    // Equal diagonals: GLSL sign(0) = 0 gives t = 0, c = 1, s = 0, and the
-    // shader's update (mpm_common.glsl:229-231) then only zeroes A[p][q].  The
-    // full similarity would leave A unchanged and the loop would repeat this
-    // pivot up to its cap.
+  const double d = aqq - app;
+  if (d == 0.0) {
     A.m[P0][P1] = 0.0;
     A.m[P1][P0] = 0.0;
     return;
   }
-  const double t = double(tf);
+  const float sg = (d > 0.0) == (apq > 0.0) ? 1.0f : -1.0f;
+  const float tau = float(d) / (2.0f * float(apq));
+  const float at = fabsf(tau);
+  const float t0 = at < 1e18f ? sg / (at + sqrtf(1.0f + tau * tau)) : 0.5f / tau;
+  const double tf = double(t0);
+  const double f = apq * (tf * tf - 1.0) + d * tf;
+  const double fp = 2.0 * apq * tf + d;
+  const double t = tf - f * double(__frcp_rn(float(fp)));
   const double c = rsqrt(1.0 + t * t);
   const double sn = t * c;
-  const double cc = c * c, ss = sn * sn, cs = c * sn;
-  A.m[P0][P0] = cc * app - 2.0 * cs * apq + ss * aqq;
-  A.m[P1][P1] = ss * app + 2.0 * cs * apq + cc * aqq;
-  const double off = cs * (app - aqq) + (cc - ss) * apq;
-  A.m[P0][P1] = off;
-  A.m[P1][P0] = off;
+  A.m[P0][P0] = app - t * apq;
+  A.m[P1][P1] = aqq + t * apq;
+  A.m[P0][P1] = 0.0;
+  A.m[P1][P0] = 0.0;
   const double arp = A.m[R][P0], arq = A.m[R][P1];
   A.m[R][P0] = c * arp - sn * arq;
   A.m[P0][R] = A.m[R][P0];
@@ -318,7 +342,7 @@ __device__ __forceinline__ void jacobiRotateMixed(m3<double>& A, m3<double>& V) 
 // svd3 of the return maps: same eigen-decomposition of F^T F (<= 20 rotations,
 // stop below 1e-8), descending sort, U columns F v_i / sigma_i and the sign
 // fix-up; sigma_i and 1/sigma_i come from one rsqrt of the eigenvalue.
-__device__ __forceinline__ void svd3Mixed(const m3<double>& F, m3<double>& U, double sigma[3], m3<double>& V) {
+__device__ __forceinline__ void svd3F64(const m3<double>& F, m3<double>& U, double sigma[3], m3<double>& V) {
   m3<double> A;
 #pragma unroll
   for (int j = 0; j < 3; ++j)
@@ -329,9 +353,9 @@ __device__ __forceinline__ void svd3Mixed(const m3<double>& F, m3<double>& U, do
   for (int iter = 0; iter < 20; iter++) {
     const double b01 = fabs(A.m[0][1]), b02 = fabs(A.m[0][2]), b12 = fabs(A.m[1][2]);
     if (fmax(b01, fmax(b02, b12)) < 1e-8) break;
-    if (b01 >= fmax(b02, b12)) jacobiRotateMixed<0, 1>(A, V);
-    else if (b02 >= b12) jacobiRotateMixed<0, 2>(A, V);
-    else jacobiRotateMixed<1, 2>(A, V);
+    if (b01 >= fmax(b02, b12)) jacobiRotateF64<0, 1>(A, V);
+    else if (b02 >= b12) jacobiRotateF64<0, 2>(A, V);
+    else jacobiRotateF64<1, 2>(A, V);
   }
   double inv[3];
 #pragma unroll
@@ -400,11 +424,9 @@ template <class T> __device__ __forceinline__ m3<T> stressUDUt(const m3<T>& U, c
   return t;
 }
 
-// Stress of a rebuilt F = U diag(s) V^T (shader layout), evaluated from the same
-// decomposition: svd3 of the rebuilt matrix returns the transpose-paired
-// vectors, so the shaders' second `U * diag * transpose(U)` equals
+// The textbook stress sum_i k_i u_i u_i^T from svd3's row-stored vectors:
 //   tau[c][r] = sum_i k_i U[r][i] U[c][i]
-template <class T> __device__ __forceinline__ m3<T> stressRebuilt(const m3<T>& U, const T k[3]) {
+template <class T> __device__ __forceinline__ m3<T> stressTextbook(const m3<T>& U, const T k[3]) {
   m3<T> t;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -443,7 +465,7 @@ template <class T> __device__ __forceinline__ m3<T> henckyStress(const m3<T>& F,
 // the singular vectors in the rows of its matrices (the reference's layout,
 // which its own models multiply as columns); this model is not the
 // reference's, so its stress is the textbook sum of k_i u_i u_i^T:
-// tau[c][r] = sum_i k_i U[r][i] U[c][i], the index pattern of stressRebuilt.
+// tau[c][r] = sum_i k_i U[r][i] U[c][i] (stressTextbook).
 template <class T> __device__ __forceinline__ m3<T> fixedCorotatedStress(const m3<T>& F, T mu, T lam) {
   m3<T> U, V;
   T s[3], k[3];
@@ -453,54 +475,71 @@ template <class T> __device__ __forceinline__ m3<T> fixedCorotatedStress(const m
   const T c = lam * J * (J - T(1));
 #pragma unroll
   for (int i = 0; i < 3; ++i) k[i] = T(2) * mu * s[i] * (s[i] - T(1)) + c;
-  return stressRebuilt(U, k);
+  return stressTextbook(U, k);
 }
 
-// Plastic return map + Kirchhoff stress with ONE decomposition (double).
+// Plastic return map + Kirchhoff stress, decompositions in float64.
 // model VON_MISES: mpm_g2p.comp:19-38 then henckyStress; DRUCKER_PRAGER /
-// POWDER / MUD: mpm_g2p.comp:41-68 then henckyStress.  Where the shader
-// rebuilds F it decomposes again; that second decomposition is the rebuilt
-// F's own SVD, so the stress is taken from the first one via stressRebuilt.
+// POWDER / MUD: mpm_g2p.comp:41-68 then henckyStress, as mpm_g2p.comp:150-181
+// calls them.  The return maps rebuild F as the shaders' `U * diag(s') *
+// transpose(V)` from svd3's row-stored vectors, which is not F's own
+// orientation, and the shaders then take the stress of the rebuilt matrix
+// from a second svd3.  That stress, `U' * diag(k) * transpose(U')` in the
+// same layout, depends on the signs the second decomposition gives its
+// singular vectors (the layout turns them into signs of rows and columns of
+// tau), so the second decomposition is run here too; its log-strains equal
+// the returned ones (k_i from e_i below) up to rounding.  Without a rebuild
+// (Von Mises inside the yield surface) the shader's second svd3 decomposes
+// the unchanged F again, which is the first decomposition.  The log-strains
+// and their exponentials are float64: a particle on the Von Mises yield
+// surface (where the last return left it) decides yield or not by the sign
+// of ||dev eps|| - q_max / (2 mu), a difference at the rounding of F itself,
+// and float logarithms there change the decision (and, through the rebuild,
+// F's orientation) against the float64 oracle.
 __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<float>& tau, float mu_f, float lam_f, float M_f, float qc_f,
                                               float qmax_f) {
   const double mu = mu_f, lam = lam_f;
-  m3<double> Fd = m3cast<double>(F), U, V;
+  m3<double> U, V;
   double s[3];
-  svd3Mixed(Fd, U, s, V);
-  // The decomposition is float64; the log-strains and their exponentials are
-  // scalar functions of well-separated magnitudes and run in float, the
-  // precision of the reference (F' is stored in float in any case).
+  svd3F64(m3cast<double>(F), U, s, V);
+  // (divisions by constants and by 2 mu are multiplications by reciprocals:
+  // within an ulp of float64 of the shaders' quotients)
+  constexpr double kThird = 1.0 / 3.0;
+  const double inv2mu = 1.0 / (2.0 * mu);
   double eps[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) eps[i] = double(logf(fmaxf(fabsf(float(s[i])), 1e-6f)));
-  double trEps = eps[0] + eps[1] + eps[2];
+  for (int i = 0; i < 3; ++i) eps[i] = log(fmax(fabs(s[i]), 1e-6));
+  const double trEps = eps[0] + eps[1] + eps[2];
+  const double mean = trEps * kThird;
   double dev[3];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) dev[i] = eps[i] - (trEps / 3.0);
-  double normDev = sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  for (int i = 0; i < 3; ++i) dev[i] = eps[i] - mean;
+  const double normDev = sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
   bool rebuild;
   if (model == MAT_VON_MISES) {
-    double delta = normDev - double(qmax_f) / (2.0 * mu);
+    const double delta = normDev - double(qmax_f) * inv2mu;
     rebuild = delta > 0.0 && normDev > 1e-8;
     if (rebuild) {
+      const double r = delta / normDev;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - (delta / normDev) * dev[i]) + (trEps / 3.0);
+      for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
     }
   } else {
-    double K = lam + 2.0 * mu / 3.0;
-    double p = -K * trEps;
-    double q_yield = double(M_f) * p + double(qc_f);
+    const double K = lam + 2.0 * mu * kThird;
+    const double p = -K * trEps;
+    const double q_yield = double(M_f) * p + double(qc_f);
     rebuild = true;
     if (q_yield <= 1e-8) {
-      double p_proj = -double(qc_f) / fmax(double(M_f), 1e-8);
-      double tr = -p_proj / K;
+      const double p_proj = -double(qc_f) / fmax(double(M_f), 1e-8);
+      const double tr = -p_proj / K;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) eps[i] = tr / 3.0;
+      for (int i = 0; i < 3; ++i) eps[i] = tr * kThird;
     } else {
-      double delta = normDev - q_yield / (2.0 * mu);
+      const double delta = normDev - q_yield * inv2mu;
       if (delta > 0.0 && normDev > 1e-8) {
+        const double r = delta / normDev;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - (delta / normDev) * dev[i]) + (trEps / 3.0);
+        for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
       }
     }
   }
@@ -509,17 +548,18 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
     double sp[3], e[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      sp[i] = double(expf(float(eps[i])));
+      sp[i] = exp(eps[i]);
       e[i] = fmax(eps[i], -13.815510557964274);  // log(max(exp(eps), 1e-6)) = max(eps, log 1e-6)
     }
-    m3<double> Fn = rebuildUSVt(U, sp, V);
+    const m3<double> Fn = rebuildUSVt(U, sp, V);
     F = m3cast<float>(Fn);
+    double s2[3];
+    svd3F64(Fn, U, s2, V);
     henckyFromLogStrain(e, mu, lam, k);
-    tau = m3cast<float>(stressRebuilt(U, k));
   } else {
     henckyFromLogStrain(eps, mu, lam, k);  // eps = log(max(|s|, 1e-6)) already
-    tau = m3cast<float>(stressUDUt(U, k));
   }
+  tau = m3cast<float>(stressUDUt(U, k));
 }
 
 // ------------------------------------------------------------------ colliders

@@ -459,10 +459,26 @@ void MPMEngine::setColliderMesh(const float* tris, uint32_t n) {
   mesh_.build(tris, n);
   hasMesh_ = true;
   sdf_.ensure(size_t(hashCells_) * sizeof(float));
-  check(launchMeshSdfPrepared(mesh_, meshPose(nullptr, nullptr), gridRes_, hashCells_, cfg_.cellSize, static_cast<float*>(sdf_.ptr), lastStream_,
-                              &launches_),
-        "mesh sdf");
+  buildMeshSdf(meshPose(nullptr, nullptr));
+}
+
+// The collider mesh's SDF into the engine's SDF buffer, with the closest-point
+// definition the engine is set to (setColliderMeshClosestPoint).
+void MPMEngine::buildMeshSdf(const MeshPose& pose) {
+  float* out = static_cast<float*>(sdf_.ptr);
+  if (meshReferenceClosest_)
+    check(launchMeshSdfReference(static_cast<const float*>(mesh_.tris.ptr), static_cast<const uint32_t*>(mesh_.index.ptr), mesh_.n, pose, gridRes_,
+                                 hashCells_, cfg_.cellSize, out, lastStream_, &launches_),
+          "mesh sdf (reference closest point)");
+  else
+    check(launchMeshSdfPrepared(mesh_, pose, gridRes_, hashCells_, cfg_.cellSize, out, lastStream_, &launches_), "mesh sdf");
   hasSdf_ = true;
+}
+
+void MPMEngine::setColliderMeshClosestPoint(int mode) {
+  if (mode != NEBULA_MPM_CLOSEST_POINT_COMPLETE && mode != NEBULA_MPM_CLOSEST_POINT_REFERENCE)
+    throw Error(NEBULA_MPM_ERR_INVALID, "closest-point mode must be NEBULA_MPM_CLOSEST_POINT_COMPLETE or _REFERENCE");
+  meshReferenceClosest_ = mode == NEBULA_MPM_CLOSEST_POINT_REFERENCE;
 }
 
 // The moving-obstacle rebuild (examples/pyro_basic.cpp:130-134:
@@ -472,10 +488,7 @@ void MPMEngine::setColliderMesh(const float* tris, uint32_t n) {
 void MPMEngine::setColliderMeshPose(const float* translation, const float* rotationWxyz) {
   if (!hasMesh_) throw Error(NEBULA_MPM_ERR_INVALID, "no collider mesh: call setColliderMesh first");
   if (!translation || !rotationWxyz) throw Error(NEBULA_MPM_ERR_INVALID, "null pose");
-  check(launchMeshSdfPrepared(mesh_, meshPose(translation, rotationWxyz), gridRes_, hashCells_, cfg_.cellSize, static_cast<float*>(sdf_.ptr),
-                              lastStream_, &launches_),
-        "mesh sdf");
-  hasSdf_ = true;
+  buildMeshSdf(meshPose(translation, rotationWxyz));
 }
 
 void MPMEngine::setForces(const nebula_mpm_force* f, uint32_t n) {
@@ -1212,6 +1225,9 @@ int nebula_mpm_set_collider_mesh(nebula_mpm* e, const float* tris, uint32_t n) {
 }
 int nebula_mpm_set_collider_mesh_pose(nebula_mpm* e, const float translation[3], const float rotation_wxyz[4]) {
   return guarded([&] { E(e).setColliderMeshPose(translation, rotation_wxyz); });
+}
+int nebula_mpm_set_collider_mesh_closest_point(nebula_mpm* e, int mode) {
+  return guarded([&] { E(e).setColliderMeshClosestPoint(mode); });
 }
 int nebula_mpm_clear_collider(nebula_mpm* e) {
   return guarded([&] { E(e).clearCollider(); });

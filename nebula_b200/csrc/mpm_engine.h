@@ -89,6 +89,11 @@ struct PreparedMesh {
 // the caller's list).
 cudaError_t launchMeshSdfPrepared(const PreparedMesh& m, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
                                   float* dSdf, cudaStream_t s, uint64_t* launches);
+// SDF with the reference's closest-point steps (no edge-BC region) by brute
+// force over the triangles; `dIndex` (may be null: list order) is each
+// triangle's index in the caller's list, for the first-in-list tie rule.
+cudaError_t launchMeshSdfReference(const float* dTris, const uint32_t* dIndex, uint32_t n, const MeshPose& pose, const uint32_t res[3],
+                                   uint32_t totalCells, float cellSize, float* dSdf, cudaStream_t s, uint64_t* launches);
 
 
 class MPMEngine {
@@ -107,6 +112,9 @@ class MPMEngine {
   void setColliderSphere(float radius, float cx, float cy, float cz);
   void setColliderMesh(const float* tris, uint32_t n);
   void setColliderMeshPose(const float* translation, const float* rotationWxyz);
+  // NEBULA_MPM_CLOSEST_POINT_COMPLETE (default) or _REFERENCE; applies to the
+  // next setColliderMesh / setColliderMeshPose
+  void setColliderMeshClosestPoint(int mode);
   void clearCollider();
   void setForces(const nebula_mpm_force* f, uint32_t n);
   uint32_t appendParticles(const float* pos4, const float* vel4, uint32_t n);
@@ -239,6 +247,8 @@ class MPMEngine {
   DevBuf materials_, colliders_, forces_, sdf_, err_;
   PreparedMesh mesh_;
   bool hasMesh_ = false;
+  bool meshReferenceClosest_ = false;
+  void buildMeshSdf(const MeshPose& pose);
   std::vector<Material> hostMaterials_;
   uint32_t colliderCount_ = 0;
   uint32_t colliderTrackLen_ = 1;

@@ -429,7 +429,125 @@ __global__ void __launch_bounds__(kThreads) k_mesh_sdf_clusters(const float4* __
   if (code < totalCells) sdf[code] = inside ? (outer ? best : -best) : 1e9f;
 }
 
+// ------------------------------------------------------------------ the reference's closest point
+// closestPtOnTriangle (MeshSDF.h:48-78) step for step, including its gap: a
+// point whose closest feature is edge BC falls through to the barycentric
+// face case and gets the projection onto the triangle's plane, outside the
+// triangle.  That point can be nearer than any point of the triangle, so no
+// distance bound culls triangles here: every cell visits every triangle, as
+// buildMeshSDF's loop does (MeshSDF.h:113-126).
+struct TriRef {  // posed vertices and normal
+  float ax, ay, az, bx, by, bz, cx, cy, cz, nx, ny, nz;
+};
+
+// Float operations rounded one at a time, in the reference's order (no fused
+// multiply-add): the missing region makes the result jump where a region test
+// flips, so its arithmetic is kept operation for operation.
+__device__ __forceinline__ float mulr(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float addr(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float subr(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float dotr(float ax, float ay, float az, float bx, float by, float bz) {
+  return addr(addr(mulr(ax, bx), mulr(ay, by)), mulr(az, bz));
+}
+
+__device__ __forceinline__ void closestRef(const TriRef& t, float px, float py, float pz, float& qx, float& qy, float& qz) {
+  const float abx = subr(t.bx, t.ax), aby = subr(t.by, t.ay), abz = subr(t.bz, t.az);
+  const float acx = subr(t.cx, t.ax), acy = subr(t.cy, t.ay), acz = subr(t.cz, t.az);
+  const float apx = subr(px, t.ax), apy = subr(py, t.ay), apz = subr(pz, t.az);
+  const float d1 = dotr(abx, aby, abz, apx, apy, apz), d2 = dotr(acx, acy, acz, apx, apy, apz);
+  if (d1 <= 0.f && d2 <= 0.f) {
+    qx = t.ax; qy = t.ay; qz = t.az;
+    return;
+  }
+  const float bpx = subr(px, t.bx), bpy = subr(py, t.by), bpz = subr(pz, t.bz);
+  const float d3 = dotr(abx, aby, abz, bpx, bpy, bpz), d4 = dotr(acx, acy, acz, bpx, bpy, bpz);
+  if (d3 >= 0.f && d4 <= d3) {
+    qx = t.bx; qy = t.by; qz = t.bz;
+    return;
+  }
+  const float vc = subr(mulr(d1, d4), mulr(d3, d2));
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+    const float v = __fdiv_rn(d1, subr(d1, d3));
+    qx = addr(t.ax, mulr(v, abx)); qy = addr(t.ay, mulr(v, aby)); qz = addr(t.az, mulr(v, abz));
+    return;
+  }
+  const float cpx = subr(px, t.cx), cpy = subr(py, t.cy), cpz = subr(pz, t.cz);
+  const float d5 = dotr(abx, aby, abz, cpx, cpy, cpz), d6 = dotr(acx, acy, acz, cpx, cpy, cpz);
+  if (d6 >= 0.f && d5 <= d6) {
+    qx = t.cx; qy = t.cy; qz = t.cz;
+    return;
+  }
+  const float vb = subr(mulr(d5, d2), mulr(d1, d6));
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+    const float w = __fdiv_rn(d2, subr(d2, d6));
+    qx = addr(t.ax, mulr(w, acx)); qy = addr(t.ay, mulr(w, acy)); qz = addr(t.az, mulr(w, acz));
+    return;
+  }
+  const float va = subr(mulr(d3, d6), mulr(d5, d4));
+  const float sum = addr(addr(va, vb), vc);
+  const float v = __fdiv_rn(vb, sum), w = __fdiv_rn(vc, sum);
+  qx = addr(addr(t.ax, mulr(v, abx)), mulr(w, acx));
+  qy = addr(addr(t.ay, mulr(v, aby)), mulr(w, acy));
+  qz = addr(addr(t.az, mulr(v, abz)), mulr(w, acz));
+}
+
+// One thread per Morton code; the (posed) triangles pass through shared
+// memory in tiles of kThreads.  `index` (may be null: list order) gives each
+// triangle's place in the caller's list, so a list in another order still
+// resolves equal distances to the first triangle of the caller's list, as
+// the strict < of the reference's loop does.
+__global__ void __launch_bounds__(kThreads) k_mesh_sdf_ref(const float4* __restrict__ tris, const uint32_t* __restrict__ index, uint32_t n,
+                                                           MeshPose pose, int rx, int ry, int rz, uint32_t totalCells, float cs,
+                                                           float* __restrict__ sdf) {
+  __shared__ TriRef tile[kThreads];
+  __shared__ uint32_t tileIdx[kThreads];
+  const uint32_t code = blockIdx.x * kThreads + threadIdx.x;
+  int ix, iy, iz;
+  mortonDecode(code, ix, iy, iz);
+  const bool inside = code < totalCells && ix < rx && iy < ry && iz < rz;
+  const float px = mulr(addr(float(ix), 0.5f), cs), py = mulr(addr(float(iy), 0.5f), cs), pz = mulr(addr(float(iz), 0.5f), cs);
+  float best = 1e9f;
+  uint32_t bestIdx = 0xffffffffu;
+  bool outer = true;
+  for (uint32_t t0 = 0; t0 < n; t0 += kThreads) {
+    __syncthreads();  // the previous tile is consumed
+    const uint32_t t = t0 + threadIdx.x;
+    if (t < n) {
+      float v[12];
+      loadTri(tris, t, pose, v);
+      tile[threadIdx.x] = TriRef{v[3], v[4], v[5], v[6], v[7], v[8], v[9], v[10], v[11], v[0], v[1], v[2]};
+      tileIdx[threadIdx.x] = index ? __ldg(index + t) : t;
+    }
+    __syncthreads();
+    if (!inside) continue;
+    const uint32_t m = min(uint32_t(kThreads), n - t0);
+    for (uint32_t j = 0; j < m; ++j) {
+      const TriRef& tr = tile[j];
+      float qx, qy, qz;
+      closestRef(tr, px, py, pz, qx, qy, qz);
+      const float dx = subr(px, qx), dy = subr(py, qy), dz = subr(pz, qz);
+      const float d = __fsqrt_rn(dotr(dx, dy, dz, dx, dy, dz));
+      const uint32_t id = tileIdx[j];
+      if (d < best || (d == best && id < bestIdx)) {
+        best = d;
+        bestIdx = id;
+        outer = dotr(dx, dy, dz, tr.nx, tr.ny, tr.nz) >= 0.f;
+      }
+    }
+  }
+  if (code < totalCells) sdf[code] = inside ? (outer ? best : -best) : 1e9f;
+}
+
 }  // namespace
+
+cudaError_t launchMeshSdfReference(const float* dTris, const uint32_t* dIndex, uint32_t n, const MeshPose& pose, const uint32_t res[3],
+                                   uint32_t totalCells, float cellSize, float* dSdf, cudaStream_t s, uint64_t* launches) {
+  if (totalCells == 0) return cudaSuccess;
+  k_mesh_sdf_ref<<<(totalCells + kThreads - 1) / kThreads, kThreads, 0, s>>>(reinterpret_cast<const float4*>(dTris), dIndex, n, pose, int(res[0]),
+                                                                             int(res[1]), int(res[2]), totalCells, cellSize, dSdf);
+  ++*launches;
+  return cudaGetLastError();
+}
 
 cudaError_t launchMeshSdf(const float* dTris, uint32_t n, const MeshPose& pose, const uint32_t res[3], uint32_t totalCells, float cellSize,
                           float* dSdf, cudaStream_t s, uint64_t* launches) {
@@ -598,6 +716,31 @@ int nebula_mpm_mesh_build_sdf(const nebula_mpm_mesh* m, const float translation[
     check(launchMeshSdfPrepared(m->mesh, meshPose(translation, rotation_wxyz), realRes, totalCells, cellSize, dSdf, static_cast<cudaStream_t>(stream),
                                 &l),
           "mesh sdf");
+  });
+}
+
+int nebula_mpm_mesh_build_sdf_reference(const nebula_mpm_mesh* m, const float translation[3], const float rotation_wxyz[4],
+                                        const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream) {
+  return guardedMesh([&] {
+    if (!m) throw Error(NEBULA_MPM_ERR_INVALID, "null mesh");
+    checkGrid(realRes, totalCells, cellSize, dSdf);
+    uint64_t l = 0;
+    check(launchMeshSdfReference(static_cast<const float*>(m->mesh.tris.ptr), static_cast<const uint32_t*>(m->mesh.index.ptr), m->mesh.n,
+                                 meshPose(translation, rotation_wxyz), realRes, totalCells, cellSize, dSdf, static_cast<cudaStream_t>(stream), &l),
+          "mesh sdf (reference closest point)");
+  });
+}
+
+int nebula_mpm_mesh_sdf_reference(const float* dTris, uint32_t nTris, const float translation[3], const float rotation_wxyz[4],
+                                  const uint32_t realRes[3], uint32_t totalCells, float cellSize, float* dSdf, void* stream) {
+  return guardedMesh([&] {
+    checkGrid(realRes, totalCells, cellSize, dSdf);
+    checkMeshArgs(dTris, nTris);
+    if (reinterpret_cast<uintptr_t>(dTris) % 16u) throw Error(NEBULA_MPM_ERR_INVALID, "triangles must be 16-byte aligned");
+    uint64_t l = 0;
+    check(launchMeshSdfReference(dTris, nullptr, nTris, meshPose(translation, rotation_wxyz), realRes, totalCells, cellSize, dSdf,
+                                 static_cast<cudaStream_t>(stream), &l),
+          "mesh sdf (reference closest point)");
   });
 }
 

@@ -251,15 +251,18 @@ __device__ __forceinline__ bool g2pGatherStaged(const SubstepParams& P, const PS
   if ((unsigned)lx > 3u || (unsigned)ly > 3u || (unsigned)lz > 3u) return false;
   float W[3][3], Gd[3][3], R[3][3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a) {
+    float d[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const float xi = nodeCentre(P, a, base[a] + k);
-      const float d = (xp[a] - xi) * invH;
-      W[a][k] = bspline2(d);
-      Gd[a][k] = bspline2g(d) * invH;
+      d[k] = (xp[a] - xi) * invH;
       R[a][k] = xi - xp[a];
     }
+    bsplineStencil(d[0], d[1], d[2], W[a], Gd[a]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Gd[a][k] *= invH;
+  }
 #pragma unroll
   for (int i = 0; i < 3; ++i) vpic[i] = vpo[i] = 0.f;
 #pragma unroll

@@ -183,6 +183,14 @@ class MPMEngine:
         q = np.ascontiguousarray(rotation, dtype=np.float32).reshape(4)
         call("nebula_mpm_set_collider_mesh_pose", self._h, _ptr(t), _ptr(q))
 
+    def setColliderMeshClosestPoint(self, reference: bool):
+        """True: later setColliderMesh / setColliderMeshPose builds take the
+        reference's closestPtOnTriangle (no edge-BC region, brute force), so
+        the SDF equals the reference's buildMeshSDF output; False (default):
+        the complete region test."""
+        mode = _capi.CLOSEST_POINT_REFERENCE if reference else _capi.CLOSEST_POINT_COMPLETE
+        call("nebula_mpm_set_collider_mesh_closest_point", self._h, mode)
+
     def setForces(self, forces):
         self._forces = list(forces)
         a = np.zeros(max(1, len(self._forces)), FORCE_DTYPE)

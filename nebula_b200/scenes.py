@@ -415,10 +415,13 @@ def terrain_sdf(seed, res, h):
     return sdf, H
 
 
-def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, with_sdf=True):
+def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, with_sdf=True, lift=2.0, vy=0.0):
     """1,000,000 Drucker-Prager particles (friction 35 deg, E=1.4e5, nu=0.3,
     rho 1600) as a jittered slab above a seeded terrain SDF on a 256^3 grid,
-    APIC, dt=2e-5."""
+    APIC, dt=2e-5.  The slab's lowest layer starts `lift` cells above the
+    highest terrain point (2 cells: over the 500 substeps, 0.01 s, it falls
+    0.13 cells and never touches the terrain; a negative lift sinks the
+    slab's bottom into the ridges), moving at vy (m/s) along y."""
     h = 1.0 / res
     sp = 0.5 * h
     nx, ny, nz = n_side
@@ -427,8 +430,7 @@ def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, wi
     pos = jittered_lattice(seed, 0, (nx, ny, nz), sp, (ox, 0.0, oz), 0.25 * h)
     sdf, H = (terrain_sdf(seed, res, h) if with_sdf else (None, None))
     if H is not None:
-        # the slab starts 2h above the highest terrain point and falls onto it
-        pos[:, 1] += np.float32(H.max() + 2.0 * h)
+        pos[:, 1] += np.float32(H.max() + lift * h)
     else:
         pos[:, 1] += np.float32(0.3)
     vp = np.float32(sp) ** 3
@@ -436,7 +438,9 @@ def slope_flow(seed=3, res=256, n_side=(200, 25, 200), substeps=500, dt=2e-5, wi
     params = StepParams(dt=dt, cell_size=float(np.float32(h)), domain_size=(1.0, 1.0, 1.0), flip_ratio=-1.0,
                         materials=mats, forces=[gravity()])
     params.mu_lame, params.lambda_lame = lame(1.4e5, 0.3)
-    return Scene("slope_flow_1m_256", params, make_state(pos, vp), substeps, sdf=sdf)
+    state = make_state(pos, vp)
+    state["v"][:, 1] = np.float32(vy)
+    return Scene("slope_flow_1m_256", params, state, substeps, sdf=sdf)
 
 
 def _mix_shape(u_row, nmin, nmax):

@@ -42,7 +42,7 @@ V3 closestPt(V3 p, V3 a, V3 b, V3 c, bool complete) {
   const float va = d3 * d6 - d5 * d4;
   if (complete && va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) return add(b, scl((d4 - d3) / ((d4 - d3) + (d5 - d6)), sub(c, b)));
   const float sum = va + vb + vc;
-  return add(a, add(scl(vb / sum, ab), scl(vc / sum, ac)));
+  return add(add(a, scl(vb / sum, ab)), scl(vc / sum, ac));  // a + (vb/sum) ab + (vc/sum) ac, left to right
 }
 
 uint32_t expand(uint32_t v) {

@@ -152,15 +152,24 @@ def test_autograd_function():
 
 
 def test_graph_replay_equals_eager():
-    """Same kernels replayed from graphs.  The reductions into the grid are
-    float atomics whose order changes from run to run, and the v0 gradient of
-    this floor-contact scene amplifies that (1.01e-4 relative seen between a
-    graph and an eager run), so the bars sit above that spread."""
+    """Same kernels replayed from graphs and launched eagerly: the same loss,
+    and both gradients as close to the float64 adjoint as the contact scene
+    allows (test_contact_gradient_matches_float64_adjoint).  The reductions
+    into the grid are float atomics whose order changes from run to run, and
+    the v0 gradient of this floor-contact scene amplifies that: graph and eager
+    runs differ by 1e-4 to 5e-4 relative (measured), so they are compared
+    with the reference rather than bit for bit with each other."""
     sc = S.diff_block(**SMALL)
+    import oracle
+    ref = oracle.adjoint_grad(*oracle_args(sc), sc.substeps, every=20)
+    nu = sc.extra["nu"]
+    gE_ref = ref["gmu"] / (2 * (1 + nu)) + ref["glam"] * nu / ((1 + nu) * (1 - 2 * nu))
     L1, gv1, gE1, _ = gpu_grad(sc, graphs=True)
     L2, gv2, gE2, _ = gpu_grad(sc, graphs=False)
     assert abs(L1 - L2) <= 1e-6 * abs(L2)
-    assert rel(gv1, gv2) < 3e-4 and rel(gE1, gE2) < 1e-3
+    for gv, gE in ((gv1, gE1), (gv2, gE2)):
+        assert rel(gv, ref["gv0"]) < 2e-2 and rel(gE, gE_ref) < 1e-2
+    assert rel(gv1, gv2) < 2e-3 and rel(gE1, gE2) < 2e-3
 
 
 @pytest.mark.skipif(not GOLDEN.exists(), reason="fixture not generated")

@@ -9,13 +9,20 @@ Bars (from the reference's own tests and the parity contract):
     ref-fp32 oracle, with the error against the fp64 oracle printed.
 
 Plastic models: the shaders rebuild F as `U * diag * transpose(V)` from svd3's
-row-stored vectors (mpm_g2p.comp:35,67), which loses det F's sign whenever the
-descending sort applies an odd permutation; near-equal singular values make
-that choice (and so F's orientation, and through later (I + dt grad v) F
-products its stresses and velocities) depend on rounding.  The reference's own
-float32 and float64 runs already disagree there.  Plastic trajectories are
-held to the 1e-4 bar on x; v, the singular values and |det| of F are printed
-with looser sanity bounds.
+row-stored vectors (mpm_g2p.comp:35,67), which is not F's own orientation and
+loses det F's sign whenever the descending sort applies an odd permutation;
+near-equal singular values (Drucker-Prager sand at the apex has three) make
+that orientation depend on rounding.  The trajectory bars are therefore stated
+per quantity as 1e-4 or three times the reference algorithm's own sensitivity,
+whichever is larger: the oracle is run again with relative noise on every P2G
+sum of every substep, of the size of the measured difference between the GPU's
+and the oracle's P2G grid (a few 1e-7: the rounding another summation order
+leaves), and the largest spread of each quantity between those runs and the
+plain one is that sensitivity.  Positions, |det F| and the singular values of F come out
+at 1e-4 for every plastic model except the singular values of
+Von Mises and VISCOPLASTIC_MUD, whose yield decisions and viscous term make
+them drift by 1e-4 and more under that noise alone; F itself is held to 1e-4
+after one substep, before the orientation ambiguity can act.
 """
 import numpy as np
 import pytest
@@ -208,10 +215,11 @@ def test_g2p_pass_elastic(flip):
 @pytest.mark.parametrize("model", [S.MAT_DRUCKER_PRAGER, S.MAT_VON_MISES, S.MAT_GRANULAR_POWDER, S.MAT_VISCOPLASTIC_MUD],
                          ids=["drucker_prager", "von_mises", "powder", "mud"])
 def test_g2p_pass_plastic(model):
-    """Plastic return maps against the oracle in the CUDA path's precision policy.
-    The rebuilt F's orientation and the post-return stress are ill-conditioned in
-    the reference algorithm (near-equal singular values); x, v, B, the singular
-    values of F and |det F| are compared."""
+    """Plastic return maps against the oracle in the CUDA path's precision
+    policy, one G2P on identical grid input from a state 20 substeps in: x,
+    v, B, the singular values of F and |det F| within 1e-5.  (F's orientation
+    and the stress follow the rounding of the gather's sums wherever singular
+    values coincide; test_return_map_on_identical_F holds them.)"""
     sc = S.shear_block(model)
     sc.state = advanced(sc, 20, mode="mixed")
     gs, os_ = g2p_one_pass(sc, "mixed")
@@ -222,6 +230,38 @@ def test_g2p_pass_plastic(model):
     print("G2P plastic %d: sigma %.2e |detF| %.2e F %.2e stress %.2e" % (model, rel_l2(sg, so), rel_l2(dg, do), rel_l2(state_F(gs), state_F(os_)),
                                                                         rel_l2(stress6(gs), stress6(os_))))
     assert rel_l2(sg, so) < 1e-5 and rel_l2(dg, do) < 1e-5
+
+
+@pytest.mark.parametrize("model", [S.MAT_DRUCKER_PRAGER, S.MAT_VON_MISES, S.MAT_GRANULAR_POWDER, S.MAT_VISCOPLASTIC_MUD],
+                         ids=["drucker_prager", "von_mises", "powder", "mud"])
+def test_return_map_on_identical_F(model):
+    """The return map and the stress alone: one G2P over a grid at rest (mass
+    1, zero momentum), so grad v = 0 and both sides apply the return map to
+    the very same F (the state 20 substeps into the shear block).  The rebuilt
+    F and its F^T F within 1e-5; the Kirchhoff stress of the second
+    decomposition (the shaders' henckyStress of the rebuilt F) within 1e-4:
+    its log-strains are the returned ones here, which the shaders recompute
+    from the second decomposition's singular values, and where two of those
+    coincide the decomposition stops with off-diagonals up to 1e-8, so the
+    recomputed ones carry ~1e-8 (4e-5 relative on the Drucker-Prager
+    stress, measured)."""
+    sc = S.shear_block(model)
+    sc.state = advanced(sc, 20, mode="mixed")
+    nc = sc.params.hash_cells
+    mom = np.zeros((2 * nc, 4), np.float32)
+    mass = np.ones(nc, np.float32)
+    o = OracleBackend(sc.params, sc.n, mode="mixed")
+    o.upload_particles(sc.state)
+    o.upload_grid(mom, mass)
+    o.g2p()
+    g = GpuBackend(sc.params, sc.n)
+    g.upload_particles(sc.state)
+    g.upload_grid(mom, mass)
+    g.g2p()
+    gs, os_ = g.read_state(), o.read_state()
+    e = {"F": rel_l2(state_F(gs), state_F(os_)), "FtF": rel_l2(FtF(gs), FtF(os_)), "stress": rel_l2(stress6(gs), stress6(os_))}
+    print("return map %d on identical F: " % model + ", ".join("%s %.2e" % kv for kv in e.items()))
+    assert e["F"] <= 1e-5 and e["FtF"] <= 1e-5 and e["stress"] <= 1e-4, e
 
 
 # ----------------------------------------------------------------------------- trajectories
@@ -271,24 +311,151 @@ def test_trajectory_elastic_block_as_specified_20_substeps():
     assert ex <= 1e-4 and eF <= 1e-4
 
 
-@pytest.mark.parametrize("make", [lambda: S.shear_block(S.MAT_DRUCKER_PRAGER), lambda: S.shear_block(S.MAT_VON_MISES),
-                                  lambda: S.shear_block(S.MAT_GRANULAR_POWDER), lambda: S.shear_block(S.MAT_VISCOPLASTIC_MUD),
-                                  S.multimaterial],
-                         ids=["dp_shear", "vm_shear", "powder_shear", "mud_shear", "multimaterial_80k_128"])
-def test_trajectory_plastic_100_substeps(make):
-    sc = make()
-    gs, r = run_pair(sc, 100, ["mixed", "ref32"])
-    m, rr = r["mixed"], r["ref32"]
-    ex, ev = rel_l2(gs["P"][:, :3], m["P"][:, :3]), rel_l2(gs["v"][:, :3], m["v"][:, :3])
-    (sg, dg), (sm, dm) = sing(gs), sing(m)
-    es, ed = rel_l2(sg, sm), rel_l2(dg, dm)
-    print("%s 100 substeps vs mixed: x %.2e v %.2e sigma(F) %.2e |detF| %.2e (F %.2e stress %.2e); x %.2e vs ref32" %
-          (sc.name, ex, ev, es, ed, rel_l2(state_F(gs), state_F(m)), rel_l2(stress6(gs), stress6(m)), rel_l2(gs["P"][:, :3], rr["P"][:, :3])))
-    # x carries the 1e-4 bar; v and the singular values of F inherit the
-    # reference's F-orientation ambiguity (see the module docstring) and get
-    # sanity bounds only
-    assert ex <= 1e-4
-    assert ev <= 1e-2 and es <= 5e-3 and ed <= 1e-3
+def FtF(st):
+    F = np.stack([st["F0"][:, :3], st["F1"][:, :3], st["F2"][:, :3]], 1).astype(np.float64)
+    return np.einsum("nci,ncj->nij", F, F)
+
+
+def quantities(st):
+    """The compared quantities of a particle state: x, v, singular values and
+    |det| of F, F^T F (invariant under the rebuild's left factor)."""
+    s, d = sing(st)
+    return {"x": st["P"][:, :3], "v": st["v"][:, :3], "sigma": s, "detF": d, "FtF": FtF(st), "F": state_F(st)}
+
+
+def run_noisy(o, n, rel=1e-7, seed=1):
+    """n oracle substeps with every P2G sum (node momentum and mass)
+    multiplied by 1 + rel * N(0, 1): the size of the rounding differences
+    that another summation order (the GPU's float atomics) leaves in them."""
+    rng = np.random.default_rng(seed)
+    for _ in range(n):
+        o.zero_grid()
+        o.bin()
+        o.p2g()
+        mom, mass = o.get_grid()
+        mom[: o.nc, :3] *= 1.0 + rel * rng.standard_normal((o.nc, 3))
+        mass *= 1.0 + rel * rng.standard_normal(o.nc)
+        o.set_grid(mom.astype(np.float32), mass.astype(np.float32))
+        o.grid_update()
+        o.sdf_bc()
+        o.g2p()
+
+
+def p2g_rounding(sc):
+    """Relative L2 difference between the engine's and the oracle's P2G grid
+    (momentum and mass) for the scene's initial state: the size of the
+    rounding differences the GPU's summation order leaves in every substep's
+    grid sums (at least 1e-7)."""
+    eng = engine_for_scene(sc)
+    mom, mass = eng.export_grid(sc.params.dt)
+    eng.cleanup()
+    o = oracle_for(sc)
+    o.zero_grid()
+    o.bin()
+    o.p2g()
+    omom, omass = o.get_grid()
+    nc = sc.params.hash_cells
+    return max(1e-7, rel_l2(mom[:, :3], omom[:nc, :3]), rel_l2(mass, omass))
+
+
+def oracle_sensitivity(sc, n, mode="mixed", seeds=(1, 2)):
+    """(oracle state after n substeps, largest relative L2 spread of each
+    quantity between that run and runs whose P2G sums carry relative noise of
+    the size p2g_rounding measures, every substep): the reference
+    algorithm's own conditioning at the GPU's rounding."""
+    rel = p2g_rounding(sc)
+    a = oracle_for(sc, mode)
+    a.run(n)
+    sa = a.get_state()
+    qa = quantities(sa)
+    sens = {k: 0.0 for k in qa}
+    for seed in seeds:
+        b = oracle_for(sc, mode)
+        run_noisy(b, n, rel=rel, seed=seed)
+        qb = quantities(b.get_state())
+        for k in qa:
+            sens[k] = max(sens[k], rel_l2(qb[k], qa[k]))
+    sens["noise"] = rel
+    return sa, sens
+
+
+PLASTIC = [S.MAT_DRUCKER_PRAGER, S.MAT_VON_MISES, S.MAT_GRANULAR_POWDER, S.MAT_VISCOPLASTIC_MUD]
+PLASTIC_IDS = ["dp_shear", "vm_shear", "powder_shear", "mud_shear"]
+
+
+@pytest.mark.parametrize("model", PLASTIC, ids=PLASTIC_IDS)
+def test_trajectory_plastic_100_substeps(model):
+    """x, |det F|, singular values of F and F^T F after 100 substeps against
+    the oracle in the CUDA path's precision policy, each within 1e-4 or three
+    times the oracle's own spread under rounding-sized noise on its P2G sums."""
+    sc = S.shear_block(model)
+    eng = engine_for_scene(sc)
+    eng.run_substeps(sc.params.dt, 100)
+    qg = quantities(eng.state())
+    ref, sens = oracle_sensitivity(sc, 100)
+    qr = quantities(ref)
+    line = []
+    for k in ("x", "detF", "sigma", "FtF", "v"):
+        e, bar = rel_l2(qg[k], qr[k]), max(1e-4, 3.0 * sens[k])
+        line.append("%s %.2e (bar %.1e, oracle spread %.1e)" % (k, e, bar, sens[k]))
+        assert e <= bar, (k, e, bar)
+    per = np.abs(qg["sigma"] - qr["sigma"]).max(axis=1)
+    top = np.sort(per)[::-1]
+    share = float(np.sum(top[:10] ** 2) / max(np.sum(per ** 2), 1e-300))
+    print("%s 100 substeps vs mixed (P2G noise %.1e): %s; F %.2e; top-10 particles hold %.0f%% of the sigma error" %
+          (sc.name, sens["noise"], ", ".join(line), rel_l2(qg["F"], qr["F"]), 100 * share))
+    for k in ("x", "detF"):
+        assert sens[k] <= 1e-4 / 3.0, (k, sens[k])  # these carry the plain 1e-4 bar
+
+
+@pytest.mark.parametrize("model", PLASTIC, ids=PLASTIC_IDS)
+def test_plastic_F_short_horizon(model):
+    """F itself after 1 substep (before the rebuild's orientation ambiguity can
+    act) within 1e-4; after 10 substeps the singular values and |det F| within
+    1e-4 and F within 1e-4 or three times the oracle's own spread."""
+    sc = S.shear_block(model)
+    for n in (1, 10):
+        eng = engine_for_scene(sc)
+        eng.run_substeps(sc.params.dt, n)
+        qg = quantities(eng.state())
+        ref, sens = oracle_sensitivity(sc, n)
+        qr = quantities(ref)
+        e = {k: rel_l2(qg[k], qr[k]) for k in ("F", "sigma", "detF", "x")}
+        print("%s %d substeps: F %.2e (oracle spread %.1e) sigma %.2e |detF| %.2e x %.2e" % (sc.name, n, e["F"], sens["F"], e["sigma"],
+                                                                                           e["detF"], e["x"]))
+        assert e["x"] <= 1e-4 and e["sigma"] <= 1e-4 and e["detF"] <= 1e-4, e
+        assert e["F"] <= (1e-4 if n == 1 else max(1e-4, 3.0 * sens["F"])), (n, e["F"], sens["F"])
+        eng.cleanup()
+
+
+# Oracle spread of the Drucker-Prager sand half of the 80,000-particle
+# multimaterial scene after its 200 substeps, between a run from the seeded
+# state and one from positions perturbed by 1e-7 (measured with the mixed
+# oracle: singular values 1.23e-4, |det F| 2.07e-5, F^T F 5.2e-4; the jelly
+# half: singular values 2.8e-9, F 5.9e-9).
+CFG2_SAND_SPREAD = {"sigma": 1.23e-4, "detF": 2.07e-5}
+
+
+def test_trajectory_multimaterial_cfg2_200_substeps():
+    """The 80,000-particle multimaterial scene on 128^3 for its full 200
+    substeps against the mixed oracle: positions, and F of the ELASTIC jelly
+    half, within 1e-4; the Drucker-Prager sand half's |det F| within 1e-4 and
+    its singular values within three times the oracle's own spread (1.23e-4)."""
+    sc = S.load_config("cfg2")
+    assert sc.n == 80000 and sc.substeps == 200
+    gs, r = run_pair(sc, sc.substeps, ["mixed", "fp64"])
+    m = r["mixed"]
+    mat = m["mat"]
+    jelly, sand = mat == 0, mat == 1
+    assert jelly.sum() == 40000 and sand.sum() == 40000
+    qg, qm, q64 = quantities(gs), quantities(m), quantities(r["fp64"])
+    e = {"x": rel_l2(qg["x"], qm["x"]), "jelly_F": rel_l2(qg["F"][jelly], qm["F"][jelly]),
+         "jelly_sigma": rel_l2(qg["sigma"][jelly], qm["sigma"][jelly]), "sand_detF": rel_l2(qg["detF"][sand], qm["detF"][sand]),
+         "sand_sigma": rel_l2(qg["sigma"][sand], qm["sigma"][sand])}
+    print("multimaterial cfg2 200 substeps vs mixed: " + ", ".join("%s %.2e" % kv for kv in e.items()) +
+          "; vs fp64: x %.2e jelly F %.2e" % (rel_l2(qg["x"], q64["x"]), rel_l2(qg["F"][jelly], q64["F"][jelly])))
+    assert e["x"] <= 1e-4 and e["jelly_F"] <= 1e-4 and e["jelly_sigma"] <= 1e-4 and e["sand_detF"] <= 1e-4, e
+    assert e["sand_sigma"] <= max(1e-4, 3.0 * CFG2_SAND_SPREAD["sigma"]), e
 
 
 def test_trajectory_fluid_100_substeps():
@@ -328,6 +495,48 @@ def test_trajectory_sdf_terrain_small():
     (sg, dg), (sm, dm) = sing(gs), sing(ms)
     print("terrain 60 substeps: x %.3e sigma(F) %.3e vs mixed" % (ex, rel_l2(sg, sm)))
     assert ex <= 1e-4 and rel_l2(sg, sm) <= 1e-4
+
+
+def test_trajectory_slope_cfg3_100_substeps():
+    """The benched scene as benched: 1,000,000 Drucker-Prager particles on
+    256^3 over the 256^3 terrain SDF, dt = 2e-5, its first 100 substeps,
+    against the mixed oracle.  The slab starts two cells above the highest
+    terrain point and falls for the whole run (0.13 cells in 500 substeps),
+    so the grid SDF boundary acts on the nodes above the ridges while F stays
+    near the identity; positions, F, its singular values and |det F| within
+    1e-4 (the oracle's own spread under a 1e-7 perturbation of x0 is 1e-7 on
+    x and below 1e-9 on the rest)."""
+    sc = S.load_config("cfg3")
+    assert sc.n == 1000000 and sc.params.grid_res == (256, 256, 256) and sc.sdf is not None
+    gs, r = run_pair(sc, 100, ["mixed"])
+    qg, qm = quantities(gs), quantities(r["mixed"])
+    e = {k: rel_l2(qg[k], qm[k]) for k in ("x", "v", "F", "sigma", "detF", "FtF")}
+    print("slope cfg3 100 substeps vs mixed: " + ", ".join("%s %.2e" % kv for kv in e.items()))
+    assert all(e[k] <= 1e-4 for k in ("x", "F", "sigma", "detF", "FtF")), e
+
+
+def test_trajectory_terrain_contact_200_substeps():
+    """The slope scene on 128^3 (120,000 particles) sunk one cell into the
+    ridges and moving down at 1 m/s, so that the particle SDF push-out
+    (mpm_g2p.comp:220-252) and the grid SDF boundary (mpm_nanovdb_bc.comp:23-54)
+    act from the first substep: 200 substeps against the mixed oracle.  The
+    pushed-out particles restart from F = I and Drucker-Prager rebuilds the
+    others with three equal singular values, so F's orientation is left out;
+    x, v, the singular values, |det F| and F^T F within 1e-4 (the oracle's own
+    spread under rounding-sized noise on its grid sums is below 1e-6 for all
+    of them on this scene)."""
+    sc = S.slope_flow(res=128, n_side=(100, 12, 100), dt=2e-5, lift=-1.0, vy=-1.0)
+    gs, r = run_pair(sc, 200, ["mixed"])
+    ref = r["mixed"]
+    qg, qr = quantities(gs), quantities(ref)
+    line = []
+    for k in ("x", "v", "sigma", "detF", "FtF"):
+        err = rel_l2(qg[k], qr[k])
+        line.append("%s %.2e" % (k, err))
+        assert err <= 1e-4, (k, err)
+    moved = np.abs(state_F(ref) - np.eye(3).ravel()).max(axis=1) > 1e-3
+    print("terrain contact 200 substeps vs mixed: %s; %d particles with F != I" % (", ".join(line), int(moved.sum())))
+    assert moved.sum() > 1000  # the push-out and the boundary acted
 
 
 # ----------------------------------------------------------------------------- engine surface
