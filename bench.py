@@ -36,7 +36,7 @@ UNIT = "particle-substeps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20, help="timed steps (default 20 x 25 substeps = the workload's 500 substeps)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nebula", choices=["nebula", "reference"])
     ap.add_argument("--workload", default="slope", choices=["slope", "elastic", "multimaterial"])

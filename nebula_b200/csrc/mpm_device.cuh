@@ -478,7 +478,7 @@ template <class T> __device__ __forceinline__ m3<T> fixedCorotatedStress(const m
   return stressTextbook(U, k);
 }
 
-// Plastic return map + Kirchhoff stress, decompositions in float64.
+// Plastic return maps + Kirchhoff stress, decompositions in float64.
 // model VON_MISES: mpm_g2p.comp:19-38 then henckyStress; DRUCKER_PRAGER /
 // POWDER / MUD: mpm_g2p.comp:41-68 then henckyStress, as mpm_g2p.comp:150-181
 // calls them.  The return maps rebuild F as the shaders' `U * diag(s') *
@@ -490,18 +490,84 @@ template <class T> __device__ __forceinline__ m3<T> fixedCorotatedStress(const m
 // tau), so the second decomposition is run here too; its log-strains equal
 // the returned ones (k_i from e_i below) up to rounding.  Without a rebuild
 // (Von Mises inside the yield surface) the shader's second svd3 decomposes
-// the unchanged F again, which is the first decomposition.  The log-strains
-// and their exponentials are float64: a particle on the Von Mises yield
-// surface (where the last return left it) decides yield or not by the sign
-// of ||dev eps|| - q_max / (2 mu), a difference at the rounding of F itself,
-// and float logarithms there change the decision (and, through the rebuild,
-// F's orientation) against the float64 oracle.
+// the unchanged F again, which is the first decomposition.
+
+// Drucker-Prager (and POWDER / MUD) after the first decomposition.  The map
+// from log-strains to returned log-strains is continuous (the apex branch and
+// the deviatoric scaling meet where q_yield and delta reach zero), so the
+// log-strains, the projection and the exponentials are float: a log-strain
+// is formed as log1p of |sigma| - 1 taken in float64 (relative error of a
+// few float ulps even for strains of 1e-4, where log of a float sigma near 1
+// would lose three digits), and sigma' - 1 as expm1, so the rebuilt F in
+// float64 carries the float rounding of F itself.
+__device__ __forceinline__ float logStrain(double sigma) {
+  const double a = fabs(sigma);
+  if (a > 0.5 && a < 2.0) return log1pf(float(a - 1.0));
+  return logf(float(fmax(a, 1e-6)));
+}
+__device__ __forceinline__ double expStrain(float e) { return fabsf(e) < 0.5f ? 1.0 + double(expm1f(e)) : double(expf(e)); }
+
+__device__ __forceinline__ void druckerPragerFromSvd(m3<float>& F, m3<float>& tau, m3<double>& U, const double s[3], m3<double>& V, float mu,
+                                                     float lam, float M, float qc) {
+  constexpr float kThird = 1.0f / 3.0f;
+  float eps[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) eps[i] = logStrain(s[i]);
+  const float trEps = eps[0] + eps[1] + eps[2];
+  const float mean = trEps * kThird;
+  float dev[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) dev[i] = eps[i] - mean;
+  const float normDev = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const float K = lam + 2.0f * mu * kThird;
+  const float q_yield = M * (-K * trEps) + qc;
+  if (q_yield <= 1e-8f) {
+    const float tr = (qc / fmaxf(M, 1e-8f)) / K;  // -p_proj / K with p_proj = -qc / max(M, 1e-8)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eps[i] = tr * kThird;
+  } else {
+    const float delta = normDev - q_yield / (2.0f * mu);
+    if (delta > 0.0f && normDev > 1e-8f) {
+      const float r = delta / normDev;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
+    }
+  }
+  // the second decomposition's log-strains: log(max(exp(eps), 1e-6)) = max(eps, log 1e-6)
+  double sp[3];
+  float e[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    sp[i] = expStrain(eps[i]);
+    e[i] = fmaxf(eps[i], -13.815510557964274f);
+  }
+  const float te = e[0] + e[1] + e[2];
+  float k[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) k[i] = lam * te + 2.0f * mu * e[i];
+  const m3<double> Fn = rebuildUSVt(U, sp, V);
+  F = m3cast<float>(Fn);
+  double s2[3];
+  svd3F64(Fn, U, s2, V);
+  const double kd[3] = {double(k[0]), double(k[1]), double(k[2])};
+  tau = m3cast<float>(stressUDUt(U, kd));
+}
+
+// Von Mises, all in float64 after the decomposition as well: a particle on
+// the yield surface (where the last return left it) decides yield or not by
+// the sign of ||dev eps|| - q_max / (2 mu), a difference at the rounding of F
+// itself, and float logarithms there change the decision (and, through the
+// rebuild, F's orientation) against the float64 oracle.
 __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<float>& tau, float mu_f, float lam_f, float M_f, float qc_f,
                                               float qmax_f) {
-  const double mu = mu_f, lam = lam_f;
   m3<double> U, V;
   double s[3];
   svd3F64(m3cast<double>(F), U, s, V);
+  if (model != MAT_VON_MISES) {
+    druckerPragerFromSvd(F, tau, U, s, V, mu_f, lam_f, M_f, qc_f);
+    return;
+  }
+  const double mu = mu_f, lam = lam_f;
   // (divisions by constants and by 2 mu are multiplications by reciprocals:
   // within an ulp of float64 of the shaders' quotients)
   constexpr double kThird = 1.0 / 3.0;
@@ -515,36 +581,12 @@ __device__ __forceinline__ void plasticReturn(uint32_t model, m3<float>& F, m3<f
 #pragma unroll
   for (int i = 0; i < 3; ++i) dev[i] = eps[i] - mean;
   const double normDev = sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
-  bool rebuild;
-  if (model == MAT_VON_MISES) {
-    const double delta = normDev - double(qmax_f) * inv2mu;
-    rebuild = delta > 0.0 && normDev > 1e-8;
-    if (rebuild) {
-      const double r = delta / normDev;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
-    }
-  } else {
-    const double K = lam + 2.0 * mu * kThird;
-    const double p = -K * trEps;
-    const double q_yield = double(M_f) * p + double(qc_f);
-    rebuild = true;
-    if (q_yield <= 1e-8) {
-      const double p_proj = -double(qc_f) / fmax(double(M_f), 1e-8);
-      const double tr = -p_proj / K;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) eps[i] = tr * kThird;
-    } else {
-      const double delta = normDev - q_yield * inv2mu;
-      if (delta > 0.0 && normDev > 1e-8) {
-        const double r = delta / normDev;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
-      }
-    }
-  }
+  const double delta = normDev - double(qmax_f) * inv2mu;
   double k[3];
-  if (rebuild) {
+  if (delta > 0.0 && normDev > 1e-8) {
+    const double r = delta / normDev;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) eps[i] = (dev[i] - r * dev[i]) + mean;
     double sp[3], e[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
