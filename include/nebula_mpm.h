@@ -328,13 +328,14 @@ int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
 /* Launch shape of the per-substep kernels (block and tile sizes), picked per
  * GPU and workload by the project's autotuner (nebula_b200/autotune.py, a
  * JSON cache keyed by GPU and configuration).  fused_threads: CTA size of the
- * fused G2P/P2G kernel = particles per P2G chunk (128 or 256);
- * fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the fused
- * and grid-update kernels (0 = as many as fit; larger values are capped at
- * that); grid_batch: grid nodes per thread per round (2 or 4); fused_split:
- * work items per particle brick of the fused kernel (1-4, 0 = the default 4):
- * 1 keeps a brick's chunks in one CTA, k > 1 deals them over k CTAs (more
- * parallel items for scenes with few bricks, one tile flush per item).  Every shape
+ * fused G2P/P2G kernel (192 or 256; each warp takes 32 slots of the brick per
+ * round); fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the
+ * fused and grid-update kernels (0 = as many as fit; larger values are capped
+ * at that); grid_batch: grid nodes per thread per round (2 or 4); fused_split:
+ * work items per particle brick of the fused kernel (1-4, 0 = the default 1):
+ * 1 keeps a brick in one CTA, k > 1 cuts its slots into k contiguous parts
+ * handled by k CTAs (more parallel items for scenes with few bricks, one
+ * staging and one tile flush per item).  Every shape
  * computes the same substep (float sums may associate differently).  No
  * counterpart in the reference (its dispatch sizes are fixed in the shaders). */
 typedef struct nebula_mpm_launch_config {

@@ -1,10 +1,10 @@
 """Block- and tile-size autotuner for the per-substep kernels.
 
 The fused G2P/P2G kernel and the grid update take their launch shape from a
-``nebula_mpm_launch_config``: the fused kernel's CTA size (= particles per P2G
-chunk, 128 or 256), how many persistent CTAs each of the two kernels keeps per
-SM, the grid kernel's nodes per thread per round (2 or 4), and how many work
-items the fused kernel deals per particle brick (1-4).  Which shape is
+``nebula_mpm_launch_config``: the fused kernel's CTA size (192 or 256 threads),
+how many persistent CTAs each of the two kernels keeps per SM, the grid
+kernel's nodes per thread per round (2 or 4), and into how many work items
+the fused kernel cuts a particle brick (1-4).  Which shape is
 fastest depends on the GPU and on the workload (particles per brick, scene
 sizes, FLIP or APIC, the material mix), so ``tune`` times candidate shapes on
 the caller's own workload with CUDA events and keeps the fastest, by
@@ -35,7 +35,7 @@ from typing import Callable, Iterable
 from . import _capi
 
 CACHE_ENV = "NEBULA_B200_TUNE_CACHE"
-CACHE_VERSION = 2  # 2: shapes carry fused_split
+CACHE_VERSION = 3  # 2: shapes carry fused_split; 3: 192-thread CTAs, contiguous brick parts
 
 
 @dataclass(frozen=True)
@@ -44,7 +44,7 @@ class LaunchShape:
     fused_ctas_per_sm: int = 0  # 0 = as many as fit
     grid_ctas_per_sm: int = 0
     grid_batch: int = 4
-    fused_split: int = 4  # fused-kernel items per particle brick
+    fused_split: int = 1  # fused-kernel items per particle brick
 
     def to_c(self) -> _capi.LaunchConfig:
         return _capi.LaunchConfig(int(self.fused_threads), int(self.fused_ctas_per_sm), int(self.grid_ctas_per_sm), int(self.grid_batch),
@@ -66,7 +66,7 @@ class LaunchShape:
 @dataclass(frozen=True)
 class Limits:
     """Most CTAs per SM (occupancy) of each variant: fused[threads == 256], grid[batch == 4]."""
-    fused: tuple = (6, 3)
+    fused: tuple = (4, 3)
     grid: tuple = (8, 8)
 
     def fused_max(self, threads: int) -> int:
@@ -93,7 +93,7 @@ def _ctas_options(most: int, extra: Iterable[int]) -> list[int]:
 
 def fused_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:
     c = []
-    for threads in (256, 128):
+    for threads in (256, 192):
         most = limits.fused_max(threads)
         for k in _ctas_options(most, (most - 1, most // 2)):
             c.append(replace(base, fused_threads=threads, fused_ctas_per_sm=k))

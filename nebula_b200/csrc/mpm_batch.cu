@@ -274,8 +274,13 @@ void BatchEngine::seal() {
   check(cudaMemset(gridAcc_.ptr, 0, gridAcc_.bytes), "cudaMemset");
   check(cudaMemset(gridVel_.ptr, 0, gridVel_.bytes), "cudaMemset");
   tiles_ = (nbTotal_ + kBrickScanTile - 1) / kBrickScanTile;
-  for (DevBuf* b : {&bCount_, &bFlag_, &bStart_, &pbBrick_, &gbBrick_}) {
+  for (DevBuf* b : {&bCount_, &bFlag_, &pbBrick_, &gbBrick_}) {
     b->alloc(size_t(nbTotal_) * sizeof(uint32_t));
+    check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
+  }
+  // per-cell counts (kept zeroed between binnings) and starts of the in-brick cell order
+  for (DevBuf* b : {&cCount_, &cStart_}) {
+    b->alloc(size_t(nbTotal_) * 64u * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
   pbStart_.alloc(size_t(nbTotal_ + 1) * sizeof(uint32_t));
@@ -305,7 +310,8 @@ BrickBuffers BatchEngine::brickBuffers() {
   b.tiles = tiles_;
   b.brickCount = static_cast<uint32_t*>(bCount_.ptr);
   b.brickFlag = static_cast<uint32_t*>(bFlag_.ptr);
-  b.brickStart = static_cast<uint32_t*>(bStart_.ptr);
+  b.cellCount = static_cast<uint32_t*>(cCount_.ptr);
+  b.cellStart = static_cast<uint32_t*>(cStart_.ptr);
   b.pbBrick = static_cast<uint32_t*>(pbBrick_.ptr);
   b.pbStart = static_cast<uint32_t*>(pbStart_.ptr);
   b.gbBrick = static_cast<uint32_t*>(gbBrick_.ptr);

@@ -64,6 +64,45 @@ __device__ __forceinline__ uint32_t warpAggInc(uint32_t mask, uint32_t* counter,
   return base + __popc(peers & ((1u << lane) - 1u));
 }
 
+// The same for lanes whose keys come in a few runs (particles in cell order),
+// in two halves so the atomic's round trip overlaps other work: the claim
+// finds the groups with one ballot per distinct key instead of a match, and
+// every group leader issues its atomic at once; the rank reads the leader's
+// result later.  Every lane of `mask` calls both with the same mask.
+struct GroupTicket {
+  uint32_t peers;  // lanes of this lane's key
+  uint32_t base;   // the leader's atomic result (in the leader)
+};
+__device__ __forceinline__ GroupTicket warpGroupClaim(uint32_t mask, uint32_t* counter, uint32_t key) {
+  uint32_t pending = mask, mine = 0;
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const uint32_t k = __shfl_sync(mask, key, leader);
+    const uint32_t peers = __ballot_sync(mask, key == k);
+    if (key == k) mine = peers;
+    pending &= ~peers;
+  }
+  GroupTicket g{mine, 0u};
+  if (int(laneId()) == __ffs(mine) - 1) g.base = atomicAdd(counter + key, uint32_t(__popc(mine)));
+  return g;
+}
+__device__ __forceinline__ uint32_t warpGroupRank(uint32_t mask, const GroupTicket& g) {
+  const uint32_t base = __shfl_sync(mask, g.base, __ffs(g.peers) - 1);
+  return base + __popc(g.peers & ((1u << laneId()) - 1u));
+}
+
+// counter[key] += number of lanes of `mask` holding key (keys in a few runs).
+__device__ __forceinline__ void warpGroupAdd(uint32_t mask, uint32_t* counter, uint32_t key) {
+  uint32_t pending = mask;
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const uint32_t k = __shfl_sync(mask, key, leader);
+    const uint32_t peers = __ballot_sync(mask, key == k);
+    if (int(laneId()) == leader) atomicAdd(counter + k, uint32_t(__popc(peers)));
+    pending &= ~peers;
+  }
+}
+
 // Mark every brick holding a node of the 3x3x3 stencil around cell (cx,cy,cz).
 __device__ __forceinline__ void markStencilBricks(const SubstepParams& P, int cx, int cy, int cz, uint32_t* flag) {
   const int cr = int(P.cubeRes) - 1;
@@ -145,9 +184,10 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(SubstepParams P0, Scen
   auto body = [&](const SubstepParams& P, uint32_t base) {
     int cx, cy, cz;
     cellCoords(P, p.x, p.y, p.z, cx, cy, cz);
-    const uint32_t b = base + (mortonEncode(cx, cy, cz) >> 6);
-    B.binKey[i] = b;
-    B.binRank[i] = warpAggInc(mask, B.brickCount, b);
+    const uint32_t c = (base << 6) + mortonEncode(cx, cy, cz);
+    B.binKey[i] = c;
+    B.binRank[i] = warpAggInc(mask, B.cellCount, c);
+    (void)warpAggInc(mask, B.brickCount, c >> 6);
     markStencilBricks(P, cx, cy, cz, B.brickFlag + base);
   };
   if constexpr (BATCH) {
@@ -321,13 +361,10 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   uint32_t rc = s_prefix[0] + (warp > 0 ? s_warp[0][warp - 1] : 0u) + ic - sc;
   uint32_t rp = s_prefix[1] + (warp > 0 ? s_warp[1][warp - 1] : 0u) + ip - sp;
   uint32_t rg = s_prefix[2] + (warp > 0 ? s_warp[2][warp - 1] : 0u) + ig - sg;
-  uint32_t starts[kBrickScanItems];
 #pragma unroll
   for (int k = 0; k < kBrickScanItems; ++k) {
     const uint32_t b = b0 + k;
-    starts[k] = rc;
     if (b < B.nb) {
-      if (!full) B.brickStart[b] = rc;
       if (cnt[k]) {
         B.pbBrick[rp] = b;
         B.pbStart[rp] = rc;
@@ -340,11 +377,6 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
     }
     rc += cnt[k];
   }
-  if (full) {
-    uint4* ps = reinterpret_cast<uint4*>(B.brickStart + b0);
-    ps[0] = make_uint4(starts[0], starts[1], starts[2], starts[3]);
-    ps[1] = make_uint4(starts[4], starts[5], starts[6], starts[7]);
-  }
   if (tile == B.tiles - 1 && threadIdx.x == 0) {
     // the last tile's look-back finished, so all three totals are final
     const uint32_t npb = s_prefix[1] + s_warp[1][WL];
@@ -354,9 +386,33 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   }
 }
 
-// Sorted slot of buffer index t: the start of its brick plus its rank.
+// Cell starts of every listed particle brick: one warp per brick scans its 64
+// cell counts (two per lane) from the brick's first slot, and clears the
+// counts for the next binning.
+__global__ void __launch_bounds__(kThreads) k_cell_scan(BrickBuffers B) {
+  waitForPredecessorGrid();
+  const uint32_t numPB = B.counters[kCntNumPB];
+  const uint32_t lane = laneId();
+  const uint32_t warps = gridDim.x * (kThreads / 32);
+  for (uint32_t e = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); e < numPB; e += warps) {
+    const uint32_t b = B.pbBrick[e], start = B.pbStart[e];
+    uint2* pc = reinterpret_cast<uint2*>(B.cellCount + (size_t(b) << 6)) + lane;
+    const uint2 c = *pc;
+    *pc = make_uint2(0u, 0u);
+    uint32_t incl = c.x + c.y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= uint32_t(o)) incl += y;
+    }
+    const uint32_t first = start + incl - c.x - c.y;
+    reinterpret_cast<uint2*>(B.cellStart + (size_t(b) << 6))[lane] = make_uint2(first, first + c.x);
+  }
+}
+
+// Sorted slot of buffer index t: the start of its cell plus its rank.
 __device__ __forceinline__ void permScatterOne(const BrickBuffers& B, uint32_t n, uint32_t* err, uint32_t t) {
-  const uint32_t slot = B.brickStart[B.binKey[t]] + B.binRank[t];
+  const uint32_t slot = B.cellStart[B.binKey[t]] + B.binRank[t];
   if (slot < n) B.perm[slot] = t;
   else atomicOr(err, kErrBinRange);
 }
@@ -373,7 +429,7 @@ __device__ __forceinline__ void permScatterStrided(const BrickBuffers& B, uint32
       rank[k] = t < n ? B.binRank[t] : 0u;
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) start[k] = base + uint64_t(k) * stride < n ? B.brickStart[key[k]] : 0u;
+    for (int k = 0; k < 4; ++k) start[k] = base + uint64_t(k) * stride < n ? B.cellStart[key[k]] : 0u;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const uint64_t t = base + uint64_t(k) * stride;
@@ -444,11 +500,18 @@ __device__ __forceinline__ void p2gRegister(SM& sm, uint32_t packed, uint32_t pa
   if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(packed);
 }
 
-template <bool FLIP, int CHUNK>
-struct G2P2GSmem {
-  P2GSmemT<CHUNK> p2g;
-  float4 v[216];
+// Shared memory of the fused kernel (THREADS = the CTA size, 128 or 256).
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;  // a lane with no row for the warp's P2G
+
+template <bool FLIP, int THREADS>
+struct FusedSmem {
+  float4 rows[THREADS * kRow];  // P2G input rows; warp w owns rows [32 w, 32 w + 32)
+  float tiles[4 * kTileNodes];  // the item's 8^3 accumulation tile (mass, mom.x, mom.y, mom.z planes)
+  float mass[THREADS];          // the particle mass of an exact-form row
+  float4 v[216];                // staged 6^3 node block (v, mass)
   float4 vo[FLIP ? 216 : 1];
+  uint32_t markMask[2];         // grid-active marks of the item brick's 3^3 neighbour bricks, by item parity
+  uint32_t items[2];            // claimed items by item parity
 };
 
 // P2G inputs of one particle in separable form.  The quadratic B-spline weight
@@ -520,6 +583,16 @@ __device__ __forceinline__ bool p2gRow(const SubstepParams& P, const PState& s, 
       else row[3 * c + d] = make_float4(A[0] * sa, A[1] * sa, A[2] * sa, Wc);
     }
   return exact;
+}
+
+// Contribution of a usual-form row's three factors to its stencil node.
+__device__ __forceinline__ void p2gNodeTermXYZ(const float4 X, const float4 Y, const float4 Z, float acc[4]) {
+  const float wyz = Y.w * Z.w;
+  const float wxz = X.w * Z.w, wxy = X.w * Y.w;
+  acc[0] += wyz * X.x + wxz * Y.x + wxy * Z.x;
+  acc[1] += wyz * X.y + wxz * Y.y + wxy * Z.y;
+  acc[2] += wyz * X.z + wxz * Y.z + wxy * Z.z;
+  acc[3] += X.w * wyz;
 }
 
 // Contribution of a usual-form row to its stencil node (dx, dy, dz).
@@ -676,14 +749,6 @@ struct StagedGrid {
     return true;
   }
 };
-
-// Generic gather for particles whose stencil leaves the staged block (outside
-// the grid interior); kept out of line to keep the hot loop small.
-template <bool FLIP>
-__device__ __forceinline__ void gatherFallback(const SubstepParams& P, const PState& st, const StagedGrid<FLIP>& grid, float vpic[3], float vpo[3],
-                                            float Gv[3][3], float Bn[3][3]) {
-  g2pGather(P, st, grid, vpic, vpo, Gv, Bn);
-}
 
 // A particle's stencil centre among the brick's 6^3 cells (block origin ox,
 // oy, oz), packed as rx | ry << 3 | rz << 6 (cellSlotOf gives its slot), or -1.
@@ -864,23 +929,89 @@ __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridB
 }
 
 // ------------------------------------------------------------------ fused G2P -> update -> P2G
-// One item of a particle brick: G2P of the particles in the chunks of sorted
-// slots [start, end) of brick `b` (the scene's own brick id) that begin at
-// start, start + stride, ... (stride = CHUNK times the items per brick), from
-// the staged grid; particle update, binning count under the global brick key
-// brickBase + (Morton >> 6), and P2G of the updated particles.
-template <bool FLIP, int CHUNK>
-__device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP, CHUNK>& S, uint32_t b, uint32_t start, uint32_t end,
-                                          uint32_t stride, uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur,
-                                          StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B,
-                                          const GridBuffers& G, float dtStress, uint32_t* err) {
-  constexpr int kChunk = CHUNK;
-  auto& sm = S.p2g;
+// P2G of one warp's rows (written by the lanes holding a row, key = packed
+// stencil-centre cell, kNoKey for none): the lanes of equal key form a group,
+// and for each group lanes 0..26 take the cell's 27 stencil nodes, sum the
+// group's rows (each read at a known address, no list to follow) and add the
+// sums into the tile with shared-memory float reductions.  Warps do not wait
+// for one another.
+__device__ __forceinline__ void p2gWarpGroups(const SubstepParams& P, const float4* __restrict__ wrows, const float* __restrict__ wmass, float* tile,
+                                              uint32_t key, uint32_t exactMask, int tx, int ty, int tz) {
+  const int lane = threadIdx.x & 31;
+  const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
+  const int cr = int(P.cubeRes);
+  // a tile wholly inside the grid needs no per-node bounds test
+  const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
+  __syncwarp();  // the rows are visible to every lane
+  uint32_t pending = __ballot_sync(0xffffffffu, key != kNoKey);
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const uint32_t k = __shfl_sync(0xffffffffu, key, leader);
+    const uint32_t peers = __ballot_sync(0xffffffffu, key == k);
+    pending &= ~peers;
+    const int lx = int(k & 7u) + dx, ly = int((k >> 3) & 7u) + dy, lz = int(k >> 6) + dz;  // tile-local node
+    const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
+    if (lane < 27 && (inside || (nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr))) {
+      float a[4] = {0.f, 0.f, 0.f, 0.f};
+      if (!(peers & exactMask)) {
+        // usual-form rows: two per step, loads of both issued before their sums
+        uint32_t m = peers;
+        while (m) {
+          const int j0 = __ffs(m) - 1;
+          m &= m - 1u;
+          const int j1 = m ? __ffs(m) - 1 : -1;
+          m &= m - 1u;
+          const float4* r0 = wrows + j0 * kRow;
+          const float4 X0 = r0[dx], Y0 = r0[3 + dy], Z0 = r0[6 + dz];
+          float4 X1 = make_float4(0.f, 0.f, 0.f, 0.f), Y1 = X1, Z1 = X1;
+          if (j1 >= 0) {
+            const float4* r1 = wrows + j1 * kRow;
+            X1 = r1[dx]; Y1 = r1[3 + dy]; Z1 = r1[6 + dz];
+          }
+          p2gNodeTermXYZ(X0, Y0, Z0, a);
+          p2gNodeTermXYZ(X1, Y1, Z1, a);  // a missing second row adds zeros
+        }
+      } else {
+        uint32_t m = peers;
+        while (m) {
+          const int j = __ffs(m) - 1;
+          m &= m - 1u;
+          if ((exactMask >> j) & 1u) p2gNodeTermExact(wrows + j * kRow, wmass[j], dx, dy, dz, a);
+          else p2gNodeTerm(wrows + j * kRow, dx, dy, dz, a);
+        }
+      }
+      const int t = (lz * 8 + ly) * 8 + lx;
+      atomicAdd(tile + t, a[3]);
+      atomicAdd(tile + kTileNodes + t, a[0]);
+      atomicAdd(tile + 2 * kTileNodes + t, a[1]);
+      atomicAdd(tile + 3 * kTileNodes + t, a[2]);
+    }
+  }
+  __syncwarp();  // every lane has read the rows before they are written again
+}
+
+// One work item: the sorted slots [start, end) of particle brick `b` (the
+// scene's own brick id).  The binning orders a brick's particles by cell
+// (the brick's 64 cells in Morton order), so a warp's 32 consecutive slots
+// hold the particles of a few neighbouring cells: the G2P reads of the staged
+// 6^3 block are mostly broadcasts, the binning counts group into a few runs,
+// and the warp's P2G groups its lanes by stencil-centre cell
+// (p2gWarpGroups).  Per particle: G2P from the staged grid, particle update,
+// write to its slot in the next buffer, binning count under the global cell
+// key 64 brickBase + Morton code, stencil brick marks, and P2G into the
+// item's tile.  Warps take the item's rounds of 32 slots without waiting for
+// one another; the item ends with one barrier and the tile flush (one vector
+// reduction per non-zero node).  `mp` selects the item's marks.
+template <bool FLIP, int THREADS, int MS>
+__device__ __forceinline__ void g2p2gPart(const SubstepParams& P, FusedSmem<FLIP, THREADS>& S, uint32_t b, uint32_t start, uint32_t end,
+                                          uint32_t brickBase, StatePtrs cur, const uint32_t* __restrict__ pidCur, StatePtrs nxt,
+                                          uint32_t* __restrict__ pidNxt, uint32_t n, const BrickBuffers& B, const GridBuffers& G, float dtStress,
+                                          uint32_t* err, uint32_t mp) {
   int bx, by, bz;
   mortonDecode(b, bx, by, bz);
   // stage the 6^3 nodes [4b-1, 4b+4]^3 (nodes outside [0, gridRes) read as empty)
   const int sx = 4 * bx - 1, sy = 4 * by - 1, sz = 4 * bz - 1;
-  for (int q = threadIdx.x; q < 216; q += blockDim.x) {
+  for (int q = threadIdx.x; q < 216; q += THREADS) {
     const int x = sx + q % 6, y = sy + (q / 6) % 6, z = sz + q / 36;
     const bool valid = x >= 0 && y >= 0 && z >= 0 && x < P.gridRes[0] && y < P.gridRes[1] && z < P.gridRes[2];
     const uint32_t c = valid ? mortonEncode(x, y, z) : 0u;
@@ -893,94 +1024,100 @@ __device__ __forceinline__ void g2p2gItem(const SubstepParams& P, G2P2GSmem<FLIP
   __syncthreads();
   const StagedGrid<FLIP> grid{S.v, S.vo, G.vel, G.vold, sx, sy, sz};
   const int tx = sx - 1, ty = sy - 1, tz = sz - 1;
-  uint32_t par = 0;
-  for (uint32_t base = start; base < end; base += stride, par ^= 1u) {
-    const uint32_t t = base + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4* wrows = S.rows + warp * 32 * kRow;
+  float* wmass = S.mass + warp * 32;
+  const uint32_t cellBase = brickBase << 6;
+  uint32_t marks = 0;
+#pragma unroll 1
+  for (uint32_t t0 = start + uint32_t(warp) * 32u; t0 < end; t0 += THREADS) {
+    const uint32_t t = t0 + uint32_t(lane);  // the particle's slot in the next buffer
     const bool act = t < end;
     const uint32_t mask = __ballot_sync(0xffffffffu, act);
-    uint32_t marks = 0;
+    uint32_t key = kNoKey;
+    bool exact = false;
+    GroupTicket ticket{0u, 0u};
     if (act) {
       const uint32_t s = B.perm[t];
       const bool valid = s < n;
       PState st;
       int cx = 0, cy = 0, cz = 0;
-      uint32_t nb = 0;
+      uint32_t nc = 0;
       if (valid) {
         st = loadState(cur.f, s);
         const uint32_t pid = pidCur[s];
         float vpic[3], vpo[3], Gv[3][3], Bn[3][3];
-        if (!g2pGatherStaged<FLIP>(P, st, S.v, S.vo, sx, sy, sz, vpic, vpo, Gv, Bn)) gatherFallback<FLIP>(P, st, grid, vpic, vpo, Gv, Bn);
-        g2pUpdate(P, st, P.dt, vpic, vpo, Gv, Bn);
+        if (!g2pGatherStaged<FLIP>(P, st, S.v, S.vo, sx, sy, sz, vpic, vpo, Gv, Bn)) g2pGather(P, st, grid, vpic, vpo, Gv, Bn);
+        g2pUpdate<MS>(P, st, P.dt, vpic, vpo, Gv, Bn);
         storeState(nxt.f, t, st);
         pidNxt[t] = pid;
         if (!(isfinite(st.P.x) && isfinite(st.P.y) && isfinite(st.P.z))) atomicOr(err, kErrNonFinite);
         cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
-        nb = brickBase + (mortonEncode(cx, cy, cz) >> 6);
+        nc = cellBase + mortonEncode(cx, cy, cz);
       } else {
         atomicOr(err, kErrBinRange);  // a slot that maps nowhere: only after an expired scan wait
       }
-      // every active lane reaches this one call site
-      const uint32_t r = warpAggInc(mask, B.brickCount, nb);
-      B.binKey[t] = nb;
-      B.binRank[t] = r;
+      // every active lane reaches these call sites
+      ticket = warpGroupClaim(mask, B.cellCount, nc);
+      B.binKey[t] = nc;
+      warpGroupAdd(mask, B.brickCount, nc >> 6);
       if (valid) {
         if (!stencilBrickMask(P, cx, cy, cz, bx, by, bz, marks)) markStencilBricks(P, cx, cy, cz, B.brickFlag + brickBase);
-        float4* row = sm.rows + threadIdx.x * kRow;
         float m;
-        const bool exact = p2gRow(P, st, dtStress, cx, cy, cz, row, m);
-        sm.mass[threadIdx.x] = m;
-        const int key = cellPacked(cx, cy, cz, sx, sy, sz);
-        if (key >= 0) {
-          p2gRegister(sm, uint32_t(key), par, exact);
+        exact = p2gRow(P, st, dtStress, cx, cy, cz, wrows + lane * kRow, m);
+        wmass[lane] = m;
+        const int pk = cellPacked(cx, cy, cz, sx, sy, sz);
+        if (pk >= 0) {
+          key = uint32_t(pk);
         } else {
-          p2gRowGlobal(P, row, m, exact, cx, cy, cz, G.acc);
+          p2gRowGlobal(P, wrows + lane * kRow, m, exact, cx, cy, cz, G.acc);
           atomicAdd(B.counters + kCntOverflow, 1u);
         }
       }
     }
-    marks = __reduce_or_sync(0xffffffffu, marks);
-    if ((threadIdx.x & 31) == 0 && marks) atomicOr(&sm.markMask, marks);
-    p2gChunk(P, sm, par, tx, ty, tz);
+    p2gWarpGroups(P, wrows, wmass, S.tiles, key, __ballot_sync(0xffffffffu, exact), tx, ty, tz);
+    if (act) B.binRank[t] = warpGroupRank(mask, ticket);  // the count's atomic has returned by now
   }
-  // p2gChunk ended with a barrier: every warp's marks are in
-  flushBrickMarks(P, sm.markMask, bx, by, bz, B.brickFlag + brickBase);
-  p2gFlush(P, sm, tx, ty, tz, G.acc);
+  marks = __reduce_or_sync(0xffffffffu, marks);
+  if (lane == 0 && marks) atomicOr(&S.markMask[mp], marks);
+  __syncthreads();  // the tile and the marks are complete
+  flushBrickMarks(P, S.markMask[mp], bx, by, bz, B.brickFlag + brickBase);
+  p2gFlush(P, S, tx, ty, tz, G.acc);
 }
 
-// 768 / CHUNK CTAs per SM (3 of 256 threads, 6 of 128): 80 registers with some
-// spills to L1-cached local memory beat 2 CTAs of 256 at 128 registers
-// (measured on the 1M-particle slope: Drucker-Prager -3%, Von Mises -6%,
-// ELASTIC -9% per launch); shared memory is 54 KB per 256-thread CTA.
-// The queue deals `split` items per particle brick: item i is part
-// i / numPB of brick i % numPB and takes the brick's chunks part, part +
-// split, ...; parts beyond a brick's last chunk are skipped.  split = 1 keeps
-// a brick in one CTA (one staging and one tile flush per brick); more items
-// per brick shorten the longest item, which bounds small scenes.
-template <bool FLIP, bool BATCH, int CHUNK>
-__global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
-                                                    StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G,
-                                                    float dtStress, uint32_t* err, uint32_t split) {
+// Persistent CTAs pull work items from the queue: item i is part i / numPB of
+// particle brick i % numPB, whose sorted slots are cut into `split`
+// contiguous parts of near-equal size (empty parts are skipped).  split = 1
+// keeps a brick in one CTA (one staging and one tile flush per brick); more
+// parts shorten the longest item, which bounds small scenes.  768 / THREADS
+// CTAs per SM (4 of 192 threads, 3 of 256): 80 registers with some spills to
+// L1-cached local memory.  MS: the material-model set compiled in.
+template <bool FLIP, bool BATCH, int THREADS, int MS>
+__global__ void __launch_bounds__(THREADS, 768 / THREADS) k_g2p2g(SubstepParams P0, SceneTable T, StatePtrs cur, const uint32_t* __restrict__ pidCur,
+                                                      StatePtrs nxt, uint32_t* __restrict__ pidNxt, uint32_t n, BrickBuffers B, GridBuffers G,
+                                                      float dtStress, uint32_t* err, uint32_t split) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  G2P2GSmem<FLIP, CHUNK>& S = *reinterpret_cast<G2P2GSmem<FLIP, CHUNK>*>(smem_raw);
-  auto& sm = S.p2g;
+  FusedSmem<FLIP, THREADS>& S = *reinterpret_cast<FusedSmem<FLIP, THREADS>*>(smem_raw);
   waitForPredecessorGrid();
   const uint32_t numPB = B.counters[kCntNumPB];
   const uint32_t numItems = numPB * split;
-  // The tile, cell lists and counters start zeroed here and are left so by
-  // every item (the flush clears the tile, the list walk the cell heads, each
-  // chunk its cell count, thread 0 the marks after the item's last barrier).
-  p2gZeroTiles(sm);
+  // The tile starts zeroed here and is left so by every item's flush.
+  for (int q = threadIdx.x; q < 4 * kTileNodes; q += THREADS) S.tiles[q] = 0.f;
   // the claim alternates between two slots: a thread may claim the next item
   // while others still read this one, never two ahead (one barrier per claim)
   for (uint32_t it = 0;; it ^= 1u) {
-    if (threadIdx.x == 0) sm.items[it] = atomicAdd(B.counters + kCntQueueFused, 1u);
+    if (threadIdx.x == 0) {
+      S.items[it] = atomicAdd(B.counters + kCntQueueFused, 1u);
+      S.markMask[it] = 0u;  // last read by the item two back, before the previous claim's barrier
+    }
     __syncthreads();
-    const uint32_t i = sm.items[it];
+    const uint32_t i = S.items[it];
     if (i >= numItems) break;
     const uint32_t part = i / numPB, bi = i - part * numPB;
-    const uint32_t b = B.pbBrick[bi], end = min(B.pbStart[bi + 1], n), first = min(B.pbStart[bi], end) + part * uint32_t(CHUNK);
-    if (first >= end) continue;  // the brick has no chunk for this part
-    const uint32_t start = first, stride = split * uint32_t(CHUNK);
+    const uint32_t b = B.pbBrick[bi], bend = min(B.pbStart[bi + 1], n), bstart = min(B.pbStart[bi], bend);
+    const uint32_t len = (bend - bstart + split - 1u) / split;
+    const uint32_t start = min(bstart + part * len, bend), end = min(start + len, bend);
+    if (start >= end) continue;  // the brick has no particles for this part
     if constexpr (BATCH) {
       __shared__ SubstepParams sP;
       __shared__ uint32_t sBase;
@@ -991,12 +1128,10 @@ __global__ void __launch_bounds__(CHUNK, 768 / CHUNK) k_g2p2g(SubstepParams P0, 
       }
       __syncthreads();
       const uint32_t base = sBase;
-      g2p2gItem<FLIP, CHUNK>(sP, S, b - base, start, end, stride, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err);
+      g2p2gPart<FLIP, THREADS, MS>(sP, S, b - base, start, end, base, cur, pidCur, nxt, pidNxt, n, B, offsetGrid(G, base), sP.dt, err, it);
     } else {
-      g2p2gItem<FLIP, CHUNK>(P0, S, b, start, end, stride, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err);
+      g2p2gPart<FLIP, THREADS, MS>(P0, S, b, start, end, 0u, cur, pidCur, nxt, pidNxt, n, B, G, dtStress, err, it);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sm.markMask = 0u;  // read before the barrier, set again after the next claim's
   }
 }
 
@@ -1046,8 +1181,17 @@ constexpr int kShapeSlots = 64;  // device ordinals beyond this share slots modu
 LaunchShapes g_shapes[kShapeSlots];
 std::mutex g_shapesMutex;
 
-template <bool FLIP, bool BATCH, int CHUNK> void setupFused(LaunchShapes& L) {
-  L.fused[FLIP][BATCH][CHUNK == 256] = bigSmemCtasPerSm(k_g2p2g<FLIP, BATCH, CHUNK>, CHUNK, sizeof(G2P2GSmem<FLIP, CHUNK>));
+template <bool FLIP, bool BATCH, int THREADS, int MS> void setupFused(LaunchShapes& L) {
+  // every model set of one shape has the same shared memory and register bound
+  L.fused[FLIP][BATCH][THREADS == 256] = bigSmemCtasPerSm(k_g2p2g<FLIP, BATCH, THREADS, MS>, THREADS, sizeof(FusedSmem<FLIP, THREADS>));
+}
+template <int THREADS> void setupFusedShape(LaunchShapes& L) {
+  setupFused<false, false, THREADS, kModelsElastic>(L);
+  setupFused<false, false, THREADS, kModelsDruckerPrager>(L);
+  setupFused<false, false, THREADS, kModelsAny>(L);
+  setupFused<false, true, THREADS, kModelsAny>(L);
+  setupFused<true, false, THREADS, kModelsAny>(L);
+  setupFused<true, true, THREADS, kModelsAny>(L);
 }
 
 const LaunchShapes& shapes() {
@@ -1062,14 +1206,8 @@ const LaunchShapes& shapes() {
   L.grid[0] = ctasPerSm(k_grid_bricks<2>, kThreads);
   L.grid[1] = ctasPerSm(k_grid_bricks<4>, kThreads);
   L.gridBatch = ctasPerSm(k_grid_bricks_batch, kThreads);
-  setupFused<false, false, 128>(L);
-  setupFused<false, false, 256>(L);
-  setupFused<false, true, 128>(L);
-  setupFused<false, true, 256>(L);
-  setupFused<true, false, 128>(L);
-  setupFused<true, false, 256>(L);
-  setupFused<true, true, 128>(L);
-  setupFused<true, true, 256>(L);
+  setupFusedShape<192>(L);
+  setupFusedShape<256>(L);
   L.ready.store(true, std::memory_order_release);
   return L;
 }
@@ -1131,7 +1269,15 @@ cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32
 }
 
 cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches) {
-  const cudaError_t e = launchSerialized(k_brick_scan, dim3(b.tiles), dim3(kBrickScanThreads), 0, s, b, err);
+  cudaError_t e = launchSerialized(k_brick_scan, dim3(b.tiles), dim3(kBrickScanThreads), 0, s, b, err);
+  ++*launches;
+  if (e != cudaSuccess) return e;
+  // one warp per particle brick; at most one brick per particle, so the grid covers min(bricks, particles / 32) warps
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint32_t blocks = std::min<uint32_t>(blocksFor(uint64_t(b.nb) * 32u), uint32_t(std::max(sms, 1)) * 4u);
+  e = launchSerialized(k_cell_scan, dim3(blocks), dim3(kThreads), 0, s, b);
   ++*launches;
   return e;
 }
@@ -1185,34 +1331,57 @@ cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, 
 
 namespace {
 
-template <bool FLIP, bool BATCH, int CHUNK>
+template <bool FLIP, bool BATCH, int THREADS, int MS>
 cudaError_t launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt,
                         uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, uint32_t ctasPerSm, uint32_t split,
                         int numSMs, cudaStream_t s) {
-  const int blocks = persistentGrid(ctasPerSm, shapes().fused[FLIP][BATCH][CHUNK == 256], numSMs);
-  return launchSerialized(k_g2p2g<FLIP, BATCH, CHUNK>, dim3(blocks), dim3(CHUNK), sizeof(G2P2GSmem<FLIP, CHUNK>), s, P, T, cur, pidCur, nxt,
-                          pidNxt, n, b, g, dtStress, err, split);
+  const int blocks = persistentGrid(ctasPerSm, shapes().fused[FLIP][BATCH][THREADS == 256], numSMs);
+  return launchSerialized(k_g2p2g<FLIP, BATCH, THREADS, MS>, dim3(blocks), dim3(THREADS), sizeof(FusedSmem<FLIP, THREADS>), s, P, T, cur, pidCur,
+                          nxt, pidNxt, n, b, g, dtStress, err, split);
+}
+
+// The instantiation for the launch shape and the model set: model-specialised
+// kernels exist for single scenes with APIC or PIC transfer.
+template <bool BATCH, int THREADS>
+cudaError_t launchFusedShape(bool flip, int modelSet, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur,
+                             const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g,
+                             float dtStress, uint32_t* err, int numSMs, cudaStream_t s) {
+  const uint32_t k = lc.fusedCtasPerSm, sp = std::max(lc.fusedSplit, 1u);
+  if (flip) return launchFused<true, BATCH, THREADS, kModelsAny>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+  if constexpr (!BATCH) {
+    if (modelSet == kModelsElastic)
+      return launchFused<false, false, THREADS, kModelsElastic>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    if (modelSet == kModelsDruckerPrager)
+      return launchFused<false, false, THREADS, kModelsDruckerPrager>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+  }
+  return launchFused<false, BATCH, THREADS, kModelsAny>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
 }
 
 template <bool BATCH>
-cudaError_t launchFusedFor(bool flip, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur, const uint32_t* pidCur,
-                           StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err,
-                           int numSMs, cudaStream_t s) {
-  const uint32_t k = lc.fusedCtasPerSm, sp = std::max(lc.fusedSplit, 1u);
-  if (flip) {
-    if (lc.fusedThreads == 128) return launchFused<true, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-    return launchFused<true, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-  }
-  if (lc.fusedThreads == 128) return launchFused<false, BATCH, 128>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
-  return launchFused<false, BATCH, 256>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+cudaError_t launchFusedFor(bool flip, int modelSet, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur,
+                           const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g, float dtStress,
+                           uint32_t* err, int numSMs, cudaStream_t s) {
+  if (lc.fusedThreads == 192)
+    return launchFusedShape<BATCH, 192>(flip, modelSet, lc, P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
+  return launchFusedShape<BATCH, 256>(flip, modelSet, lc, P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
 }
 
 }  // namespace
 
-cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+int modelSetOf(const Material* mats, uint32_t count) {
+  bool elastic = count > 0, dp = count > 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    elastic = elastic && mats[i].model == MAT_ELASTIC;
+    dp = dp && (mats[i].model == MAT_DRUCKER_PRAGER || mats[i].model == MAT_GRANULAR_POWDER);
+  }
+  return elastic ? kModelsElastic : dp ? kModelsDruckerPrager : kModelsAny;
+}
+
+cudaError_t launchG2P2G(const SubstepParams& P, int modelSet, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                         const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                         uint64_t* launches) {
-  const cudaError_t e = launchFusedFor<false>(P.flip_ratio > 0.01f, lc, P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
+  const cudaError_t e =
+      launchFusedFor<false>(P.flip_ratio > 0.01f, modelSet, lc, P, SceneTable{}, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, numSMs, s);
   ++*launches;
   return e;
 }
@@ -1220,7 +1389,7 @@ cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* p
 cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                              const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches) {
-  const cudaError_t e = launchFusedFor<true>(flip, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
+  const cudaError_t e = launchFusedFor<true>(flip, kModelsAny, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
   ++*launches;
   return e;
 }

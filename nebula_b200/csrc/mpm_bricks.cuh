@@ -6,10 +6,12 @@
 //   g2p2g    per particle brick: G2P from the staged grid, particle update,
 //            P2G of the updated particle into a shared tile, binning count
 //   scan     brick counts / marks -> particle-brick list, grid-brick list,
-//            brick starts (single pass, decoupled look-back, compaction)
-//   perm     (brick, rank) -> sorted slot of every particle
-// Particles are physically reordered by brick every substep (ping-pong state
-// buffers plus the original particle id).
+//            brick starts (single pass, decoupled look-back, compaction),
+//            then per listed particle brick its 64 cell starts
+//   perm     (cell, rank) -> sorted slot of every particle
+// Particles are physically reordered by cell every substep (bricks in Morton
+// order, the 64 cells of a brick in Morton order; ping-pong state buffers
+// plus the original particle id).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -30,15 +32,16 @@ struct BrickBuffers {
   uint32_t tiles;             // scan tiles over nb
   uint32_t* brickCount;       // [nb] particles per brick (zeroed by the scan)
   uint32_t* brickFlag;        // [nb] grid-active marks (zeroed by the scan)
-  uint32_t* brickStart;       // [nb] first sorted slot of each brick
+  uint32_t* cellCount;        // [64 nb] particles per cell (zeroed by the scan)
+  uint32_t* cellStart;        // [64 nb] first sorted slot of each cell of a particle brick
   uint32_t* pbBrick;          // [nb] particle-brick list
   uint32_t* pbStart;          // [nb + 1] first slot of each listed brick; pbStart[numPB] = total
   uint32_t* gbBrick;          // [nb] grid-brick list, ascending (k_brick_scan writes it in brick order)
   uint32_t* counters;         // [kCntSlots]
   unsigned long long* scanState;  // [3 * tiles] status words (epoch-tagged)
   unsigned long long* scanTile;   // monotone tile counter
-  uint32_t* binKey;           // [cap] brick of each particle (by buffer index)
-  uint32_t* binRank;          // [cap] rank inside its brick
+  uint32_t* binKey;           // [cap] cell (global code: 64 x brick + Morton code in the brick) of each particle (by buffer index)
+  uint32_t* binRank;          // [cap] rank inside its cell
   uint32_t* perm;             // [cap] sorted slot -> buffer index
 };
 
@@ -63,11 +66,11 @@ struct GridBuffers {
 // Launch shape of the per-substep kernels, picked per GPU and workload by the
 // autotuner (nebula_b200/autotune.py); 0 CTAs per SM = as many as fit.
 struct LaunchConfig {
-  uint32_t fusedThreads = 256;  // k_g2p2g CTA size = particles per P2G chunk: 128 or 256
+  uint32_t fusedThreads = 256;  // k_g2p2g CTA size: 192 or 256 (a warp takes 32 slots per round)
   uint32_t fusedCtasPerSm = 0;  // persistent k_g2p2g CTAs per SM
   uint32_t gridCtasPerSm = 0;   // persistent grid-update CTAs per SM
   uint32_t gridBatch = 4;       // k_grid_bricks nodes per thread per round: 2 or 4
-  uint32_t fusedSplit = 4;      // k_g2p2g items per particle brick (1-4): a brick's chunks dealt over that many CTAs
+  uint32_t fusedSplit = 1;      // k_g2p2g items per particle brick (1-4): contiguous parts of a brick's slots
 };
 // Most CTAs per SM (occupancy) of each variant: [fusedThreads == 256], [gridBatch == 4].
 struct LaunchLimits {
@@ -79,7 +82,8 @@ LaunchLimits launchLimits(bool flip, bool batch);
 // Standalone binning of the particles in buffer order: counts + stencil marks.
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches);
-// Compaction scan (tile numbering and status epochs come from a device ticket).
+// Compaction scan (tile numbering and status epochs come from a device ticket),
+// then a second launch with the cell starts of every particle brick.
 cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches);
 cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches);
 // P2G of the particles of every listed brick (no binning, no marks).
@@ -98,8 +102,12 @@ cudaError_t launchGridBricks(const SubstepParams& P, const BrickBuffers& b, Grid
                              int numSMs, cudaStream_t s, uint64_t* launches);
 // Zero acc over the listed grid bricks (discarding a pending P2G).
 cudaError_t launchClearBricks(const BrickBuffers& b, GridBuffers g, int numSMs, cudaStream_t s, uint64_t* launches);
-// The fused G2P -> particle update -> P2G + binning count.
-cudaError_t launchG2P2G(const SubstepParams& P, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
+// The material-model set (ModelSet, mpm_particle.cuh) a fused kernel may be
+// specialised for: that of every material of the table.
+int modelSetOf(const Material* mats, uint32_t count);
+// The fused G2P -> particle update -> P2G + binning count, specialised for
+// `modelSet` where an instantiation exists.
+cudaError_t launchG2P2G(const SubstepParams& P, int modelSet, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
                         const BrickBuffers& b, GridBuffers g, float dtStress, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                         uint64_t* launches);
 // Batched forms: every scene of `T` in one launch.  `substep` selects the

@@ -103,8 +103,13 @@ MPMEngine::MPMEngine(const nebula_mpm_config& cfg) : cfg_(cfg) {
   gridVel_.alloc(size_t(ncPad_) * sizeof(float4));
   check(cudaMemset(gridAcc_.ptr, 0, gridAcc_.bytes), "cudaMemset");
   check(cudaMemset(gridVel_.ptr, 0, gridVel_.bytes), "cudaMemset");
-  for (DevBuf* b : {&bCount_, &bFlag_, &bStart_, &pbBrick_, &gbBrick_}) {
+  for (DevBuf* b : {&bCount_, &bFlag_, &pbBrick_, &gbBrick_}) {
     b->alloc(size_t(nb_) * sizeof(uint32_t));
+    check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
+  }
+  // per-cell counts (kept zeroed between binnings) and starts of the in-brick cell order
+  for (DevBuf* b : {&cCount_, &cStart_}) {
+    b->alloc(size_t(nb_) * 64u * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
   pbStart_.alloc(size_t(nb_ + 1) * sizeof(uint32_t));
@@ -328,10 +333,10 @@ void MPMEngine::setParams(const nebula_mpm_params& p) {
 }
 
 void validateLaunchConfig(const LaunchConfig& c) {
-  if (c.fusedThreads != 128 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 128 or 256");
+  if (c.fusedThreads != 192 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 192 or 256");
   if (c.gridBatch != 2 && c.gridBatch != 4) throw Error(NEBULA_MPM_ERR_INVALID, "grid_batch must be 2 or 4");
   if (c.fusedCtasPerSm > 64 || c.gridCtasPerSm > 64) throw Error(NEBULA_MPM_ERR_INVALID, "CTAs per SM must be <= 64 (0 = as many as fit)");
-  if (c.fusedSplit < 1 || c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 1-4 (0 = 4)");
+  if (c.fusedSplit < 1 || c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 1-4 (0 = 1)");
 }
 
 LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
@@ -340,7 +345,7 @@ LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
   l.fusedCtasPerSm = c.fused_ctas_per_sm;
   l.gridCtasPerSm = c.grid_ctas_per_sm;
   l.gridBatch = c.grid_batch;
-  l.fusedSplit = c.fused_split == 0 ? 4u : c.fused_split;
+  l.fusedSplit = c.fused_split == 0 ? 1u : c.fused_split;
   return l;
 }
 
@@ -713,7 +718,8 @@ BrickBuffers MPMEngine::brickBuffers() {
   b.tiles = tiles_;
   b.brickCount = static_cast<uint32_t*>(bCount_.ptr);
   b.brickFlag = static_cast<uint32_t*>(bFlag_.ptr);
-  b.brickStart = static_cast<uint32_t*>(bStart_.ptr);
+  b.cellCount = static_cast<uint32_t*>(cCount_.ptr);
+  b.cellStart = static_cast<uint32_t*>(cStart_.ptr);
   b.pbBrick = static_cast<uint32_t*>(pbBrick_.ptr);
   b.pbStart = static_cast<uint32_t*>(pbStart_.ptr);
   b.gbBrick = static_cast<uint32_t*>(gbBrick_.ptr);
@@ -834,7 +840,7 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   phaseEnd(kPhaseGrid, s, l0);
   l0 = launches_;
   phaseBegin(kPhaseFused, s);
-  check(launchG2P2G(P, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
+  check(launchG2P2G(P, modelSetOf(hostMaterials_.data(), uint32_t(hostMaterials_.size())), statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
                     static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, P.dt, err, launchCfg_, numSMs_, s, &launches_),
         "g2p2g");
   phaseEnd(kPhaseFused, s, l0);
@@ -920,7 +926,7 @@ void putKey(std::vector<unsigned char>& k, const T& v) {
 }  // namespace
 // graph keys compare these records as bytes, so none of them may have padding
 static_assert(sizeof(SubstepParams) == 24 * 4 + 4 * sizeof(void*), "SubstepParams has padding");
-static_assert(sizeof(BrickBuffers) == 2 * 4 + 12 * sizeof(void*), "BrickBuffers has padding");
+static_assert(sizeof(BrickBuffers) == 2 * 4 + 13 * sizeof(void*), "BrickBuffers has padding");
 static_assert(sizeof(StatePtrs) == 8 * sizeof(void*), "StatePtrs has padding");
 static_assert(sizeof(GridBuffers) == 3 * sizeof(void*), "GridBuffers has padding");
 static_assert(sizeof(LaunchConfig) == 5 * 4, "LaunchConfig has padding");
@@ -942,6 +948,7 @@ std::vector<unsigned char> MPMEngine::graphKey(const SubstepParams& P) {
   putKey(k, err_.ptr);
   putKey(k, launchCfg_);
   putKey(k, numSMs_);
+  putKey(k, modelSetOf(hostMaterials_.data(), uint32_t(hostMaterials_.size())));  // the fused kernel's instantiation
   return k;
 }
 

@@ -307,9 +307,21 @@ __device__ __forceinline__ bool g2pGatherStaged(const SubstepParams& P, const PS
   return true;
 }
 
+// Material-model sets the particle update is compiled for: any model
+// (dispatched per particle), or a scene whose every material is of one family,
+// for which the update holds only that family's code (a smaller kernel with
+// fewer values live across the stress; chosen by the host from the material
+// table).
+enum ModelSet : int {
+  kModelsAny = 0,
+  kModelsElastic = 1,        // ELASTIC (Hencky) only
+  kModelsDruckerPrager = 2,  // DRUCKER_PRAGER and GRANULAR_POWDER (the same return map, no viscosity)
+};
+
 // Everything of mpm_g2p.comp after the gather (lines 120-271): material,
 // F update, return map, stress, J reset, transfer, advection, SDF push-out,
 // world clamp, write-back.  Returns event bits (1 J reset, 2 SDF push-out).
+template <int MS = kModelsAny>
 __device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s, float dt, const float vpic[3], const float vpo[3],
                                               const float G[3][3], float Bn[3][3]) {
   const float h = P.cellSize;
@@ -327,7 +339,11 @@ __device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s,
     for (int b = 0; b < 3; ++b) A.m[a][b] = (a == b ? 1.f : 0.f) + dt * G[a][b];
   m3<float> Fn = m3mul(A, F);
   m3<float> tau;
-  if (mat.model == MAT_FLUID) {
+  if constexpr (MS == kModelsDruckerPrager) {
+    plasticReturn(MAT_DRUCKER_PRAGER, Fn, tau, mat.mu, mat.lam, mat.M, mat.qc, mat.qmax);
+  } else if constexpr (MS == kModelsElastic) {
+    tau = henckyStress<float>(Fn, mat.mu, mat.lam);
+  } else if (mat.model == MAT_FLUID) {
     float J = fmaxf(m3det(Fn), 1e-4f);
     float c = powf(J, 1.0f / 3.0f);
     Fn = m3zero<float>();

@@ -12,8 +12,8 @@ from nebula_b200.engine import engine_for_scene
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [A.LaunchShape(), A.LaunchShape(128, 0, 0, 4), A.LaunchShape(256, 1, 2, 2), A.LaunchShape(128, 3, 4, 2), A.LaunchShape(256, 2, 8, 4),
-          A.LaunchShape(256, 0, 0, 4, 1), A.LaunchShape(256, 0, 0, 4, 2), A.LaunchShape(128, 0, 0, 4, 3)]
+SHAPES = [A.LaunchShape(), A.LaunchShape(192, 0, 0, 4), A.LaunchShape(256, 1, 2, 2), A.LaunchShape(192, 3, 4, 2), A.LaunchShape(256, 2, 8, 4),
+          A.LaunchShape(256, 0, 0, 4, 4), A.LaunchShape(256, 0, 0, 4, 2), A.LaunchShape(192, 0, 0, 4, 3)]
 
 
 def rel(a, b):
@@ -41,18 +41,18 @@ def test_every_shape_computes_the_same_substeps(flip):
 
 def test_bad_shapes_are_rejected():
     e = engine_for_scene(S.shear_block())
-    for bad in (A.LaunchShape(64, 0, 0, 4), A.LaunchShape(256, 0, 0, 3), A.LaunchShape(256, 65, 0, 4), A.LaunchShape(256, 0, 0, 4, 5)):
+    for bad in (A.LaunchShape(64, 0, 0, 4), A.LaunchShape(128, 0, 0, 4), A.LaunchShape(256, 0, 0, 3), A.LaunchShape(256, 65, 0, 4), A.LaunchShape(256, 0, 0, 4, 5)):
         with pytest.raises(_capi.NebulaError):
             e.set_launch_config(bad)
     assert e.launch_config() == A.LaunchShape()
     lim = A.device_limits(False, False)
-    assert lim.fused_max(256) >= 1 and lim.fused_max(128) >= lim.fused_max(256) and lim.grid_max(4) >= 1
+    assert lim.fused_max(256) >= 1 and lim.fused_max(192) >= lim.fused_max(256) and lim.grid_max(4) >= 1
 
 
 def test_batch_shapes_agree_and_tune_batch_caches(tmp_path):
     scenes = S.batch_mix(only={0, 1, 2, 3})
     out = []
-    for shape in (A.LaunchShape(), A.LaunchShape(128, 0, 4, 2), A.LaunchShape(256, 0, 0, 4, 1)):
+    for shape in (A.LaunchShape(), A.LaunchShape(192, 0, 4, 2), A.LaunchShape(256, 0, 0, 4, 3)):
         b, ids = batch_for_scenes(scenes)
         b.set_launch_config(shape)
         assert b.launch_config() == shape

@@ -60,7 +60,8 @@ def test_brick_bins_match_oracle_cells(make):
 
 
 def test_brick_bins_after_substeps():
-    """Binning produced inside the fused kernel after 30 substeps."""
+    """Binning produced inside the fused kernel after 30 substeps: bricks in
+    ascending order, the particles of a brick in cell order."""
     sc = S.shear_block()
     eng = engine_for_scene(sc)
     eng.run_substeps(sc.params.dt, 30)
@@ -68,8 +69,11 @@ def test_brick_bins_after_substeps():
     ids, starts, pids = eng.export_brick_bins()
     h = sc.params.cell_size
     g = np.clip(np.floor(st["P"][:, :3].astype(np.float32) / np.float32(h)), 0, 63).astype(np.int64)
-    brick = S.morton_encode(g[:, 0], g[:, 1], g[:, 2]) >> 6
+    cell = S.morton_encode(g[:, 0], g[:, 1], g[:, 2])
+    brick = cell >> 6
     assert np.array_equal(np.repeat(ids, np.diff(starts)), brick[pids])
+    # inside a brick the particles are in cell order
+    assert np.all(np.diff(cell[pids].astype(np.int64)) >= 0)
 
 
 @pytest.mark.parametrize("make,n", [(S.shear_block, 100), (S.multimaterial, 60)], ids=["elastic_shear", "multimaterial"])

@@ -103,7 +103,7 @@ def test_host_changes_between_replays():
     pos = np.concatenate([rng.uniform(0.4, 0.6, (500, 3)), np.full((500, 1), vp)], 1).astype(np.float32)
     vel = np.zeros((500, 4), np.float32)
     both(lambda e: e.appendParticles(pos, vel))                              # live count
-    both(lambda e: e.set_launch_config({"fused_threads": 128}))              # launch shape
+    both(lambda e: e.set_launch_config({"fused_threads": 192}))              # launch shape
     both(lambda e: setattr(e, "numSubsteps", 6), step_dt=dt * 6)             # substep count
     a.sync()
     b.sync()
