@@ -460,6 +460,14 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 constexpr int kRow = 9;         // float4 per input row: 3 axes x 3 offsets (see p2gRow)
 constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
+// A tile plane (one of mass, mom.x, mom.y, mom.z) stores node (x, y, z) at
+// x + 11 y + 89 z: with strides 11 and 89 (3 and 25 modulo the 32 banks) the
+// 27 nodes of any 3x3x3 stencil in the tile fall into 27 different banks, so
+// a warp's shared-memory reductions over a stencil never conflict (with the
+// dense 8 / 64 strides the three z-layers of a stencil share 9 banks).
+constexpr int kTileSy = 11, kTileSz = 89;
+constexpr int kTilePlane = 7 * kTileSz + 7 * kTileSy + 8;  // 708 floats
+__device__ __forceinline__ int tileIndex(int x, int y, int z) { return x + kTileSy * y + kTileSz * z; }
 
 constexpr uint32_t kNoRow = 0x7FFFu;     // end of a cell's list
 constexpr uint32_t kExactRow = 0x8000u;  // next[] flag: this row is in the exact form (see p2gRow)
@@ -475,7 +483,7 @@ struct P2GSmemT {
   static constexpr int kChunk = CHUNK;
   static constexpr int kWarps = CHUNK / 32;
   float4 rows[CHUNK * kRow];
-  float tiles[kTileCopies * 4 * kTileNodes];
+  float tiles[kTileCopies * 4 * kTilePlane];
   uint32_t head[kCellSlots];   // first row of each cell's list (kNoRow: empty)
   uint16_t next[CHUNK];        // next row of the same cell, | kExactRow when the row is in the exact form
   float mass[CHUNK];           // the particle mass of an exact-form row
@@ -506,7 +514,7 @@ constexpr uint32_t kNoKey = 0xFFFFFFFFu;  // a lane with no row for the warp's P
 template <bool FLIP, int THREADS>
 struct FusedSmem {
   float4 rows[THREADS * kRow];  // P2G input rows; warp w owns rows [32 w, 32 w + 32)
-  float tiles[4 * kTileNodes];  // the item's 8^3 accumulation tile (mass, mom.x, mom.y, mom.z planes)
+  float tiles[4 * kTilePlane];  // the item's 8^3 accumulation tile (mass, mom.x, mom.y, mom.z planes; tileIndex)
   float mass[THREADS];          // the particle mass of an exact-form row
   float4 v[216];                // staged 6^3 node block (v, mass)
   float4 vo[FLIP ? 216 : 1];
@@ -638,7 +646,7 @@ __device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* 
 
 template <class SM>
 __device__ __forceinline__ void p2gZeroTiles(SM& sm) {
-  for (int q = threadIdx.x; q < kTileCopies * 4 * kTileNodes; q += blockDim.x) sm.tiles[q] = 0.f;
+  for (int q = threadIdx.x; q < kTileCopies * 4 * kTilePlane; q += blockDim.x) sm.tiles[q] = 0.f;
   for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.head[q] = kNoRow;
   if (threadIdx.x < 2) sm.numCells[threadIdx.x] = 0u;
   if (threadIdx.x == 0) sm.markMask = 0u;
@@ -654,7 +662,7 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
   const int cr = int(P.cubeRes);
-  float* tile = sm.tiles + (kTileCopies == 1 ? 0 : warp) * 4 * kTileNodes;
+  float* tile = sm.tiles + (kTileCopies == 1 ? 0 : warp) * 4 * kTilePlane;
   const uint32_t numCells = sm.numCells[par];
   // a tile wholly inside the grid needs no per-node bounds test
   const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
@@ -675,17 +683,17 @@ __device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_
         else p2gNodeTerm(sm.rows + j * kRow, dx, dy, dz, a);
         j = link & ~kExactRow;
       }
-      const int t = (lz * 8 + ly) * 8 + lx;
+      const int t = tileIndex(lx, ly, lz);
       if (kTileCopies == 1) {
         atomicAdd(tile + t, a[3]);
-        atomicAdd(tile + kTileNodes + t, a[0]);
-        atomicAdd(tile + 2 * kTileNodes + t, a[1]);
-        atomicAdd(tile + 3 * kTileNodes + t, a[2]);
+        atomicAdd(tile + kTilePlane + t, a[0]);
+        atomicAdd(tile + 2 * kTilePlane + t, a[1]);
+        atomicAdd(tile + 3 * kTilePlane + t, a[2]);
       } else {
         tile[t] += a[3];
-        tile[kTileNodes + t] += a[0];
-        tile[2 * kTileNodes + t] += a[1];
-        tile[3 * kTileNodes + t] += a[2];
+        tile[kTilePlane + t] += a[0];
+        tile[2 * kTilePlane + t] += a[1];
+        tile[3 * kTilePlane + t] += a[2];
       }
     }
     __syncwarp();
@@ -703,17 +711,18 @@ __device__ __forceinline__ void p2gFlush(const SubstepParams& P, SM& sm, int tx,
   const int cr = int(P.cubeRes);
   for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
     float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+    const int i = tileIndex(q & 7, (q >> 3) & 7, q >> 6);
 #pragma unroll
     for (int w = 0; w < kTileCopies; ++w) {
-      float* t = sm.tiles + w * 4 * kTileNodes;
-      m += t[q];
-      mx += t[kTileNodes + q];
-      my += t[2 * kTileNodes + q];
-      mz += t[3 * kTileNodes + q];
-      t[q] = 0.f;
-      t[kTileNodes + q] = 0.f;
-      t[2 * kTileNodes + q] = 0.f;
-      t[3 * kTileNodes + q] = 0.f;
+      float* t = sm.tiles + w * 4 * kTilePlane + i;
+      m += t[0];
+      mx += t[kTilePlane];
+      my += t[2 * kTilePlane];
+      mz += t[3 * kTilePlane];
+      t[0] = 0.f;
+      t[kTilePlane] = 0.f;
+      t[2 * kTilePlane] = 0.f;
+      t[3 * kTilePlane] = 0.f;
     }
     if (m == 0.f && mx == 0.f && my == 0.f && mz == 0.f) continue;
     const int nx = tx + (q & 7), ny = ty + ((q >> 3) & 7), nz = tz + (q >> 6);
@@ -980,11 +989,11 @@ __device__ __forceinline__ void p2gWarpGroups(const SubstepParams& P, const floa
           else p2gNodeTerm(wrows + j * kRow, dx, dy, dz, a);
         }
       }
-      const int t = (lz * 8 + ly) * 8 + lx;
+      const int t = tileIndex(lx, ly, lz);
       atomicAdd(tile + t, a[3]);
-      atomicAdd(tile + kTileNodes + t, a[0]);
-      atomicAdd(tile + 2 * kTileNodes + t, a[1]);
-      atomicAdd(tile + 3 * kTileNodes + t, a[2]);
+      atomicAdd(tile + kTilePlane + t, a[0]);
+      atomicAdd(tile + 2 * kTilePlane + t, a[1]);
+      atomicAdd(tile + 3 * kTilePlane + t, a[2]);
     }
   }
   __syncwarp();  // every lane has read the rows before they are written again
@@ -1102,7 +1111,7 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS) k_g2p2g(SubstepParams 
   const uint32_t numPB = B.counters[kCntNumPB];
   const uint32_t numItems = numPB * split;
   // The tile starts zeroed here and is left so by every item's flush.
-  for (int q = threadIdx.x; q < 4 * kTileNodes; q += THREADS) S.tiles[q] = 0.f;
+  for (int q = threadIdx.x; q < 4 * kTilePlane; q += THREADS) S.tiles[q] = 0.f;
   // the claim alternates between two slots: a thread may claim the next item
   // while others still read this one, never two ahead (one barrier per claim)
   for (uint32_t it = 0;; it ^= 1u) {
