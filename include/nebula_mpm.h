@@ -332,7 +332,8 @@ int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
  * round); fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the
  * fused and grid-update kernels (0 = as many as fit; larger values are capped
  * at that); grid_batch: grid nodes per thread per round (2 or 4); fused_split:
- * work items per particle brick of the fused kernel (1-4, 0 = the default 1):
+ * work items per particle brick of the fused kernel (1-4; 0, the default: 2 for
+ * scenes of up to 65,536 particles, else 1):
  * 1 keeps a brick in one CTA, k > 1 cuts its slots into k contiguous parts
  * handled by k CTAs (more parallel items for scenes with few bricks, one
  * staging and one tile flush per item).  Every shape

@@ -44,7 +44,7 @@ class LaunchShape:
     fused_ctas_per_sm: int = 0  # 0 = as many as fit
     grid_ctas_per_sm: int = 0
     grid_batch: int = 4
-    fused_split: int = 1  # fused-kernel items per particle brick
+    fused_split: int = 0  # fused-kernel items per particle brick (0 = by scene size)
 
     def to_c(self) -> _capi.LaunchConfig:
         return _capi.LaunchConfig(int(self.fused_threads), int(self.fused_ctas_per_sm), int(self.grid_ctas_per_sm), int(self.grid_batch),
@@ -101,7 +101,7 @@ def fused_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:
 
 
 def split_candidates(base: LaunchShape) -> list[LaunchShape]:
-    return [replace(base, fused_split=k) for k in (1, 2, 3, 4)]
+    return [replace(base, fused_split=k) for k in (0, 1, 2, 3, 4)]  # 0: the engine's choice by scene size
 
 
 def grid_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:

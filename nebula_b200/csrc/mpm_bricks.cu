@@ -1355,7 +1355,12 @@ template <bool BATCH, int THREADS>
 cudaError_t launchFusedShape(bool flip, int modelSet, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur,
                              const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g,
                              float dtStress, uint32_t* err, int numSMs, cudaStream_t s) {
-  const uint32_t k = lc.fusedCtasPerSm, sp = std::max(lc.fusedSplit, 1u);
+  // parts per brick by scene size when not set: scenes of up to 2^16 particles
+  // have too few bricks to fill the GPU with one item per brick (50,000
+  // particles on 64^3: 40.8 us per substep with two parts, 51.9 with one),
+  // larger ones lose to the second staging and flush (80,000 particles: 71.6 /
+  // 95.8 us; 1M: 292 / 390 us per launch)
+  const uint32_t k = lc.fusedCtasPerSm, sp = lc.fusedSplit ? lc.fusedSplit : (n <= (1u << 16) ? 2u : 1u);
   if (flip) return launchFused<true, BATCH, THREADS, kModelsAny>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
   if constexpr (!BATCH) {
     if (modelSet == kModelsElastic)

@@ -70,7 +70,7 @@ struct LaunchConfig {
   uint32_t fusedCtasPerSm = 0;  // persistent k_g2p2g CTAs per SM
   uint32_t gridCtasPerSm = 0;   // persistent grid-update CTAs per SM
   uint32_t gridBatch = 4;       // k_grid_bricks nodes per thread per round: 2 or 4
-  uint32_t fusedSplit = 1;      // k_g2p2g items per particle brick (1-4): contiguous parts of a brick's slots
+  uint32_t fusedSplit = 0;      // k_g2p2g items per particle brick (1-4): contiguous parts of a brick's slots; 0 = by scene size
 };
 // Most CTAs per SM (occupancy) of each variant: [fusedThreads == 256], [gridBatch == 4].
 struct LaunchLimits {

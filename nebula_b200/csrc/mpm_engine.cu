@@ -336,7 +336,7 @@ void validateLaunchConfig(const LaunchConfig& c) {
   if (c.fusedThreads != 192 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 192 or 256");
   if (c.gridBatch != 2 && c.gridBatch != 4) throw Error(NEBULA_MPM_ERR_INVALID, "grid_batch must be 2 or 4");
   if (c.fusedCtasPerSm > 64 || c.gridCtasPerSm > 64) throw Error(NEBULA_MPM_ERR_INVALID, "CTAs per SM must be <= 64 (0 = as many as fit)");
-  if (c.fusedSplit < 1 || c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 1-4 (0 = 1)");
+  if (c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 0-4 (0 = by scene size)");
 }
 
 LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
@@ -345,7 +345,7 @@ LaunchConfig fromAbi(const nebula_mpm_launch_config& c) {
   l.fusedCtasPerSm = c.fused_ctas_per_sm;
   l.gridCtasPerSm = c.grid_ctas_per_sm;
   l.gridBatch = c.grid_batch;
-  l.fusedSplit = c.fused_split == 0 ? 1u : c.fused_split;
+  l.fusedSplit = c.fused_split;
   return l;
 }
 

@@ -19,7 +19,7 @@ def test_candidates_stay_within_occupancy():
     assert all(s.fused_threads == 192 for s in g)
     assert {(s.grid_batch, s.grid_ctas_per_sm) for s in g} == {(4, 0), (4, 4), (4, 2), (2, 0), (2, 4), (2, 2)}
     sp = A.split_candidates(A.LaunchShape(fused_threads=192, fused_ctas_per_sm=3))
-    assert [s.fused_split for s in sp] == [1, 2, 3, 4] and all(s.fused_ctas_per_sm == 3 for s in sp)
+    assert [s.fused_split for s in sp] == [0, 1, 2, 3, 4] and all(s.fused_ctas_per_sm == 3 for s in sp)
     one = A.Limits(fused=(1, 1), grid=(1, 1))
     assert len(A.fused_candidates(A.LaunchShape(), one)) == 2 and len(A.grid_candidates(A.LaunchShape(), one)) == 2
 
@@ -31,7 +31,7 @@ def cost(s):
     c += {0: 0.5, 3: 0.0, 2: 0.3, 1: 2.0}[s.fused_ctas_per_sm]
     c += 0.0 if s.grid_batch == 2 else 0.1
     c += {0: 0.2, 4: 0.0, 2: 0.05, 8: 0.3}[s.grid_ctas_per_sm]
-    c += {1: 0.4, 2: 0.1, 3: 0.0, 4: 0.05}[s.fused_split]
+    c += {0: 0.3, 1: 0.4, 2: 0.1, 3: 0.0, 4: 0.05}[s.fused_split]
     return c
 
 
@@ -58,7 +58,7 @@ def test_descent_finds_the_cheapest_shape_and_caches_it(tmp_path):
     d = json.loads(path.read_text())
     assert set(d["entries"]) == {"gpu|k", "gpu|other"}
     assert d["entries"]["gpu|other"]["shape"] == {"fused_threads": 256, "fused_ctas_per_sm": 0, "grid_ctas_per_sm": 0, "grid_batch": 4,
-                                                  "fused_split": 1}
+                                                  "fused_split": 0}
     best3, rep3 = A.tune(lambda s: 1.0 if s == A.LaunchShape() else 2.0, "gpu|k", LIM, path, force=True)
     assert best3 == A.LaunchShape() and rep3["source"] == "measured"
 
@@ -77,6 +77,6 @@ def test_keys_and_shape_conversions(tmp_path, monkeypatch):
     s = A.LaunchShape(192, 4, 2, 2, 3)
     assert A.LaunchShape.from_c(s.to_c()) == s
     assert A.LaunchShape.coerce({"fused_threads": 192, "fused_ctas_per_sm": 4, "grid_ctas_per_sm": 2, "grid_batch": 2, "fused_split": 3}) == s
-    assert A.LaunchShape.coerce({"fused_threads": 192}).fused_split == 1
+    assert A.LaunchShape.coerce({"fused_threads": 192}).fused_split == 0
     monkeypatch.setenv(A.CACHE_ENV, str(tmp_path / "x.json"))
     assert A.cache_path() == tmp_path / "x.json"
