@@ -71,6 +71,57 @@ struct VelGrid {
   }
 };
 
+// Node box of one substep's P2G: every node a particle stencil touched lies in
+// [lo, hi] (per axis, inclusive).  lo is stored complemented (~lo), so both
+// halves grow with atomicMax from a zeroed record.
+struct NodeBox {
+  uint32_t loInv[3];
+  uint32_t hi[3];
+  uint32_t pad[2];
+};
+static_assert(sizeof(NodeBox) == 32, "NodeBox");
+
+// Fold the stencil of every particle of the block into box `b` (one atomic
+// per bound per CTA).
+__device__ __forceinline__ void boxAdd(NodeBox* b, bool valid, int cx, int cy, int cz, int cube) {
+  __shared__ uint32_t red[6][kT / 32];
+  uint32_t v[6];
+  v[0] = valid ? ~uint32_t(max(cx - 1, 0)) : 0u;
+  v[1] = valid ? ~uint32_t(max(cy - 1, 0)) : 0u;
+  v[2] = valid ? ~uint32_t(max(cz - 1, 0)) : 0u;
+  v[3] = valid ? uint32_t(min(cx + 1, cube - 1)) : 0u;
+  v[4] = valid ? uint32_t(min(cy + 1, cube - 1)) : 0u;
+  v[5] = valid ? uint32_t(min(cz + 1, cube - 1)) : 0u;
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = max(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k][warp] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    uint32_t m = 0;
+    for (int w = 0; w < kT / 32; ++w) m = max(m, red[threadIdx.x][w]);
+    if (m) atomicMax(threadIdx.x < 3 ? &b->loInv[threadIdx.x] : &b->hi[threadIdx.x - 3], m);
+  }
+}
+
+// The cells of box `b` (an empty box when no particle folded in), visited
+// with a grid-stride loop: fn(Morton code).
+template <class Fn>
+__device__ __forceinline__ void forBox(const NodeBox& b, Fn&& fn) {
+  const int lo[3] = {int(~b.loInv[0]), int(~b.loInv[1]), int(~b.loInv[2])};
+  const int n[3] = {int(b.hi[0]) - lo[0] + 1, int(b.hi[1]) - lo[1] + 1, int(b.hi[2]) - lo[2] + 1};
+  if (b.loInv[0] == 0u || n[0] <= 0 || n[1] <= 0 || n[2] <= 0) return;
+  const uint32_t total = uint32_t(n[0]) * uint32_t(n[1]) * uint32_t(n[2]);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int x = lo[0] + int(i % uint32_t(n[0])), y = lo[1] + int((i / uint32_t(n[0])) % uint32_t(n[1])), z = lo[2] + int(i / (uint32_t(n[0]) * uint32_t(n[1])));
+    fn(mortonEncode(x, y, z));
+  }
+}
+
 // ------------------------------------------------------------------ forward
 __global__ void __launch_bounds__(kT) k_init(const float4* __restrict__ x0, const float4* __restrict__ v0, const float* __restrict__ E, float nu,
                                              uint32_t n, St st, float2* lame) {
@@ -87,28 +138,35 @@ __global__ void __launch_bounds__(kT) k_init(const float4* __restrict__ x0, cons
   lame[p] = make_float2(e / (2.0f * (1.0f + nu)), e * nu / ((1.0f + nu) * (1.0f - 2.0f * nu)));
 }
 
-__global__ void __launch_bounds__(kT) k_fwd_p2g(SubstepParams P, St st, uint32_t n, float4* acc) {
+__global__ void __launch_bounds__(kT) k_fwd_p2g(SubstepParams P, St st, uint32_t n, float4* acc, NodeBox* box) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const PState s = loadState(st.f, p);
-  p2gParticle(P, s, P.dt, [&](int nx, int ny, int nz, float mx, float my, float mz, float m) {
-    redAddV4(acc + mortonEncode(nx, ny, nz), mx, my, mz, m);
-  });
+  int c[3] = {0, 0, 0};
+  if (p < n) {
+    const PState s = loadState(st.f, p);
+    cellCoords(P, s.P.x, s.P.y, s.P.z, c[0], c[1], c[2]);
+    p2gParticle(P, s, P.dt, [&](int nx, int ny, int nz, float mx, float my, float mz, float m) {
+      redAddV4(acc + mortonEncode(nx, ny, nz), mx, my, mz, m);
+    });
+  }
+  boxAdd(box, p < n, c[0], c[1], c[2], int(P.cubeRes));
 }
 
-__global__ void __launch_bounds__(kT) k_fwd_grid(SubstepParams P, const float4* __restrict__ acc, float4* vel, AdjScalars* sc) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= P.hashCells) return;
-  const float4 a = acc[c];
-  int ix, iy, iz;
-  mortonDecode(c, ix, iy, iz);
-  float3 v, vo;
-  const bool ok = gridNode(P, ix, iy, iz, a.w, a.x, a.y, a.z, v, vo);
-  vel[c] = ok ? make_float4(v.x, v.y, v.z, a.w) : make_float4(0.f, 0.f, 0.f, a.w);
-  if (ok) {
-    const float ux = a.x / a.w, uy = a.y / a.w, uz = a.z / a.w;
-    if (sqrtf(ux * ux + uy * uy + uz * uz) > 15.0f) atomicOr(&sc->events, 4u);
-  }
+// Grid update over the substep's node box (G2P reads no node outside it);
+// `clear` zeroes acc behind the read for the next substep's P2G.
+__global__ void __launch_bounds__(kT) k_fwd_grid(SubstepParams P, float4* acc, float4* vel, AdjScalars* sc, const NodeBox* box, int clear) {
+  forBox(*box, [&](uint32_t c) {
+    const float4 a = acc[c];
+    if (clear) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    int ix, iy, iz;
+    mortonDecode(c, ix, iy, iz);
+    float3 v, vo;
+    const bool ok = gridNode(P, ix, iy, iz, a.w, a.x, a.y, a.z, v, vo);
+    vel[c] = ok ? make_float4(v.x, v.y, v.z, a.w) : make_float4(0.f, 0.f, 0.f, a.w);
+    if (ok) {
+      const float ux = a.x / a.w, uy = a.y / a.w, uz = a.z / a.w;
+      if (sqrtf(ux * ux + uy * uy + uz * uz) > 15.0f) atomicOr(&sc->events, 4u);
+    }
+  });
 }
 
 __global__ void __launch_bounds__(kT) k_fwd_g2p(SubstepParams P, St in, St out, const float2* __restrict__ lame, uint32_t n,
@@ -452,10 +510,20 @@ __global__ void __launch_bounds__(kT) k_adj_g2p(SubstepParams P, St st, const fl
 
 // Grid adjoint: v = walls(cap(p/m) + g dt); turns the grid-velocity adjoint
 // into momentum and mass adjoints (p_bar, m_bar), in place.
-__global__ void __launch_bounds__(kT) k_adj_grid(SubstepParams P, const float4* __restrict__ acc, float4* gadj) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= P.hashCells) return;
+// Over the substep's node box (the G2P adjoint scattered into no node outside
+// it, and the P2G adjoint gathers from none).  acc is read for the last time
+// here and cleared behind the read (the segment's next recomputation
+// accumulates into it again); `other` -- the grid adjoint of the next substep
+// back -- is cleared over the box where the substep after this one left it.
+__device__ __forceinline__ void adjGridNode(const SubstepParams& P, float4* acc, float4* gadj, uint32_t c);
+__global__ void __launch_bounds__(kT) k_adj_grid(SubstepParams P, float4* acc, float4* gadj, const NodeBox* box, float4* other,
+                                                 const NodeBox* otherBox) {
+  forBox(*box, [&](uint32_t c) { adjGridNode(P, acc, gadj, c); });
+  if (otherBox) forBox(*otherBox, [&](uint32_t c) { other[c] = make_float4(0.f, 0.f, 0.f, 0.f); });
+}
+__device__ __forceinline__ void adjGridNode(const SubstepParams& P, float4* acc, float4* gadj, uint32_t c) {
   const float4 a = acc[c];
+  acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
   const float m = a.w;
   if (m < 1e-10f) {
     gadj[c] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -640,16 +708,24 @@ AdjointEngine::AdjointEngine(const nebula_mpm_adjoint_config& cfg) : cfg_(cfg) {
   for (auto& b : ck_) b.alloc(stBytes);
   segState_.resize(every_);
   for (uint32_t j = 1; j < every_; ++j) segState_[j].alloc(stBytes);
+  // grids start zeroed and are left so by the grid passes that read them last
   segAcc_.resize(every_);
   segVel_.resize(every_);
   for (uint32_t j = 0; j < every_; ++j) {
     segAcc_[j].alloc(gBytes);
     segVel_[j].alloc(gBytes);
+    check(cudaMemset(segAcc_[j].ptr, 0, gBytes), "cudaMemset");
   }
   acc_.alloc(gBytes);
   vel_.alloc(gBytes);
+  check(cudaMemset(acc_.ptr, 0, gBytes), "cudaMemset");
   for (auto& b : adj_) b.alloc(size_t(11) * n_ * sizeof(float4));
-  gadj_.alloc(gBytes);
+  for (auto& g : gadj_) g.alloc(gBytes);
+  boxes_.alloc(size_t(std::max(cfg.substeps, 1u)) * sizeof(NodeBox));
+  check(cudaMemset(boxes_.ptr, 0, boxes_.bytes), "cudaMemset");
+  int sms = 0;
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "cudaDeviceGetAttribute");
+  gridBlocks_ = uint32_t(std::max(sms, 1)) * 2u;  // grid-stride over a node box
   mub_.alloc(size_t(n_) * sizeof(float));
   lamb_.alloc(size_t(n_) * sizeof(float));
   finalBuf_ = int(cfg.substeps & 1u);
@@ -676,16 +752,18 @@ void AdjointEngine::setGraphs(bool on) {
   useGraphs_ = on;
 }
 
-void AdjointEngine::substepForward(const float4* const* in, float4* const* out, float4* acc, float4* vel, cudaStream_t s) {
+// One forward substep into grid buffers acc (zero on entry) and vel; the P2G's
+// node box goes to box[k].  clear: zero acc behind the grid update's read.
+void AdjointEngine::substepForward(const float4* const* in, float4* const* out, float4* acc, float4* vel, uint32_t k, bool clear, cudaStream_t s) {
   St si, so;
-  for (int k = 0; k < 8; ++k) {
-    si.f[k] = const_cast<float4*>(in[k]);
-    so.f[k] = out ? out[k] : nullptr;
+  for (int q = 0; q < 8; ++q) {
+    si.f[q] = const_cast<float4*>(in[q]);
+    so.f[q] = out ? out[q] : nullptr;
   }
   AdjScalars* sc = static_cast<AdjScalars*>(scal_.ptr);
-  check(cudaMemsetAsync(acc, 0, size_t(nc_) * sizeof(float4), s), "memset grid");
-  k_fwd_p2g<<<blocks(n_), kT, 0, s>>>(P_, si, n_, acc);
-  k_fwd_grid<<<blocks(nc_), kT, 0, s>>>(P_, acc, vel, sc);
+  NodeBox* box = static_cast<NodeBox*>(boxes_.ptr) + k;
+  k_fwd_p2g<<<blocks(n_), kT, 0, s>>>(P_, si, n_, acc, box);
+  k_fwd_grid<<<gridBlocks_, kT, 0, s>>>(P_, acc, vel, sc, box, clear ? 1 : 0);
   launches_ += 2;
   if (out) {
     k_fwd_g2p<<<blocks(n_), kT, 0, s>>>(P_, si, so, static_cast<const float2*>(lame_.ptr), n_, vel, sc);
@@ -699,6 +777,7 @@ void AdjointEngine::forwardBody(cudaStream_t s) {
   AdjScalars* sc = static_cast<AdjScalars*>(scal_.ptr);
   check(cudaMemsetAsync(sc, 0, offsetof(AdjScalars, target), s), "memset com");
   check(cudaMemsetAsync(&sc->events, 0, sizeof(uint32_t), s), "memset events");
+  check(cudaMemsetAsync(boxes_.ptr, 0, size_t(cfg_.substeps) * sizeof(NodeBox), s), "memset boxes");
   St s0 = stPtrs(ping_[0], n_);
   k_init<<<blocks(n_), kT, 0, s>>>(static_cast<const float4*>(x0_.ptr), static_cast<const float4*>(v0_.ptr), static_cast<const float*>(E_.ptr),
                                    cfg_.nu, n_, s0, static_cast<float2*>(lame_.ptr));
@@ -708,7 +787,7 @@ void AdjointEngine::forwardBody(cudaStream_t s) {
   for (uint32_t k = 0; k < cfg_.substeps; ++k) {
     if (k % every_ == 0) check(cudaMemcpyAsync(ck_[k / every_].ptr, ping_[cur].ptr, stBytes, cudaMemcpyDeviceToDevice, s), "checkpoint");
     St a = stPtrs(ping_[cur], n_), b = stPtrs(ping_[cur ^ 1], n_);
-    substepForward(a.f, b.f, static_cast<float4*>(acc_.ptr), static_cast<float4*>(vel_.ptr), s);
+    substepForward(a.f, b.f, static_cast<float4*>(acc_.ptr), static_cast<float4*>(vel_.ptr), k, true, s);
     cur ^= 1;
   }
   St fin = stPtrs(ping_[cur], n_);
@@ -724,29 +803,37 @@ void AdjointEngine::backwardBody(cudaStream_t s) {
   check(cudaMemsetAsync(mub_.ptr, 0, size_t(n_) * sizeof(float), s), "memset");
   check(cudaMemsetAsync(lamb_.ptr, 0, size_t(n_) * sizeof(float), s), "memset");
   check(cudaMemsetAsync(adj_[0].ptr, 0, adjBytes, s), "memset");
+  // the grid adjoints start zeroed; each reverse substep then clears the other
+  // buffer over the box the substep after it left dirty
+  for (auto& g : gadj_) check(cudaMemsetAsync(g.ptr, 0, size_t(nc_) * sizeof(float4), s), "memset grid adjoint");
+  NodeBox* boxes = static_cast<NodeBox*>(boxes_.ptr);
   int o = 0;
   k_adj_seed<<<blocks(n_), kT, 0, s>>>(static_cast<const float4*>(x0_.ptr), cfg_.rho0, n_, sc, adjPtrs(adj_[o], n_));
   ++launches_;
   const float2* lame = static_cast<const float2*>(lame_.ptr);
   float* mub = static_cast<float*>(mub_.ptr);
   float* lamb = static_cast<float*>(lamb_.ptr);
-  float4* gadj = static_cast<float4*>(gadj_.ptr);
   for (int seg = int(segs_) - 1; seg >= 0; --seg) {
     const uint32_t k0 = uint32_t(seg) * every_, k1 = std::min(cfg_.substeps, k0 + every_), len = k1 - k0;
     auto stateOf = [&](uint32_t j) { return j == 0 ? stPtrs(ck_[seg], n_) : stPtrs(segState_[j], n_); };
-    // recompute the segment, keeping every substep's input state and grid
+    // recompute the segment, keeping every substep's input state, grid and node box
+    check(cudaMemsetAsync(boxes + k0, 0, size_t(len) * sizeof(NodeBox), s), "memset boxes");
     for (uint32_t j = 0; j < len; ++j) {
       St in = stateOf(j);
       St out = j + 1 < len ? stateOf(j + 1) : St{};
-      substepForward(in.f, j + 1 < len ? out.f : nullptr, static_cast<float4*>(segAcc_[j].ptr), static_cast<float4*>(segVel_[j].ptr), s);
+      substepForward(in.f, j + 1 < len ? out.f : nullptr, static_cast<float4*>(segAcc_[j].ptr), static_cast<float4*>(segVel_[j].ptr), k0 + j,
+                     false, s);
     }
     // reverse the segment
     for (int j = int(len) - 1; j >= 0; --j) {
       St st = stateOf(uint32_t(j));
       AdjPtrs ob = adjPtrs(adj_[o], n_), ib = adjPtrs(adj_[o ^ 1], n_);
-      check(cudaMemsetAsync(gadj, 0, size_t(nc_) * sizeof(float4), s), "memset grid adjoint");
+      const uint32_t k = k0 + uint32_t(j);
+      float4* gadj = static_cast<float4*>(gadj_[k & 1u].ptr);
+      float4* other = static_cast<float4*>(gadj_[(k + 1u) & 1u].ptr);
+      const NodeBox* otherBox = k + 1u < cfg_.substeps ? boxes + k + 1u : nullptr;
       k_adj_g2p<<<blocks(n_), kT, 0, s>>>(P_, st, lame, n_, static_cast<const float4*>(segVel_[j].ptr), ob, ib, gadj, mub, lamb);
-      k_adj_grid<<<blocks(nc_), kT, 0, s>>>(P_, static_cast<const float4*>(segAcc_[j].ptr), gadj);
+      k_adj_grid<<<gridBlocks_, kT, 0, s>>>(P_, static_cast<float4*>(segAcc_[j].ptr), gadj, boxes + k, other, otherBox);
       k_adj_p2g<<<blocks(n_), kT, 0, s>>>(P_, st, n_, gadj, ib);
       launches_ += 3;
       o ^= 1;

@@ -42,7 +42,7 @@ class AdjointEngine {
   void bindDevice() const;
   void forwardBody(cudaStream_t s);
   void backwardBody(cudaStream_t s);
-  void substepForward(const float4* const* in, float4* const* out, float4* acc, float4* vel, cudaStream_t s);
+  void substepForward(const float4* const* in, float4* const* out, float4* acc, float4* vel, uint32_t k, bool clear, cudaStream_t s);
   void run(bool fwd, cudaStream_t s);
 
   nebula_mpm_adjoint_config cfg_;
@@ -59,7 +59,9 @@ class AdjointEngine {
   std::vector<DevBuf> segAcc_, segVel_;  // grids of the segment's substeps
   DevBuf acc_, vel_;               // forward grid scratch
   DevBuf adj_[2];                  // adjoint state: x, v ([n] float4), B, F, T ([3n] float4 rows each)
-  DevBuf gadj_;                    // grid adjoint [nc] float4
+  DevBuf gadj_[2];                 // grid adjoint [nc] float4, alternating by substep
+  DevBuf boxes_;                   // per substep: the P2G's node box (NodeBox, mpm_adjoint.cu)
+  uint32_t gridBlocks_ = 1;        // CTAs of the grid passes (grid-stride over a node box)
   DevBuf mub_, lamb_;              // per-particle accumulated adjoints of mu, lambda
   bool haveForward_ = false;
   bool useGraphs_ = true;
