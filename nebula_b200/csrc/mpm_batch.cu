@@ -210,7 +210,7 @@ void BatchEngine::normalizeOrder(cudaStream_t st) {
 
 void BatchEngine::discardPending(cudaStream_t st) {
   if (!pending_) return;
-  check(launchClearBricks(brickBuffers(), gridBuffers(), numSMs_, st, &launches_), "clear bricks");
+  check(launchClearBricks(brickBuffers(cur_), gridBuffers(), numSMs_, st, &launches_), "clear bricks");
   pending_ = false;
 }
 
@@ -274,12 +274,12 @@ void BatchEngine::seal() {
   check(cudaMemset(gridAcc_.ptr, 0, gridAcc_.bytes), "cudaMemset");
   check(cudaMemset(gridVel_.ptr, 0, gridVel_.bytes), "cudaMemset");
   tiles_ = (nbTotal_ + kBrickScanTile - 1) / kBrickScanTile;
-  for (DevBuf* b : {&bCount_, &bFlag_, &pbBrick_, &gbBrick_}) {
+  for (DevBuf* b : {&bCount_, &bFlag_, &bStart_, &pbBrick_, &gbBrick_}) {
     b->alloc(size_t(nbTotal_) * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
-  // per-cell counts (kept zeroed between binnings) and starts of the in-brick cell order
-  for (DevBuf* b : {&cCount_, &cStart_}) {
+  // per-cell counts of two binnings (each cleared by the fused kernel after the one that follows it)
+  for (DevBuf* b : {&cCount_[0], &cCount_[1]}) {
     b->alloc(size_t(nbTotal_) * 64u * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
@@ -304,14 +304,16 @@ void BatchEngine::seal() {
   tablesDirty_ = true;
 }
 
-BrickBuffers BatchEngine::brickBuffers() {
+// q: the buffer whose state the binning describes (its counts are array q).
+BrickBuffers BatchEngine::brickBuffers(int q) {
   BrickBuffers b;
   b.nb = nbTotal_;
   b.tiles = tiles_;
   b.brickCount = static_cast<uint32_t*>(bCount_.ptr);
   b.brickFlag = static_cast<uint32_t*>(bFlag_.ptr);
-  b.cellCount = static_cast<uint32_t*>(cCount_.ptr);
-  b.cellStart = static_cast<uint32_t*>(cStart_.ptr);
+  b.brickStart = static_cast<uint32_t*>(bStart_.ptr);
+  b.cellCount = static_cast<uint32_t*>(cCount_[q & 1].ptr);
+  b.cellPrev = static_cast<uint32_t*>(cCount_[(q & 1) ^ 1].ptr);
   b.pbBrick = static_cast<uint32_t*>(pbBrick_.ptr);
   b.pbStart = static_cast<uint32_t*>(pbStart_.ptr);
   b.gbBrick = static_cast<uint32_t*>(gbBrick_.ptr);
@@ -445,9 +447,11 @@ void BatchEngine::uploadTables(float subDt, uint32_t substeps, cudaStream_t st) 
 // ------------------------------------------------------------------ substeps
 void BatchEngine::buildPending(cudaStream_t st) {
   const SceneTable T = table();
-  BrickBuffers B = brickBuffers();
+  BrickBuffers B = brickBuffers(cur_);
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
+  // a binning from scratch: neither count array may hold an earlier binning's counts
+  for (DevBuf& c : cCount_) check(cudaMemsetAsync(c.ptr, 0, c.bytes, st), "clear cell counts");
   check(launchBrickCountBatch(T, statePtrs(cur_).f[0], live_, B, st, &launches_), "brick count");
   check(launchBrickScan(B, err, st, &launches_), "brick scan");
   check(launchPermScatter(B, live_, err, st, &launches_), "perm scatter");
@@ -457,17 +461,18 @@ void BatchEngine::buildPending(cudaStream_t st) {
 
 void BatchEngine::substep(uint32_t k, cudaStream_t st) {
   const SceneTable T = table();
-  BrickBuffers B = brickBuffers();
+  // the binning of the state read (buffer cur_) and of the state written
+  const BrickBuffers B = brickBuffers(cur_), Bn = brickBuffers(cur_ ^ 1);
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   const bool fold = live_ < kFoldScatterMax;
   check(launchGridBricksBatch(T, k, B, G, fold ? live_ : 0u, err, launchCfg_, numSMs_, st, &launches_), "grid bricks");
   check(launchG2P2GBatch(T, G.vold != nullptr, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
-                         static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, err, launchCfg_, numSMs_, st, &launches_),
+                         static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, Bn, G, err, launchCfg_, numSMs_, st, &launches_),
         "g2p2g");
-  check(launchBrickScan(B, err, st, &launches_), "brick scan");
+  check(launchBrickScan(Bn, err, st, &launches_), "brick scan");
   // the permutation of this binning: here, or by the next grid launch
-  if (!fold) check(launchPermScatter(B, live_, err, st, &launches_), "perm scatter");
+  if (!fold) check(launchPermScatter(Bn, live_, err, st, &launches_), "perm scatter");
   cur_ ^= 1;
   permuted_ = true;
 }

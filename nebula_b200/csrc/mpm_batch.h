@@ -71,7 +71,7 @@ class BatchEngine {
   void substep(uint32_t k, cudaStream_t st);
   bool anyFlip() const;
   StatePtrs statePtrs(int buf);
-  BrickBuffers brickBuffers();
+  BrickBuffers brickBuffers(int q);
   GridBuffers gridBuffers();
   SceneTable table() const;
   void clearGraphs();
@@ -90,7 +90,7 @@ class BatchEngine {
   int cur_ = 0;
   bool permuted_ = false;
   DevBuf gridAcc_, gridVel_, gridVold_;
-  DevBuf bCount_, bFlag_, cCount_, cStart_, pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_, err_;
+  DevBuf bCount_, bFlag_, bStart_, cCount_[2], pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_, err_;
   uint32_t tiles_ = 1;
   // device tables
   DevBuf tParams_, tBrickBase_, tPartBase_, tMaterials_, tForces_, tTrack_;

@@ -361,10 +361,13 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   uint32_t rc = s_prefix[0] + (warp > 0 ? s_warp[0][warp - 1] : 0u) + ic - sc;
   uint32_t rp = s_prefix[1] + (warp > 0 ? s_warp[1][warp - 1] : 0u) + ip - sp;
   uint32_t rg = s_prefix[2] + (warp > 0 ? s_warp[2][warp - 1] : 0u) + ig - sg;
+  uint32_t starts[kBrickScanItems];
 #pragma unroll
   for (int k = 0; k < kBrickScanItems; ++k) {
     const uint32_t b = b0 + k;
+    starts[k] = rc;
     if (b < B.nb) {
+      if (!full) B.brickStart[b] = rc;
       if (cnt[k]) {
         B.pbBrick[rp] = b;
         B.pbStart[rp] = rc;
@@ -377,6 +380,11 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
     }
     rc += cnt[k];
   }
+  if (full) {
+    uint4* ps = reinterpret_cast<uint4*>(B.brickStart + b0);
+    ps[0] = make_uint4(starts[0], starts[1], starts[2], starts[3]);
+    ps[1] = make_uint4(starts[4], starts[5], starts[6], starts[7]);
+  }
   if (tile == B.tiles - 1 && threadIdx.x == 0) {
     // the last tile's look-back finished, so all three totals are final
     const uint32_t npb = s_prefix[1] + s_warp[1][WL];
@@ -386,65 +394,55 @@ __global__ void __launch_bounds__(kBrickScanThreads) k_brick_scan(BrickBuffers B
   }
 }
 
-// Cell starts of every listed particle brick: one warp per brick scans its 64
-// cell counts (two per lane) from the brick's first slot, and clears the
-// counts for the next binning.
-__global__ void __launch_bounds__(kThreads) k_cell_scan(BrickBuffers B) {
-  waitForPredecessorGrid();
-  const uint32_t numPB = B.counters[kCntNumPB];
+// Sorted slots of the buffer indices t of one warp (every lane calls it; `valid`
+// per lane): the start of the particle's brick, plus the counts of the cells
+// of the brick below its cell, plus its rank in its cell.  The lanes' keys
+// come in a few bricks (the buffer holds particles in cell order), and for
+// each distinct brick the warp reads its 64 counts once (two per lane) and
+// scans them.
+__device__ __forceinline__ void permScatterWarp(const BrickBuffers& B, uint32_t n, uint32_t* err, uint32_t t, bool valid) {
   const uint32_t lane = laneId();
-  const uint32_t warps = gridDim.x * (kThreads / 32);
-  for (uint32_t e = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); e < numPB; e += warps) {
-    const uint32_t b = B.pbBrick[e], start = B.pbStart[e];
-    uint2* pc = reinterpret_cast<uint2*>(B.cellCount + (size_t(b) << 6)) + lane;
-    const uint2 c = *pc;
-    *pc = make_uint2(0u, 0u);
+  const uint32_t key = valid ? B.binKey[t] : 0u;
+  const uint32_t rank = valid ? B.binRank[t] : 0u;
+  const uint32_t brick = key >> 6, cell = key & 63u;
+  const uint32_t start = valid ? B.brickStart[brick] : 0u;
+  uint32_t below = 0;
+  uint32_t pending = __ballot_sync(0xffffffffu, valid);
+  while (pending) {
+    const uint32_t b = __shfl_sync(0xffffffffu, brick, __ffs(pending) - 1);
+    const uint2 c = reinterpret_cast<const uint2*>(B.cellCount + (size_t(b) << 6))[lane];
     uint32_t incl = c.x + c.y;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= uint32_t(o)) incl += y;
     }
-    const uint32_t first = start + incl - c.x - c.y;
-    reinterpret_cast<uint2*>(B.cellStart + (size_t(b) << 6))[lane] = make_uint2(first, first + c.x);
+    const uint32_t pairBelow = __shfl_sync(0xffffffffu, incl - c.x - c.y, cell >> 1);
+    const uint32_t evenCount = __shfl_sync(0xffffffffu, c.x, cell >> 1);
+    const bool mine = valid && brick == b;
+    if (mine) below = pairBelow + ((cell & 1u) ? evenCount : 0u);
+    pending &= ~__ballot_sync(0xffffffffu, mine);
+  }
+  if (valid) {
+    const uint32_t slot = start + below + rank;
+    if (slot < n) B.perm[slot] = t;
+    else atomicOr(err, kErrBinRange);
   }
 }
 
-// Sorted slot of buffer index t: the start of its cell plus its rank.
-__device__ __forceinline__ void permScatterOne(const BrickBuffers& B, uint32_t n, uint32_t* err, uint32_t t) {
-  const uint32_t slot = B.cellStart[B.binKey[t]] + B.binRank[t];
-  if (slot < n) B.perm[slot] = t;
-  else atomicOr(err, kErrBinRange);
-}
-
-// Scatter of buffer indices t0, t0 + stride, ... < n, four per round with
-// the loads of a round issued before their dependent loads and stores.
+// The same over buffer indices t0, t0 + stride, ... < n (t0 - lane and stride
+// multiples of 32, so the warp's lanes stay together).
 __device__ __forceinline__ void permScatterStrided(const BrickBuffers& B, uint32_t n, uint32_t* err, uint64_t t0, uint64_t stride) {
-  for (uint64_t base = t0; base < n; base += 4 * stride) {
-    uint32_t key[4], rank[4], start[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint64_t t = base + uint64_t(k) * stride;
-      key[k] = t < n ? B.binKey[t] : 0u;
-      rank[k] = t < n ? B.binRank[t] : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) start[k] = base + uint64_t(k) * stride < n ? B.cellStart[key[k]] : 0u;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint64_t t = base + uint64_t(k) * stride;
-      if (t >= n) continue;
-      const uint32_t slot = start[k] + rank[k];
-      if (slot < n) B.perm[slot] = uint32_t(t);
-      else atomicOr(err, kErrBinRange);
-    }
+  for (uint64_t w = t0 - laneId(); w < n; w += stride) {
+    const uint64_t t = w + laneId();
+    permScatterWarp(B, n, err, uint32_t(t < n ? t : 0u), t < n);
   }
 }
 
 __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint32_t n, uint32_t* err) {
   waitForPredecessorGrid();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) permScatterOne(B, n, err, t);
+  permScatterWarp(B, n, err, t < n ? t : 0u, t < n);
 }
 
 // ------------------------------------------------------------------ shared-memory P2G
@@ -1124,6 +1122,9 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS) k_g2p2g(SubstepParams 
     if (i >= numItems) break;
     const uint32_t part = i / numPB, bi = i - part * numPB;
     const uint32_t b = B.pbBrick[bi], bend = min(B.pbStart[bi + 1], n), bstart = min(B.pbStart[bi], bend);
+    // the permutation has read the previous binning's counts of this brick:
+    // clear them for the binning after this one (every part writes the same zeros)
+    if (threadIdx.x < 32) reinterpret_cast<uint2*>(B.cellPrev + (size_t(b) << 6))[threadIdx.x] = make_uint2(0u, 0u);
     const uint32_t len = (bend - bstart + split - 1u) / split;
     const uint32_t start = min(bstart + part * len, bend), end = min(start + len, bend);
     if (start >= end) continue;  // the brick has no particles for this part
@@ -1278,15 +1279,7 @@ cudaError_t launchBrickCountBatch(const SceneTable& T, const float4* pos, uint32
 }
 
 cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches) {
-  cudaError_t e = launchSerialized(k_brick_scan, dim3(b.tiles), dim3(kBrickScanThreads), 0, s, b, err);
-  ++*launches;
-  if (e != cudaSuccess) return e;
-  // one warp per particle brick; at most one brick per particle, so the grid covers min(bricks, particles / 32) warps
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const uint32_t blocks = std::min<uint32_t>(blocksFor(uint64_t(b.nb) * 32u), uint32_t(std::max(sms, 1)) * 4u);
-  e = launchSerialized(k_cell_scan, dim3(blocks), dim3(kThreads), 0, s, b);
+  const cudaError_t e = launchSerialized(k_brick_scan, dim3(b.tiles), dim3(kBrickScanThreads), 0, s, b, err);
   ++*launches;
   return e;
 }

@@ -6,9 +6,9 @@
 //   g2p2g    per particle brick: G2P from the staged grid, particle update,
 //            P2G of the updated particle into a shared tile, binning count
 //   scan     brick counts / marks -> particle-brick list, grid-brick list,
-//            brick starts (single pass, decoupled look-back, compaction),
-//            then per listed particle brick its 64 cell starts
-//   perm     (cell, rank) -> sorted slot of every particle
+//            brick starts (single pass, decoupled look-back, compaction)
+//   perm     (cell, rank) -> sorted slot of every particle: its brick's start
+//            plus the counts of the brick's lower cells plus its rank
 // Particles are physically reordered by cell every substep (bricks in Morton
 // order, the 64 cells of a brick in Morton order; ping-pong state buffers
 // plus the original particle id).
@@ -32,8 +32,13 @@ struct BrickBuffers {
   uint32_t tiles;             // scan tiles over nb
   uint32_t* brickCount;       // [nb] particles per brick (zeroed by the scan)
   uint32_t* brickFlag;        // [nb] grid-active marks (zeroed by the scan)
-  uint32_t* cellCount;        // [64 nb] particles per cell (zeroed by the scan)
-  uint32_t* cellStart;        // [64 nb] first sorted slot of each cell of a particle brick
+  uint32_t* brickStart;       // [nb] first sorted slot of each brick
+  // Per-cell particle counts, two arrays used in turn: the binning of the
+  // state in buffer q counts into array q, the fused kernel that reads that
+  // state (and counts its output into the other array) clears array q brick
+  // by brick as it takes the bricks' items, after the permutation has read it.
+  uint32_t* cellCount;        // [64 nb] the counts of this binning
+  uint32_t* cellPrev;         // [64 nb] the counts of the binning before it (cleared by the fused kernel)
   uint32_t* pbBrick;          // [nb] particle-brick list
   uint32_t* pbStart;          // [nb + 1] first slot of each listed brick; pbStart[numPB] = total
   uint32_t* gbBrick;          // [nb] grid-brick list, ascending (k_brick_scan writes it in brick order)
@@ -82,8 +87,7 @@ LaunchLimits launchLimits(bool flip, bool batch);
 // Standalone binning of the particles in buffer order: counts + stencil marks.
 cudaError_t launchBrickCount(const SubstepParams& P, const float4* pos, uint32_t n, const BrickBuffers& b, uint32_t* err, cudaStream_t s,
                              uint64_t* launches);
-// Compaction scan (tile numbering and status epochs come from a device ticket),
-// then a second launch with the cell starts of every particle brick.
+// Compaction scan (tile numbering and status epochs come from a device ticket).
 cudaError_t launchBrickScan(const BrickBuffers& b, uint32_t* err, cudaStream_t s, uint64_t* launches);
 cudaError_t launchPermScatter(const BrickBuffers& b, uint32_t n, uint32_t* err, cudaStream_t s, uint64_t* launches);
 // P2G of the particles of every listed brick (no binning, no marks).

@@ -103,12 +103,12 @@ MPMEngine::MPMEngine(const nebula_mpm_config& cfg) : cfg_(cfg) {
   gridVel_.alloc(size_t(ncPad_) * sizeof(float4));
   check(cudaMemset(gridAcc_.ptr, 0, gridAcc_.bytes), "cudaMemset");
   check(cudaMemset(gridVel_.ptr, 0, gridVel_.bytes), "cudaMemset");
-  for (DevBuf* b : {&bCount_, &bFlag_, &pbBrick_, &gbBrick_}) {
+  for (DevBuf* b : {&bCount_, &bFlag_, &bStart_, &pbBrick_, &gbBrick_}) {
     b->alloc(size_t(nb_) * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
-  // per-cell counts (kept zeroed between binnings) and starts of the in-brick cell order
-  for (DevBuf* b : {&cCount_, &cStart_}) {
+  // per-cell counts of two binnings (each cleared by the fused kernel after the one that follows it)
+  for (DevBuf* b : {&cCount_[0], &cCount_[1]}) {
     b->alloc(size_t(nb_) * 64u * sizeof(uint32_t));
     check(cudaMemset(b->ptr, 0, b->bytes), "cudaMemset");
   }
@@ -712,14 +712,16 @@ StatePtrs MPMEngine::statePtrs(int buf) {
 }
 StatePtrs MPMEngine::statePtrs() { return statePtrs(cur_); }
 
-BrickBuffers MPMEngine::brickBuffers() {
+// q: the buffer whose state the binning describes (its counts are array q).
+BrickBuffers MPMEngine::brickBuffers(int q) {
   BrickBuffers b;
   b.nb = nb_;
   b.tiles = tiles_;
   b.brickCount = static_cast<uint32_t*>(bCount_.ptr);
   b.brickFlag = static_cast<uint32_t*>(bFlag_.ptr);
-  b.cellCount = static_cast<uint32_t*>(cCount_.ptr);
-  b.cellStart = static_cast<uint32_t*>(cStart_.ptr);
+  b.brickStart = static_cast<uint32_t*>(bStart_.ptr);
+  b.cellCount = static_cast<uint32_t*>(cCount_[q & 1].ptr);
+  b.cellPrev = static_cast<uint32_t*>(cCount_[(q & 1) ^ 1].ptr);
   b.pbBrick = static_cast<uint32_t*>(pbBrick_.ptr);
   b.pbStart = static_cast<uint32_t*>(pbStart_.ptr);
   b.gbBrick = static_cast<uint32_t*>(gbBrick_.ptr);
@@ -799,7 +801,7 @@ void MPMEngine::normalizeOrder(cudaStream_t s) {
 
 void MPMEngine::discardPending(cudaStream_t s) {
   if (!pending_) return;
-  check(launchClearBricks(brickBuffers(), gridBuffers(), numSMs_, s, &launches_), "clear bricks");
+  check(launchClearBricks(brickBuffers(cur_), gridBuffers(), numSMs_, s, &launches_), "clear bricks");
   pending_ = false;
 }
 
@@ -809,11 +811,13 @@ bool MPMEngine::pendingMatches(float subDt) const {
 
 // Bin the current particles (buffer order), then P2G them into the brick grid.
 void MPMEngine::buildPending(const SubstepParams& P, cudaStream_t s) {
-  BrickBuffers B = brickBuffers();
+  BrickBuffers B = brickBuffers(cur_);
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   uint64_t l0 = launches_;
   phaseBegin(kPhaseBin, s);
+  // a binning from scratch: neither count array may hold an earlier binning's counts
+  for (DevBuf& c : cCount_) check(cudaMemsetAsync(c.ptr, 0, c.bytes, s), "clear cell counts");
   check(launchBrickCount(P, statePtrs(cur_).f[0], live_, B, err, s, &launches_), "brick count");
   check(launchBrickScan(B, err, s, &launches_), "brick scan");
   check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
@@ -830,7 +834,8 @@ void MPMEngine::buildPending(const SubstepParams& P, cudaStream_t s) {
 // One substep on the pending grid: grid update, fused G2P + P2G (+ binning
 // count), brick scan, permutation.  Leaves the next substep's grid pending.
 void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
-  BrickBuffers B = brickBuffers();
+  // the binning of the state read (buffer cur_) and of the state written
+  const BrickBuffers B = brickBuffers(cur_), Bn = brickBuffers(cur_ ^ 1);
   GridBuffers G = gridBuffers();
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   uint64_t l0 = launches_;
@@ -841,14 +846,14 @@ void MPMEngine::substepFused(const SubstepParams& P, cudaStream_t s) {
   l0 = launches_;
   phaseBegin(kPhaseFused, s);
   check(launchG2P2G(P, modelSetOf(hostMaterials_.data(), uint32_t(hostMaterials_.size())), statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
-                    static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, B, G, P.dt, err, launchCfg_, numSMs_, s, &launches_),
+                    static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, Bn, G, P.dt, err, launchCfg_, numSMs_, s, &launches_),
         "g2p2g");
   phaseEnd(kPhaseFused, s, l0);
   l0 = launches_;
   phaseBegin(kPhaseBin, s);
-  check(launchBrickScan(B, err, s, &launches_), "brick scan");
+  check(launchBrickScan(Bn, err, s, &launches_), "brick scan");
   // the permutation of this binning: here, or by the next grid launch
-  if (!fold) check(launchPermScatter(B, live_, err, s, &launches_), "perm scatter");
+  if (!fold) check(launchPermScatter(Bn, live_, err, s, &launches_), "perm scatter");
   phaseEnd(kPhaseBin, s, l0);
   cur_ ^= 1;
   permuted_ = true;
@@ -926,7 +931,7 @@ void putKey(std::vector<unsigned char>& k, const T& v) {
 }  // namespace
 // graph keys compare these records as bytes, so none of them may have padding
 static_assert(sizeof(SubstepParams) == 24 * 4 + 4 * sizeof(void*), "SubstepParams has padding");
-static_assert(sizeof(BrickBuffers) == 2 * 4 + 13 * sizeof(void*), "BrickBuffers has padding");
+static_assert(sizeof(BrickBuffers) == 2 * 4 + 14 * sizeof(void*), "BrickBuffers has padding");
 static_assert(sizeof(StatePtrs) == 8 * sizeof(void*), "StatePtrs has padding");
 static_assert(sizeof(GridBuffers) == 3 * sizeof(void*), "GridBuffers has padding");
 static_assert(sizeof(LaunchConfig) == 5 * 4, "LaunchConfig has padding");
@@ -943,7 +948,7 @@ std::vector<unsigned char> MPMEngine::graphKey(const SubstepParams& P) {
   putKey(k, statePtrs(1));
   putKey(k, pid_[0].ptr);
   putKey(k, pid_[1].ptr);
-  putKey(k, brickBuffers());
+  putKey(k, brickBuffers(cur_));
   putKey(k, gridBuffers());
   putKey(k, err_.ptr);
   putKey(k, launchCfg_);
@@ -1061,7 +1066,7 @@ void MPMEngine::exportBrickBins(uint32_t* numBricks, uint32_t* brickIds, uint32_
   // after a step the last binning's permutation waits for the next grid
   // launch, which reads the bin keys again: scatter it here (the same
   // values) and keep the keys intact
-  check(launchPermScatter(brickBuffers(), live_, static_cast<uint32_t*>(err_.ptr), s, &launches_), "perm scatter");
+  check(launchPermScatter(brickBuffers(cur_), live_, static_cast<uint32_t*>(err_.ptr), s, &launches_), "perm scatter");
   DevBuf sortedTmp;
   sortedTmp.alloc(size_t(std::max<uint32_t>(live_, 1u)) * sizeof(uint32_t));
   uint32_t* tmp = static_cast<uint32_t*>(sortedTmp.ptr);

@@ -174,7 +174,7 @@ class MPMEngine {
   void substepDense(const SubstepParams& P, cudaStream_t s);
   // brick-sparse fused pipeline
   StatePtrs statePtrs(int buf);
-  BrickBuffers brickBuffers();
+  BrickBuffers brickBuffers(int q);
   GridBuffers gridBuffers();
   void ensureDense();
   void normalizeOrder(cudaStream_t s);
@@ -237,7 +237,7 @@ class MPMEngine {
   // brick-sparse grid + binning
   uint32_t ncPad_ = 64, nb_ = 1, tiles_ = 1;
   DevBuf gridAcc_, gridVel_, gridVold_;
-  DevBuf bCount_, bFlag_, cCount_, cStart_, pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_;
+  DevBuf bCount_, bFlag_, bStart_, cCount_[2], pbBrick_, pbStart_, gbBrick_, counters_, scanState_, scanTile_, binKey_, binRank_, perm_;
   bool pending_ = false;
   float pendingDt_ = 0.f;
   bool pendingApic_ = false;
