@@ -329,7 +329,8 @@ int nebula_mpm_set_pipeline(nebula_mpm* e, int pipeline);
  * GPU and workload by the project's autotuner (nebula_b200/autotune.py, a
  * JSON cache keyed by GPU and configuration).  fused_threads: CTA size of the
  * fused G2P/P2G kernel (192 or 256; each warp takes 32 slots of the brick per
- * round); fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the
+ * round; 0, the default: 192 for scenes of 65,537 to 524,287 particles, else
+ * 256); fused_ctas_per_sm, grid_ctas_per_sm: persistent CTAs per SM of the
  * fused and grid-update kernels (0 = as many as fit; larger values are capped
  * at that); grid_batch: grid nodes per thread per round (2 or 4); fused_split:
  * work items per particle brick of the fused kernel (1-4; 0, the default: 2 for

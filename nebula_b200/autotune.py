@@ -40,7 +40,7 @@ CACHE_VERSION = 3  # 2: shapes carry fused_split; 3: 192-thread CTAs, contiguous
 
 @dataclass(frozen=True)
 class LaunchShape:
-    fused_threads: int = 256
+    fused_threads: int = 0  # 0 = by scene size
     fused_ctas_per_sm: int = 0  # 0 = as many as fit
     grid_ctas_per_sm: int = 0
     grid_batch: int = 4
@@ -92,7 +92,7 @@ def _ctas_options(most: int, extra: Iterable[int]) -> list[int]:
 
 
 def fused_candidates(base: LaunchShape, limits: Limits) -> list[LaunchShape]:
-    c = []
+    c = [replace(base, fused_threads=0, fused_ctas_per_sm=0)]  # the engine's choice by scene size
     for threads in (256, 192):
         most = limits.fused_max(threads)
         for k in _ctas_options(most, (most - 1, most // 2)):

@@ -71,7 +71,7 @@ struct GridBuffers {
 // Launch shape of the per-substep kernels, picked per GPU and workload by the
 // autotuner (nebula_b200/autotune.py); 0 CTAs per SM = as many as fit.
 struct LaunchConfig {
-  uint32_t fusedThreads = 256;  // k_g2p2g CTA size: 192 or 256 (a warp takes 32 slots per round)
+  uint32_t fusedThreads = 0;    // k_g2p2g CTA size: 192 or 256 (a warp takes 32 slots per round); 0 = by scene size
   uint32_t fusedCtasPerSm = 0;  // persistent k_g2p2g CTAs per SM
   uint32_t gridCtasPerSm = 0;   // persistent grid-update CTAs per SM
   uint32_t gridBatch = 4;       // k_grid_bricks nodes per thread per round: 2 or 4

@@ -333,7 +333,8 @@ void MPMEngine::setParams(const nebula_mpm_params& p) {
 }
 
 void validateLaunchConfig(const LaunchConfig& c) {
-  if (c.fusedThreads != 192 && c.fusedThreads != 256) throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 192 or 256");
+  if (c.fusedThreads != 0 && c.fusedThreads != 192 && c.fusedThreads != 256)
+    throw Error(NEBULA_MPM_ERR_INVALID, "fused_threads must be 192 or 256 (0 = by scene size)");
   if (c.gridBatch != 2 && c.gridBatch != 4) throw Error(NEBULA_MPM_ERR_INVALID, "grid_batch must be 2 or 4");
   if (c.fusedCtasPerSm > 64 || c.gridCtasPerSm > 64) throw Error(NEBULA_MPM_ERR_INVALID, "CTAs per SM must be <= 64 (0 = as many as fit)");
   if (c.fusedSplit > 4) throw Error(NEBULA_MPM_ERR_INVALID, "fused_split must be 0-4 (0 = by scene size)");

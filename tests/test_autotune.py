@@ -12,22 +12,22 @@ def test_candidates_stay_within_occupancy():
     f = A.fused_candidates(A.LaunchShape(), LIM)
     assert A.LaunchShape() in f
     for s in f:
-        assert s.fused_threads in (192, 256)
+        assert s.fused_threads in (0, 192, 256)
         assert s.fused_ctas_per_sm == 0 or 1 <= s.fused_ctas_per_sm < LIM.fused_max(s.fused_threads)
-    assert {(s.fused_threads, s.fused_ctas_per_sm) for s in f} == {(256, 0), (256, 2), (256, 1), (192, 0), (192, 3), (192, 2)}
+    assert {(s.fused_threads, s.fused_ctas_per_sm) for s in f} == {(0, 0), (256, 0), (256, 2), (256, 1), (192, 0), (192, 3), (192, 2)}
     g = A.grid_candidates(A.LaunchShape(fused_threads=192), LIM)
     assert all(s.fused_threads == 192 for s in g)
     assert {(s.grid_batch, s.grid_ctas_per_sm) for s in g} == {(4, 0), (4, 4), (4, 2), (2, 0), (2, 4), (2, 2)}
     sp = A.split_candidates(A.LaunchShape(fused_threads=192, fused_ctas_per_sm=3))
     assert [s.fused_split for s in sp] == [0, 1, 2, 3, 4] and all(s.fused_ctas_per_sm == 3 for s in sp)
     one = A.Limits(fused=(1, 1), grid=(1, 1))
-    assert len(A.fused_candidates(A.LaunchShape(), one)) == 2 and len(A.grid_candidates(A.LaunchShape(), one)) == 2
+    assert len(A.fused_candidates(A.LaunchShape(), one)) == 3 and len(A.grid_candidates(A.LaunchShape(), one)) == 2
 
 
 def cost(s):
     """Fastest at 192 threads, 3 CTAs/SM, 3 items per brick, grid batch 2 with 4 CTAs/SM."""
     c = 10.0
-    c += 0.0 if s.fused_threads == 192 else 1.0
+    c += 0.0 if s.fused_threads == 192 else 1.0 if s.fused_threads == 256 else 1.5
     c += {0: 0.5, 3: 0.0, 2: 0.3, 1: 2.0}[s.fused_ctas_per_sm]
     c += 0.0 if s.grid_batch == 2 else 0.1
     c += {0: 0.2, 4: 0.0, 2: 0.05, 8: 0.3}[s.grid_ctas_per_sm]
@@ -57,7 +57,7 @@ def test_descent_finds_the_cheapest_shape_and_caches_it(tmp_path):
     A.tune(lambda s: 1.0 if s == A.LaunchShape() else 2.0, "gpu|other", LIM, path)
     d = json.loads(path.read_text())
     assert set(d["entries"]) == {"gpu|k", "gpu|other"}
-    assert d["entries"]["gpu|other"]["shape"] == {"fused_threads": 256, "fused_ctas_per_sm": 0, "grid_ctas_per_sm": 0, "grid_batch": 4,
+    assert d["entries"]["gpu|other"]["shape"] == {"fused_threads": 0, "fused_ctas_per_sm": 0, "grid_ctas_per_sm": 0, "grid_batch": 4,
                                                   "fused_split": 0}
     best3, rep3 = A.tune(lambda s: 1.0 if s == A.LaunchShape() else 2.0, "gpu|k", LIM, path, force=True)
     assert best3 == A.LaunchShape() and rep3["source"] == "measured"
