@@ -506,17 +506,14 @@ __global__ void __launch_bounds__(kThreads) k_perm_scatter(BrickBuffers B, uint3
 }
 
 // ------------------------------------------------------------------ shared-memory P2G
-// A CTA handles one particle brick at a time, in chunks of kChunk particles.
-// Each particle's P2G inputs go to a shared row, and the row is pushed onto a
-// linked list of the cell its stencil is centred on (6^3 cells around the
-// brick; the first row of a cell also appends the cell to the chunk's list of
-// non-empty cells).  A warp then takes whole cells: lanes 0..26 own the cell's
-// 27 stencil nodes, walk the cell's list and accumulate its particles'
-// contributions in registers, then add them into the brick's 8^3 tile (see
-// kTileCopies).  Two barriers per chunk.  The brick ends with one vector
-// reduction per non-zero node of the tile.
+// A CTA handles one particle brick at a time.  Each particle's P2G inputs go
+// to its lane's row in shared memory in separable form (p2gRow); the lanes of
+// a warp are grouped by the cell their stencils are centred on, and for each
+// group lanes 0..26 take the cell's 27 nodes, sum the group's rows and add the
+// sums into the brick's 8^3 accumulation tile with shared-memory float
+// reductions (p2gWarpGroups).  The item ends with one barrier and one vector
+// reduction to global memory per non-zero node of the tile (p2gFlush).
 constexpr int kRow = 9;         // float4 per input row: 3 axes x 3 offsets (see p2gRow)
-constexpr int kCellSlots = 216; // 6^3 stencil centres around a brick
 constexpr int kTileNodes = 512; // 8^3
 // A tile plane (one of mass, mom.x, mom.y, mom.z) stores node (x, y, z) at
 // x + 11 y + 89 z: with strides 11 and 89 (3 and 25 modulo the 32 banks) the
@@ -526,48 +523,17 @@ constexpr int kTileNodes = 512; // 8^3
 constexpr int kTileSy = 11, kTileSz = 89;
 constexpr int kTilePlane = 7 * kTileSz + 7 * kTileSy + 8;  // 708 floats
 __device__ __forceinline__ int tileIndex(int x, int y, int z) { return x + kTileSy * y + kTileSz * z; }
-
-constexpr uint32_t kNoRow = 0x7FFFu;     // end of a cell's list
-constexpr uint32_t kExactRow = 0x8000u;  // next[] flag: this row is in the exact form (see p2gRow)
-// Copies of the brick's 8^3 accumulation tile: 1 = one tile shared by the
-// warps, updated with shared-memory float reductions (a warp owns one cell at
-// a time, so warps collide only on the nodes where neighbouring cells'
-// stencils overlap); kWarps = one private tile per warp with plain adds.
-constexpr int kTileCopies = 1;
-
-// CHUNK = the CTA size = particles per chunk (128 or 256).
-template <int CHUNK>
-struct P2GSmemT {
-  static constexpr int kChunk = CHUNK;
-  static constexpr int kWarps = CHUNK / 32;
-  float4 rows[CHUNK * kRow];
-  float tiles[kTileCopies * 4 * kTilePlane];
-  uint32_t head[kCellSlots];   // first row of each cell's list (kNoRow: empty)
-  uint16_t next[CHUNK];        // next row of the same cell, | kExactRow when the row is in the exact form
-  float mass[CHUNK];           // the particle mass of an exact-form row
-  uint16_t cells[kCellSlots];  // the chunk's non-empty cells
-  uint32_t numCells[2];        // by chunk parity, so resetting one never races the next chunk
-  uint32_t markMask;           // grid-active marks of the item brick's 3^3 neighbour bricks
-  uint32_t item;
-  uint32_t items[2];           // fused kernel: claimed items by iteration parity
-};
-using P2GSmem = P2GSmemT<kThreads>;
-
-// A stencil-centre cell among the 6^3 around a brick: its coordinates
-// relative to the block origin packed as rx | ry << 3 | rz << 6 (the chunk's
-// cell list holds these), and its slot (rz * 6 + ry) * 6 + rx in head[].
-__device__ __forceinline__ uint32_t cellSlotOf(uint32_t packed) { return ((packed >> 6) * 6u + ((packed >> 3) & 7u)) * 6u + (packed & 7u); }
-
-// Push this thread's row onto the list of the packed cell (`par`: the chunk's parity).
-template <class SM>
-__device__ __forceinline__ void p2gRegister(SM& sm, uint32_t packed, uint32_t par, bool exact) {
-  const uint32_t prev = atomicExch(&sm.head[cellSlotOf(packed)], threadIdx.x);
-  sm.next[threadIdx.x] = uint16_t(prev | (exact ? kExactRow : 0u));
-  if (prev == kNoRow) sm.cells[atomicAdd(&sm.numCells[par], 1u)] = uint16_t(packed);
-}
-
-// Shared memory of the fused kernel (THREADS = the CTA size, 128 or 256).
 constexpr uint32_t kNoKey = 0xFFFFFFFFu;  // a lane with no row for the warp's P2G
+
+// Shared memory of the standalone P2G kernel.
+struct P2GSmem {
+  float4 rows[kThreads * kRow];  // P2G input rows; warp w owns rows [32 w, 32 w + 32)
+  float tiles[4 * kTilePlane];   // the item's 8^3 accumulation tile
+  float mass[kThreads];          // the particle mass of an exact-form row
+  uint32_t item;
+};
+
+// Shared memory of the fused kernel (THREADS = the CTA size, 192 or 256).
 
 template <bool FLIP, int THREADS>
 struct FusedSmem {
@@ -702,86 +668,19 @@ __device__ __noinline__ void p2gRowGlobal(const SubstepParams& P, const float4* 
       }
 }
 
-template <class SM>
-__device__ __forceinline__ void p2gZeroTiles(SM& sm) {
-  for (int q = threadIdx.x; q < kTileCopies * 4 * kTilePlane; q += blockDim.x) sm.tiles[q] = 0.f;
-  for (int q = threadIdx.x; q < kCellSlots; q += blockDim.x) sm.head[q] = kNoRow;
-  if (threadIdx.x < 2) sm.numCells[threadIdx.x] = 0u;
-  if (threadIdx.x == 0) sm.markMask = 0u;
-}
-
-// Called by every thread once the chunk's rows are written and registered;
-// ends synced.  Tile origin (node) = (bx, by, bz) * 4 - 2; stencil-centre
-// cells start at + 1.
-template <class SM>
-__device__ __forceinline__ void p2gChunk(const SubstepParams& P, SM& sm, uint32_t par, int tx, int ty, int tz) {
-  constexpr int kChunk = SM::kChunk, kWarps = SM::kWarps;
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
-  const int cr = int(P.cubeRes);
-  float* tile = sm.tiles + (kTileCopies == 1 ? 0 : warp) * 4 * kTilePlane;
-  const uint32_t numCells = sm.numCells[par];
-  // a tile wholly inside the grid needs no per-node bounds test
-  const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
-  for (uint32_t ci = warp; ci < numCells; ci += kWarps) {
-    const uint32_t packed = sm.cells[ci];
-    const uint32_t q = cellSlotOf(packed);
-    const int lx = int(packed & 7u) + dx, ly = int((packed >> 3) & 7u) + dy, lz = int(packed >> 6) + dz;  // tile-local node
-    const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
-    if (lane < 27 && (inside || (nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr))) {
-      float a[4] = {0.f, 0.f, 0.f, 0.f};
-      // A list holds at most kChunk rows; the bound keeps the walk finite
-      // whatever the list holds.  The row form is uniform across the warp's
-      // lanes (they walk the same row).
-      uint32_t j = sm.head[q] & 0xFFFFu;
-      for (int it = 0; j < uint32_t(kChunk) && it < kChunk; ++it) {
-        const uint32_t link = sm.next[j];
-        if (link & kExactRow) p2gNodeTermExact(sm.rows + j * kRow, sm.mass[j], dx, dy, dz, a);
-        else p2gNodeTerm(sm.rows + j * kRow, dx, dy, dz, a);
-        j = link & ~kExactRow;
-      }
-      const int t = tileIndex(lx, ly, lz);
-      if (kTileCopies == 1) {
-        atomicAdd(tile + t, a[3]);
-        atomicAdd(tile + kTilePlane + t, a[0]);
-        atomicAdd(tile + 2 * kTilePlane + t, a[1]);
-        atomicAdd(tile + 3 * kTilePlane + t, a[2]);
-      } else {
-        tile[t] += a[3];
-        tile[kTilePlane + t] += a[0];
-        tile[2 * kTilePlane + t] += a[1];
-        tile[3 * kTilePlane + t] += a[2];
-      }
-    }
-    __syncwarp();
-    if (lane == 0) sm.head[q] = kNoRow;  // every lane has read it
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) sm.numCells[par] = 0u;  // reused two chunks later, after another barrier
-}
-
-// Sum the tile copies, add every non-zero node to the global grid and leave
-// the tile zeroed (each node is read and cleared by the one thread that owns
-// it) for the CTA's next item.
+// Add every non-zero node of the tile to the global grid and leave the tile
+// zeroed (each node is read and cleared by the one thread that owns it) for
+// the CTA's next item.
 template <class SM>
 __device__ __forceinline__ void p2gFlush(const SubstepParams& P, SM& sm, int tx, int ty, int tz, float4* acc) {
   const int cr = int(P.cubeRes);
   for (int q = threadIdx.x; q < kTileNodes; q += blockDim.x) {
-    float m = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
-    const int i = tileIndex(q & 7, (q >> 3) & 7, q >> 6);
-#pragma unroll
-    for (int w = 0; w < kTileCopies; ++w) {
-      float* t = sm.tiles + w * 4 * kTilePlane + i;
-      m += t[0];
-      mx += t[kTilePlane];
-      my += t[2 * kTilePlane];
-      mz += t[3 * kTilePlane];
-      t[0] = 0.f;
-      t[kTilePlane] = 0.f;
-      t[2 * kTilePlane] = 0.f;
-      t[3 * kTilePlane] = 0.f;
-    }
+    float* t = sm.tiles + tileIndex(q & 7, (q >> 3) & 7, q >> 6);
+    const float m = t[0], mx = t[kTilePlane], my = t[2 * kTilePlane], mz = t[3 * kTilePlane];
+    t[0] = 0.f;
+    t[kTilePlane] = 0.f;
+    t[2 * kTilePlane] = 0.f;
+    t[3 * kTilePlane] = 0.f;
     if (m == 0.f && mx == 0.f && my == 0.f && mz == 0.f) continue;
     const int nx = tx + (q & 7), ny = ty + ((q >> 3) & 7), nz = tz + (q >> 6);
     if (nx < 0 || ny < 0 || nz < 0 || nx >= cr || ny >= cr || nz >= cr) continue;
@@ -818,7 +717,7 @@ struct StagedGrid {
 };
 
 // A particle's stencil centre among the brick's 6^3 cells (block origin ox,
-// oy, oz), packed as rx | ry << 3 | rz << 6 (cellSlotOf gives its slot), or -1.
+// oy, oz), packed as rx | ry << 3 | rz << 6, or -1.
 __device__ __forceinline__ int cellPacked(int cx, int cy, int cz, int ox, int oy, int oz) {
   const int rx = cx - ox, ry = cy - oy, rz = cz - oz;
   if ((unsigned)rx < 6u && (unsigned)ry < 6u && (unsigned)rz < 6u) return rx | (ry << 3) | (rz << 6);
@@ -826,34 +725,101 @@ __device__ __forceinline__ int cellPacked(int cx, int cy, int cz, int ox, int oy
 }
 
 // ------------------------------------------------------------------ P2G over particle bricks (standalone)
-// P2G of the particles in sorted slots [start, end) of brick `b` (the scene's own brick id).
-template <class SM>
-__device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, SM& sm, uint32_t b, uint32_t start, uint32_t end, StatePtrs cur,
+// P2G of one warp's rows (written by the lanes holding a row, key = packed
+// stencil-centre cell, kNoKey for none): the lanes of equal key form a group,
+// and for each group lanes 0..26 take the cell's 27 stencil nodes, sum the
+// group's rows (each read at a known address, no list to follow) and add the
+// sums into the tile with shared-memory float reductions.  Warps do not wait
+// for one another.
+__device__ __forceinline__ void p2gWarpGroups(const SubstepParams& P, const float4* __restrict__ wrows, const float* __restrict__ wmass, float* tile,
+                                              uint32_t key, uint32_t exactMask, int tx, int ty, int tz) {
+  const int lane = threadIdx.x & 31;
+  const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
+  const int cr = int(P.cubeRes);
+  // a tile wholly inside the grid needs no per-node bounds test
+  const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
+  __syncwarp();  // the rows are visible to every lane
+  uint32_t pending = __ballot_sync(0xffffffffu, key != kNoKey);
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const uint32_t k = __shfl_sync(0xffffffffu, key, leader);
+    const uint32_t peers = __ballot_sync(0xffffffffu, key == k);
+    pending &= ~peers;
+    const int lx = int(k & 7u) + dx, ly = int((k >> 3) & 7u) + dy, lz = int(k >> 6) + dz;  // tile-local node
+    const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
+    if (lane < 27 && (inside || (nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr))) {
+      float a[4] = {0.f, 0.f, 0.f, 0.f};
+      if (!(peers & exactMask)) {
+        // usual-form rows: two per step, loads of both issued before their sums
+        uint32_t m = peers;
+        while (m) {
+          const int j0 = __ffs(m) - 1;
+          m &= m - 1u;
+          const int j1 = m ? __ffs(m) - 1 : -1;
+          m &= m - 1u;
+          const float4* r0 = wrows + j0 * kRow;
+          const float4 X0 = r0[dx], Y0 = r0[3 + dy], Z0 = r0[6 + dz];
+          float4 X1 = make_float4(0.f, 0.f, 0.f, 0.f), Y1 = X1, Z1 = X1;
+          if (j1 >= 0) {
+            const float4* r1 = wrows + j1 * kRow;
+            X1 = r1[dx]; Y1 = r1[3 + dy]; Z1 = r1[6 + dz];
+          }
+          p2gNodeTermXYZ(X0, Y0, Z0, a);
+          p2gNodeTermXYZ(X1, Y1, Z1, a);  // a missing second row adds zeros
+        }
+      } else {
+        uint32_t m = peers;
+        while (m) {
+          const int j = __ffs(m) - 1;
+          m &= m - 1u;
+          if ((exactMask >> j) & 1u) p2gNodeTermExact(wrows + j * kRow, wmass[j], dx, dy, dz, a);
+          else p2gNodeTerm(wrows + j * kRow, dx, dy, dz, a);
+        }
+      }
+      const int t = tileIndex(lx, ly, lz);
+      atomicAdd(tile + t, a[3]);
+      atomicAdd(tile + kTilePlane + t, a[0]);
+      atomicAdd(tile + 2 * kTilePlane + t, a[1]);
+      atomicAdd(tile + 3 * kTilePlane + t, a[2]);
+    }
+  }
+  __syncwarp();  // every lane has read the rows before they are written again
+}
+
+// P2G of the particles in sorted slots [start, end) of brick `b` (the scene's
+// own brick id): warps take rounds of 32 slots, each lane writes its
+// particle's row, each warp adds its groups into the tile; one barrier, then
+// the flush.
+__device__ __forceinline__ void p2gBrickItem(const SubstepParams& P, P2GSmem& sm, uint32_t b, uint32_t start, uint32_t end, StatePtrs cur,
                                              uint32_t n, const BrickBuffers& B, const GridBuffers& G, float dtStress) {
-  constexpr int kChunk = SM::kChunk;
   int bx, by, bz;
   mortonDecode(b, bx, by, bz);
   const int tx = 4 * bx - 2, ty = 4 * by - 2, tz = 4 * bz - 2;
-  uint32_t par = 0;
-  for (uint32_t base = start; base < end; base += kChunk, par ^= 1u) {
-    const uint32_t t = base + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4* wrows = sm.rows + warp * 32 * kRow;
+  float* wmass = sm.mass + warp * 32;
+#pragma unroll 1
+  for (uint32_t t0 = start + uint32_t(warp) * 32u; t0 < end; t0 += kThreads) {
+    const uint32_t t = t0 + uint32_t(lane);
+    uint32_t key = kNoKey;
+    bool exact = false;
     if (t < end) {
       const uint32_t s = B.perm[t];
       if (s < n) {
         const PState st = loadState(cur.f, s);
         int cx, cy, cz;
         cellCoords(P, st.P.x, st.P.y, st.P.z, cx, cy, cz);
-        float4* row = sm.rows + threadIdx.x * kRow;
         float m;
-        const bool exact = p2gRow(P, st, dtStress, cx, cy, cz, row, m);
-        sm.mass[threadIdx.x] = m;
-        const int key = cellPacked(cx, cy, cz, tx + 1, ty + 1, tz + 1);
-        if (key >= 0) p2gRegister(sm, uint32_t(key), par, exact);
-        else p2gRowGlobal(P, row, m, exact, cx, cy, cz, G.acc);
+        exact = p2gRow(P, st, dtStress, cx, cy, cz, wrows + lane * kRow, m);
+        wmass[lane] = m;
+        const int pk = cellPacked(cx, cy, cz, tx + 1, ty + 1, tz + 1);
+        if (pk >= 0) key = uint32_t(pk);
+        else p2gRowGlobal(P, wrows + lane * kRow, m, exact, cx, cy, cz, G.acc);
       }
     }
-    p2gChunk(P, sm, par, tx, ty, tz);
+    p2gWarpGroups(P, wrows, wmass, sm.tiles, key, __ballot_sync(0xffffffffu, exact), tx, ty, tz);
   }
+  __syncthreads();  // the tile is complete
   p2gFlush(P, sm, tx, ty, tz, G.acc);
 }
 
@@ -863,9 +829,10 @@ __global__ void __launch_bounds__(kThreads) k_p2g_bricks(SubstepParams P0, Scene
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2GSmem& sm = *reinterpret_cast<P2GSmem*>(smem_raw);
   const uint32_t numPB = B.counters[kCntNumPB];
+  // the tile starts zeroed here and is left so by every item's flush
+  for (int q = threadIdx.x; q < 4 * kTilePlane; q += blockDim.x) sm.tiles[q] = 0.f;
   for (;;) {
     if (threadIdx.x == 0) sm.item = atomicAdd(B.counters + kCntQueueP2G, 1u);
-    p2gZeroTiles(sm);
     __syncthreads();
     const uint32_t i = sm.item;
     if (i >= numPB) break;
@@ -1010,67 +977,6 @@ __global__ void __launch_bounds__(kThreads) k_clear_bricks(BrickBuffers B, GridB
 }
 
 // ------------------------------------------------------------------ fused G2P -> update -> P2G
-// P2G of one warp's rows (written by the lanes holding a row, key = packed
-// stencil-centre cell, kNoKey for none): the lanes of equal key form a group,
-// and for each group lanes 0..26 take the cell's 27 stencil nodes, sum the
-// group's rows (each read at a known address, no list to follow) and add the
-// sums into the tile with shared-memory float reductions.  Warps do not wait
-// for one another.
-__device__ __forceinline__ void p2gWarpGroups(const SubstepParams& P, const float4* __restrict__ wrows, const float* __restrict__ wmass, float* tile,
-                                              uint32_t key, uint32_t exactMask, int tx, int ty, int tz) {
-  const int lane = threadIdx.x & 31;
-  const int dx = lane % 3, dy = (lane / 3) % 3, dz = lane / 9;
-  const int cr = int(P.cubeRes);
-  // a tile wholly inside the grid needs no per-node bounds test
-  const bool inside = tx >= 0 && ty >= 0 && tz >= 0 && tx + 8 <= cr && ty + 8 <= cr && tz + 8 <= cr;
-  __syncwarp();  // the rows are visible to every lane
-  uint32_t pending = __ballot_sync(0xffffffffu, key != kNoKey);
-  while (pending) {
-    const int leader = __ffs(pending) - 1;
-    const uint32_t k = __shfl_sync(0xffffffffu, key, leader);
-    const uint32_t peers = __ballot_sync(0xffffffffu, key == k);
-    pending &= ~peers;
-    const int lx = int(k & 7u) + dx, ly = int((k >> 3) & 7u) + dy, lz = int(k >> 6) + dz;  // tile-local node
-    const int nx = tx + lx, ny = ty + ly, nz = tz + lz;
-    if (lane < 27 && (inside || (nx >= 0 && ny >= 0 && nz >= 0 && nx < cr && ny < cr && nz < cr))) {
-      float a[4] = {0.f, 0.f, 0.f, 0.f};
-      if (!(peers & exactMask)) {
-        // usual-form rows: two per step, loads of both issued before their sums
-        uint32_t m = peers;
-        while (m) {
-          const int j0 = __ffs(m) - 1;
-          m &= m - 1u;
-          const int j1 = m ? __ffs(m) - 1 : -1;
-          m &= m - 1u;
-          const float4* r0 = wrows + j0 * kRow;
-          const float4 X0 = r0[dx], Y0 = r0[3 + dy], Z0 = r0[6 + dz];
-          float4 X1 = make_float4(0.f, 0.f, 0.f, 0.f), Y1 = X1, Z1 = X1;
-          if (j1 >= 0) {
-            const float4* r1 = wrows + j1 * kRow;
-            X1 = r1[dx]; Y1 = r1[3 + dy]; Z1 = r1[6 + dz];
-          }
-          p2gNodeTermXYZ(X0, Y0, Z0, a);
-          p2gNodeTermXYZ(X1, Y1, Z1, a);  // a missing second row adds zeros
-        }
-      } else {
-        uint32_t m = peers;
-        while (m) {
-          const int j = __ffs(m) - 1;
-          m &= m - 1u;
-          if ((exactMask >> j) & 1u) p2gNodeTermExact(wrows + j * kRow, wmass[j], dx, dy, dz, a);
-          else p2gNodeTerm(wrows + j * kRow, dx, dy, dz, a);
-        }
-      }
-      const int t = tileIndex(lx, ly, lz);
-      atomicAdd(tile + t, a[3]);
-      atomicAdd(tile + kTilePlane + t, a[0]);
-      atomicAdd(tile + 2 * kTilePlane + t, a[1]);
-      atomicAdd(tile + 3 * kTilePlane + t, a[2]);
-    }
-  }
-  __syncwarp();  // every lane has read the rows before they are written again
-}
-
 // One work item: the sorted slots [start, end) of particle brick `b` (the
 // scene's own brick id).  The binning orders a brick's particles by cell
 // (the brick's 64 cells in Morton order), so a warp's 32 consecutive slots
