@@ -132,6 +132,13 @@ void BatchEngine::setParams(uint32_t s, const nebula_mpm_params& p) {
 
 void BatchEngine::getParams(uint32_t s, nebula_mpm_params* p) const { *p = scene(s).params; }
 
+// The material-model set of every scene's table together (the fused kernel's instantiation).
+int BatchEngine::modelSet() const {
+  std::vector<Material> all;
+  for (const Scene& sc : scenes_) all.insert(all.end(), sc.materials.begin(), sc.materials.end());
+  return modelSetOf(all.data(), uint32_t(all.size()));
+}
+
 void BatchEngine::setMaterials(uint32_t s, const nebula_mpm_material* mats, uint32_t n) {
   Scene& sc = scene(s);
   if (n == 0) return;  // MPMEngine.cpp:240
@@ -467,7 +474,7 @@ void BatchEngine::substep(uint32_t k, cudaStream_t st) {
   uint32_t* err = static_cast<uint32_t*>(err_.ptr);
   const bool fold = live_ < kFoldScatterMax;
   check(launchGridBricksBatch(T, k, B, G, fold ? live_ : 0u, err, launchCfg_, numSMs_, st, &launches_), "grid bricks");
-  check(launchG2P2GBatch(T, G.vold != nullptr, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
+  check(launchG2P2GBatch(T, modelSet(), G.vold != nullptr, statePtrs(cur_), static_cast<const uint32_t*>(pid_[cur_].ptr), statePtrs(cur_ ^ 1),
                          static_cast<uint32_t*>(pid_[cur_ ^ 1].ptr), live_, Bn, G, err, launchCfg_, numSMs_, st, &launches_),
         "g2p2g");
   check(launchBrickScan(Bn, err, st, &launches_), "brick scan");
@@ -510,7 +517,7 @@ void BatchEngine::step(float dt, uint32_t substeps, cudaStream_t st) {
   if (!pending_) buildPending(st);
   const bool flip = gridBuffers().vold != nullptr;
   if (useGraphs_ && st != nullptr) {
-    const auto key = std::make_tuple(substeps, cur_, flip);
+    const auto key = std::make_tuple(substeps, cur_, flip, modelSet());
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       // capture: the launchers record their kernels into the graph, and the

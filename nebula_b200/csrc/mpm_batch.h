@@ -72,6 +72,7 @@ class BatchEngine {
   bool anyFlip() const;
   StatePtrs statePtrs(int buf);
   BrickBuffers brickBuffers(int q);
+  int modelSet() const;
   GridBuffers gridBuffers();
   SceneTable table() const;
   void clearGraphs();
@@ -106,8 +107,8 @@ class BatchEngine {
   float pendingDt_ = 0.f;
 
   bool useGraphs_ = true;
-  std::map<std::tuple<uint32_t, int, bool>, cudaGraphExec_t> graphs_;
-  std::map<std::tuple<uint32_t, int, bool>, uint64_t> launchesPerGraph_;
+  std::map<std::tuple<uint32_t, int, bool, int>, cudaGraphExec_t> graphs_;  // by substeps, buffer parity, FLIP, model set
+  std::map<std::tuple<uint32_t, int, bool, int>, uint64_t> launchesPerGraph_;
 
   uint64_t substeps_ = 0;
   uint64_t launches_ = 0;

@@ -1178,7 +1178,9 @@ template <bool FLIP, bool BATCH, int THREADS, int MS> void setupFused(LaunchShap
 template <int THREADS> void setupFusedShape(LaunchShapes& L) {
   setupFused<false, false, THREADS, kModelsElastic>(L);
   setupFused<false, false, THREADS, kModelsDruckerPrager>(L);
+  setupFused<false, false, THREADS, kModelsElasticVonMises>(L);
   setupFused<false, false, THREADS, kModelsAny>(L);
+  setupFused<false, true, THREADS, kModelsElasticVonMises>(L);
   setupFused<false, true, THREADS, kModelsAny>(L);
   setupFused<true, false, THREADS, kModelsAny>(L);
   setupFused<true, true, THREADS, kModelsAny>(L);
@@ -1323,7 +1325,7 @@ cudaError_t launchFused(const SubstepParams& P, const SceneTable& T, StatePtrs c
 }
 
 // The instantiation for the launch shape and the model set: model-specialised
-// kernels exist for single scenes with APIC or PIC transfer.
+// kernels exist for APIC or PIC transfer (batches: the elastic / Von Mises set).
 template <bool BATCH, int THREADS>
 cudaError_t launchFusedShape(bool flip, int modelSet, const LaunchConfig& lc, const SubstepParams& P, const SceneTable& T, StatePtrs cur,
                              const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n, const BrickBuffers& b, GridBuffers g,
@@ -1335,6 +1337,8 @@ cudaError_t launchFusedShape(bool flip, int modelSet, const LaunchConfig& lc, co
   // 95.8 us; 1M: 292 / 390 us per launch)
   const uint32_t k = lc.fusedCtasPerSm, sp = lc.fusedSplit ? lc.fusedSplit : (n <= (1u << 16) ? 2u : 1u);
   if (flip) return launchFused<true, BATCH, THREADS, kModelsAny>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+  if (modelSet == kModelsElasticVonMises)
+    return launchFused<false, BATCH, THREADS, kModelsElasticVonMises>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
   if constexpr (!BATCH) {
     if (modelSet == kModelsElastic)
       return launchFused<false, false, THREADS, kModelsElastic>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
@@ -1360,12 +1364,13 @@ cudaError_t launchFusedFor(bool flip, int modelSet, const LaunchConfig& lc, cons
 }  // namespace
 
 int modelSetOf(const Material* mats, uint32_t count) {
-  bool elastic = count > 0, dp = count > 0;
+  bool elastic = count > 0, dp = count > 0, evm = count > 0;
   for (uint32_t i = 0; i < count; ++i) {
     elastic = elastic && mats[i].model == MAT_ELASTIC;
     dp = dp && (mats[i].model == MAT_DRUCKER_PRAGER || mats[i].model == MAT_GRANULAR_POWDER);
+    evm = evm && (mats[i].model == MAT_ELASTIC || mats[i].model == MAT_VON_MISES);
   }
-  return elastic ? kModelsElastic : dp ? kModelsDruckerPrager : kModelsAny;
+  return elastic ? kModelsElastic : dp ? kModelsDruckerPrager : evm ? kModelsElasticVonMises : kModelsAny;
 }
 
 cudaError_t launchG2P2G(const SubstepParams& P, int modelSet, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
@@ -1377,10 +1382,11 @@ cudaError_t launchG2P2G(const SubstepParams& P, int modelSet, StatePtrs cur, con
   return e;
 }
 
-cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                             const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+cudaError_t launchG2P2GBatch(const SceneTable& T, int modelSet, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt,
+                             uint32_t n, const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches) {
-  const cudaError_t e = launchFusedFor<true>(flip, kModelsAny, lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
+  const cudaError_t e = launchFusedFor<true>(flip, modelSet == kModelsElasticVonMises || modelSet == kModelsElastic ? kModelsElasticVonMises : kModelsAny,
+                                             lc, SubstepParams{}, T, cur, pidCur, nxt, pidNxt, n, b, g, 0.f, err, numSMs, s);
   ++*launches;
   return e;
 }

@@ -122,8 +122,8 @@ cudaError_t launchP2GBricksBatch(const SceneTable& T, StatePtrs cur, uint32_t n,
                                  cudaStream_t s, uint64_t* launches);
 cudaError_t launchGridBricksBatch(const SceneTable& T, uint32_t substep, const BrickBuffers& b, GridBuffers g, uint32_t n, uint32_t* err,
                                   const LaunchConfig& lc, int numSMs, cudaStream_t s, uint64_t* launches);
-cudaError_t launchG2P2GBatch(const SceneTable& T, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,
-                             const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
+cudaError_t launchG2P2GBatch(const SceneTable& T, int modelSet, bool flip, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt,
+                             uint32_t n, const BrickBuffers& b, GridBuffers g, uint32_t* err, const LaunchConfig& lc, int numSMs, cudaStream_t s,
                              uint64_t* launches);
 // Run the brick scan's bounded look-back against a predecessor that never
 // publishes; *errorBits receives the device error word (kErrScanTimeout set

@@ -316,6 +316,7 @@ enum ModelSet : int {
   kModelsAny = 0,
   kModelsElastic = 1,        // ELASTIC (Hencky) only
   kModelsDruckerPrager = 2,  // DRUCKER_PRAGER and GRANULAR_POWDER (the same return map, no viscosity)
+  kModelsElasticVonMises = 3,  // ELASTIC and VON_MISES
 };
 
 // Everything of mpm_g2p.comp after the gather (lines 120-271): material,
@@ -343,6 +344,9 @@ __device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s,
     plasticReturn(MAT_DRUCKER_PRAGER, Fn, tau, mat.mu, mat.lam, mat.M, mat.qc, mat.qmax);
   } else if constexpr (MS == kModelsElastic) {
     tau = henckyStress<float>(Fn, mat.mu, mat.lam);
+  } else if constexpr (MS == kModelsElasticVonMises) {
+    if (mat.model == MAT_VON_MISES) plasticReturn(MAT_VON_MISES, Fn, tau, mat.mu, mat.lam, mat.M, mat.qc, mat.qmax);
+    else tau = henckyStress<float>(Fn, mat.mu, mat.lam);
   } else if (mat.model == MAT_FLUID) {
     float J = fmaxf(m3det(Fn), 1e-4f);
     float c = powf(J, 1.0f / 3.0f);
