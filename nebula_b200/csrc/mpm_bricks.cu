@@ -1179,6 +1179,7 @@ template <int THREADS> void setupFusedShape(LaunchShapes& L) {
   setupFused<false, false, THREADS, kModelsElastic>(L);
   setupFused<false, false, THREADS, kModelsDruckerPrager>(L);
   setupFused<false, false, THREADS, kModelsElasticVonMises>(L);
+  setupFused<false, false, THREADS, kModelsElasticDruckerPrager>(L);
   setupFused<false, false, THREADS, kModelsAny>(L);
   setupFused<false, true, THREADS, kModelsElasticVonMises>(L);
   setupFused<false, true, THREADS, kModelsAny>(L);
@@ -1344,6 +1345,9 @@ cudaError_t launchFusedShape(bool flip, int modelSet, const LaunchConfig& lc, co
       return launchFused<false, false, THREADS, kModelsElastic>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
     if (modelSet == kModelsDruckerPrager)
       return launchFused<false, false, THREADS, kModelsDruckerPrager>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
+    if (modelSet == kModelsElasticDruckerPrager)
+      return launchFused<false, false, THREADS, kModelsElasticDruckerPrager>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs,
+                                                                              s);
   }
   return launchFused<false, BATCH, THREADS, kModelsAny>(P, T, cur, pidCur, nxt, pidNxt, n, b, g, dtStress, err, k, sp, numSMs, s);
 }
@@ -1364,13 +1368,16 @@ cudaError_t launchFusedFor(bool flip, int modelSet, const LaunchConfig& lc, cons
 }  // namespace
 
 int modelSetOf(const Material* mats, uint32_t count) {
-  bool elastic = count > 0, dp = count > 0, evm = count > 0;
+  bool elastic = count > 0, dp = count > 0, evm = count > 0, edp = count > 0;
   for (uint32_t i = 0; i < count; ++i) {
-    elastic = elastic && mats[i].model == MAT_ELASTIC;
-    dp = dp && (mats[i].model == MAT_DRUCKER_PRAGER || mats[i].model == MAT_GRANULAR_POWDER);
-    evm = evm && (mats[i].model == MAT_ELASTIC || mats[i].model == MAT_VON_MISES);
+    const uint32_t m = mats[i].model;
+    const bool isDp = m == MAT_DRUCKER_PRAGER || m == MAT_GRANULAR_POWDER;
+    elastic = elastic && m == MAT_ELASTIC;
+    dp = dp && isDp;
+    evm = evm && (m == MAT_ELASTIC || m == MAT_VON_MISES);
+    edp = edp && (m == MAT_ELASTIC || isDp);
   }
-  return elastic ? kModelsElastic : dp ? kModelsDruckerPrager : evm ? kModelsElasticVonMises : kModelsAny;
+  return elastic ? kModelsElastic : dp ? kModelsDruckerPrager : evm ? kModelsElasticVonMises : edp ? kModelsElasticDruckerPrager : kModelsAny;
 }
 
 cudaError_t launchG2P2G(const SubstepParams& P, int modelSet, StatePtrs cur, const uint32_t* pidCur, StatePtrs nxt, uint32_t* pidNxt, uint32_t n,

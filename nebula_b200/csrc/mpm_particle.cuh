@@ -317,6 +317,7 @@ enum ModelSet : int {
   kModelsElastic = 1,        // ELASTIC (Hencky) only
   kModelsDruckerPrager = 2,  // DRUCKER_PRAGER and GRANULAR_POWDER (the same return map, no viscosity)
   kModelsElasticVonMises = 3,  // ELASTIC and VON_MISES
+  kModelsElasticDruckerPrager = 4,  // ELASTIC and the Drucker-Prager family
 };
 
 // Everything of mpm_g2p.comp after the gather (lines 120-271): material,
@@ -347,6 +348,9 @@ __device__ __forceinline__ uint32_t g2pUpdate(const SubstepParams& P, PState& s,
   } else if constexpr (MS == kModelsElasticVonMises) {
     if (mat.model == MAT_VON_MISES) plasticReturn(MAT_VON_MISES, Fn, tau, mat.mu, mat.lam, mat.M, mat.qc, mat.qmax);
     else tau = henckyStress<float>(Fn, mat.mu, mat.lam);
+  } else if constexpr (MS == kModelsElasticDruckerPrager) {
+    if (mat.model == MAT_ELASTIC) tau = henckyStress<float>(Fn, mat.mu, mat.lam);
+    else plasticReturn(MAT_DRUCKER_PRAGER, Fn, tau, mat.mu, mat.lam, mat.M, mat.qc, mat.qmax);
   } else if (mat.model == MAT_FLUID) {
     float J = fmaxf(m3det(Fn), 1e-4f);
     float c = powf(J, 1.0f / 3.0f);
