@@ -1165,7 +1165,7 @@ struct LaunchShapes {
   int p2g[2] = {0, 0};                          // [BATCH]
   int grid[2] = {0, 0};                         // [gridBatch == 4]
   int gridBatch = 0;                            // batched grid kernel
-  int fused[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};  // [FLIP][BATCH][CHUNK == 256]
+  int fused[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};  // [FLIP][BATCH][THREADS == 256]
 };
 constexpr int kShapeSlots = 64;  // device ordinals beyond this share slots modulo 64
 LaunchShapes g_shapes[kShapeSlots];
