@@ -521,7 +521,8 @@ __device__ __forceinline__ void druckerPragerFromSvd(m3<float>& F, m3<float>& ta
   const float normDev = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
   const float K = lam + 2.0f * mu * kThird;
   const float q_yield = M * (-K * trEps) + qc;
-  if (q_yield <= 1e-8f) {
+  const bool apex = q_yield <= 1e-8f;
+  if (apex) {
     const float tr = (qc / fmaxf(M, 1e-8f)) / K;  // -p_proj / K with p_proj = -qc / max(M, 1e-8)
 #pragma unroll
     for (int i = 0; i < 3; ++i) eps[i] = tr * kThird;
@@ -547,6 +548,16 @@ __device__ __forceinline__ void druckerPragerFromSvd(m3<float>& F, m3<float>& ta
   for (int i = 0; i < 3; ++i) k[i] = lam * te + 2.0f * mu * e[i];
   const m3<double> Fn = rebuildUSVt(U, sp, V);
   F = m3cast<float>(Fn);
+  if (apex) {
+    // three equal log-strains: the rebuilt F is a multiple of an orthogonal
+    // matrix, whose decomposition finds orthonormal singular vectors in any
+    // order and orientation, so its stress is k I (to the float64 rounding of
+    // those vectors' orthonormality, below float precision): the second
+    // decomposition is not needed
+    tau = m3zero<float>();
+    tau.m[0][0] = tau.m[1][1] = tau.m[2][2] = k[0];
+    return;
+  }
   double s2[3];
   svd3F64(Fn, U, s2, V);
   const double kd[3] = {double(k[0]), double(k[1]), double(k[2])};
