@@ -1,5 +1,6 @@
-"""bench.py's reference arm (the CPU oracle, no GPU needed) prints one JSON line
-with the keys the measurement contract asks for."""
+"""bench.py's reference arm (the reference's shaders compiled for the CPU, or
+the CPU oracle where that library is absent; no GPU needed) prints one JSON
+line with the keys the measurement contract asks for."""
 import json
 import os
 import subprocess
@@ -20,5 +21,6 @@ def test_reference_arm_prints_the_contract_line():
         assert k in line, k
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
     assert line["config"]["workload"] == "slope_flow_1m_256"
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    from oracle import ref as R
+    assert line["cpu_baseline"]["kind"] == ("reference" if R.available() else "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
