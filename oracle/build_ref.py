@@ -20,7 +20,8 @@ Every rewrite below is mechanical and changes no arithmetic:
 * the bindless ``buffers[]`` declaration and ``layout(local_size_x = ...) in;``
   are dropped (``glsl_env.hpp`` declares the buffer table), and the push-constant block becomes a struct of the same
   layout (188 bytes, asserted);
-* ``out`` / ``inout`` parameters become C++ references;
+* ``out`` / ``inout`` parameters become C++ references (arrays: references
+  to arrays);
 * unsuffixed floating literals get an ``f`` (GLSL floating literals are
   float);
 * ``.xyz`` becomes ``.xyz()`` (the only swizzle the shaders use);
@@ -37,7 +38,9 @@ type numbers and variable lists out of ``Force.h``.
 
 The three hash-scan shaders use workgroup shared memory and barriers; the
 dispatcher restates them (``ref_dispatch.cpp``), keeping their single
-1024-wide global scan.
+1024-wide global scan.  The PBF engine's spatial hash (``hash_count.comp``,
+``hash_sort.comp`` on ``common.glsl``) is built the same way, for the checker
+of ``nebula_hash_bin``.
 """
 from __future__ import annotations
 
@@ -65,8 +68,13 @@ SHADERS = {
     "mpm_grid_update.comp": True,
     "mpm_nanovdb_bc.comp": True,
     "mpm_g2p.comp": True,
+    # the PBF engine's spatial hash (Engine's hash build), on common.glsl's SimPC
+    "hash_count.comp": False,
+    "hash_sort.comp": False,
 }
-INCLUDES = ("mpm_common.glsl", "collider_common.glsl", "force_common.glsl", "force_noise.glsl")
+INCLUDES = ("mpm_common.glsl", "collider_common.glsl", "force_common.glsl", "force_noise.glsl", "common.glsl")
+# push-constant block sizes: MPMSimPC (mpm_common.glsl) and SimPC (common.glsl)
+PC_BYTES = {"mpm": 188, "hash": 200}
 
 _FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
 
@@ -84,6 +92,7 @@ def rewrite(src: str) -> str:
     src = re.sub(r"layout\s*\([^)]*\)\s*buffer\s+\w+\s*\{[^}]*\}\s*buffers\s*\[\s*\]\s*;", "", src)
     src = re.sub(r"layout\s*\([^)]*\)\s*in\s*;", "", src)
     src = re.sub(r"layout\s*\(\s*push_constant\s*\)\s*uniform\s+(\w+)", r"struct \1", src)
+    src = re.sub(r"\b(?:inout|out)\s+(\w+)\s+(\w+)\s*\[(\d+)\]", r"\1 (&\2)[\3]", src)
     src = re.sub(r"\b(?:inout|out)\s+(\w+)\s+(\w+)", r"\1& \2", src)
     src = re.sub(r"\bvoid\s+main\s*\(\s*\)", "void shader_main(uvec3 gl_GlobalInvocationID)", src)
     src = _FLOAT_LIT.sub(r"\1f", src)
@@ -148,7 +157,7 @@ WRAPPER = """// generated by oracle/build_ref.py from the reference's %(shader)s
 #include "glsl_compat.hpp"
 namespace %(ns)s {
 #include "%(shader)s.hpp"
-static_assert(sizeof(PC) == 188, "MPMSimPC push-constant layout");
+static_assert(sizeof(PC) == %(pcbytes)d, "push-constant layout");
 }  // namespace %(ns)s
 extern "C" void ref_run_%(ns)s(const void* pc, uint32_t count, int threads) {
   __builtin_memcpy(&%(ns)s::pc, pc, sizeof(%(ns)s::pc));
@@ -172,7 +181,7 @@ def generate(reference: Path) -> list:
         ns = shader.split(".")[0]
         w = GEN / ("ref_%s.cpp" % ns)
         pragma = "#pragma omp parallel for schedule(dynamic, 4096) num_threads(threads > 0 ? threads : 1)\n" if independent else ""
-        w.write_text(WRAPPER % {"shader": shader, "ns": ns, "pragma": pragma})
+        w.write_text(WRAPPER % {"shader": shader, "ns": ns, "pragma": pragma, "pcbytes": PC_BYTES[ns.split("_")[0]]})
         wrappers.append(w)
     return wrappers
 

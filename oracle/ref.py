@@ -2,8 +2,9 @@
 
 ctypes driver of ``oracle/_ref/libref_mpm.so`` (built by ``oracle/build_ref.py``
 from the reference's shader sources).  ``RefShaders`` has the per-pass
-interface of ``oracle.Oracle`` so a test can run one pass of each on the same
-inputs and compare; only ``tests/`` and ``bench.py --impl reference`` use it.
+interface of ``oracle.Oracle`` and ``hash_bin`` the interface of
+``oracle.hash_bin``, so a test can run each on the same inputs and compare;
+only ``tests/`` and ``bench.py --impl reference`` use them.
 """
 from __future__ import annotations
 
@@ -56,6 +57,7 @@ def lib():
             ("ref_g2p", [vp]),
             ("ref_substep", [vp]),
             ("ref_run", [vp, C.c_uint32]),
+            ("ref_hash_bin", [vp, vp, C.c_uint32, vp, C.c_float, vp, C.c_uint32, vp, vp, vp]),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -171,3 +173,20 @@ class RefShaders:
 
     def run(self, nsub: int):
         self._L.ref_run(self._h, nsub)
+
+
+def hash_bin(pred_p, type_flag, world_min, cell_size: float, grid_res, hash_cells: int, sorted_init=0xFFFFFFFF):
+    """The PBF engine's spatial hash run through the reference's own
+    hash_count.comp / hash_sort.comp: (cellCount, cellOffset = range ends,
+    sortedIdx), with the arguments and results of ``oracle.hash_bin``."""
+    p = np.ascontiguousarray(pred_p, np.float32).reshape(-1, 4)
+    n = p.shape[0]
+    tf = None if type_flag is None else np.ascontiguousarray(type_flag, np.uint32)
+    wm = np.ascontiguousarray(world_min, np.float32)
+    gr = np.ascontiguousarray(grid_res, np.uint32)
+    cnt = np.empty(int(hash_cells), np.uint32)
+    off = np.empty(int(hash_cells), np.uint32)
+    srt = np.full(n, sorted_init, np.uint32)
+    lib().ref_hash_bin(_ptr(p), None if tf is None else _ptr(tf), n, _ptr(wm), C.c_float(cell_size), _ptr(gr), int(hash_cells),
+                       _ptr(cnt), _ptr(off), _ptr(srt))
+    return cnt, off, srt

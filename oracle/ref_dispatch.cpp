@@ -12,6 +12,9 @@
 // hash count and hash sort always run in order, so within a cell the sorted
 // list is in ascending particle index).
 //
+// The PBF engine's spatial hash (hash_count.comp, hash_sort.comp) runs through
+// ref_hash_bin with the same scan.
+//
 // Two passes are restated here rather than compiled, because they use
 // workgroup shared memory and barriers: zero_cells.comp:11-15 (a fill) and the
 // three hash-scan shaders (hash_scan_local.comp:12-43, hash_scan_global.comp:
@@ -36,6 +39,8 @@ void ref_run_mpm_p2g(const void*, uint32_t, int);
 void ref_run_mpm_grid_update(const void*, uint32_t, int);
 void ref_run_mpm_nanovdb_bc(const void*, uint32_t, int);
 void ref_run_mpm_g2p(const void*, uint32_t, int);
+void ref_run_hash_count(const void*, uint32_t, int);
+void ref_run_hash_sort(const void*, uint32_t, int);
 }
 
 namespace {
@@ -62,6 +67,39 @@ struct SimPC {
 static_assert(sizeof(SimPC) == 188, "MPMSimPC layout");
 static_assert(offsetof(SimPC, gridRes) == 64 && offsetof(SimPC, worldMax) == 96 && offsetof(SimPC, forceCount) == 184,
               "MPMSimPC offsets");
+
+// SimPC (common.glsl:11-65), 200 bytes: the PBF engine's push constants, of
+// which the spatial hash reads the words set in hashPC() below.
+struct HashPC {
+  uint32_t w[50];
+};
+
+// hash_scan_local.comp:12-43, hash_scan_global.comp:14-34 and
+// hash_add_base.comp:12-22 over `NC` cells: offset[0, NC) gets each cell's
+// exclusive prefix inside its group of 256 plus the group's base, where the
+// bases are the exclusive prefix of the first 1024 group totals and, for any
+// later group, its own total (the single 1024-invocation global scan);
+// offset[NC, NC + groups) holds the bases.
+void scanCells(const uint32_t* count, uint32_t* offset, uint32_t NC) {
+  const uint32_t NG = (NC + 255u) / 256u;
+  for (uint32_t g = 0; g < NG; ++g) {
+    uint32_t acc = 0;
+    for (uint32_t l = 0; l < 256u; ++l) {
+      const uint32_t gid = g * 256u + l;
+      const uint32_t val = gid < NC ? count[gid] : 0u;
+      if (gid < NC) offset[gid] = acc;
+      acc += val;
+    }
+    offset[NC + g] = acc;
+  }
+  uint32_t acc = 0;
+  for (uint32_t l = 0; l < 1024u && l < NG; ++l) {
+    const uint32_t t = offset[NC + l];
+    offset[NC + l] = acc;
+    acc += t;
+  }
+  for (uint32_t c = 0; c < NC; ++c) offset[c] += offset[NC + c / 256u];
+}
 
 // Bindless slots (index 0 stays unbound: a 0 index means "none" to the shaders).
 enum Slot : uint32_t {
@@ -174,33 +212,9 @@ struct RefScene {
   void bin() {
     bind();
     SimPC c = pc();
-    const uint32_t NC = p.hashCells, NG = nGroups();
     std::fill(cellCount.begin(), cellCount.end(), 0u);  // zero_cells.comp:11-15
     ref_run_mpm_hash_count(&c, N, 1);
-    // hash_scan_local.comp:12-43: per group of 256 cells an inclusive scan;
-    // the exclusive value to each cell, the group total to cellOffset[NC + g].
-    for (uint32_t g = 0; g < NG; ++g) {
-      uint32_t acc = 0;
-      for (uint32_t l = 0; l < 256u; ++l) {
-        const uint32_t gid = g * 256u + l;
-        const uint32_t val = gid < NC ? cellCount[gid] : 0u;
-        if (gid < NC) cellOffset[gid] = acc;
-        acc += val;
-      }
-      cellOffset[NC + g] = acc;
-    }
-    // hash_scan_global.comp:14-34: one workgroup of 1024 invocations scans the
-    // first 1024 group totals and writes their exclusive prefix back.
-    {
-      uint32_t acc = 0;
-      for (uint32_t l = 0; l < 1024u && l < NG; ++l) {
-        const uint32_t s = cellOffset[NC + l];
-        cellOffset[NC + l] = acc;
-        acc += s;
-      }
-    }
-    // hash_add_base.comp:12-22
-    for (uint32_t cc = 0; cc < NC; ++cc) cellOffset[cc] += cellOffset[NC + cc / 256u];
+    scanCells(cellCount.data(), cellOffset.data(), p.hashCells);
     ref_run_mpm_hash_sort(&c, N, 1);
   }
 
@@ -325,6 +339,45 @@ void ref_g2p(void* h) { static_cast<RefScene*>(h)->g2p(); }
 void ref_substep(void* h) { static_cast<RefScene*>(h)->substep(); }
 void ref_run(void* h, uint32_t nsub) {
   for (uint32_t i = 0; i < nsub; ++i) static_cast<RefScene*>(h)->substep();
+}
+
+// The PBF engine's spatial hash over predicted positions (n float4; typeFlag
+// n words or null for all 0): zero cells, hash_count.comp, the three scan
+// passes, hash_sort.comp.  cellCount / cellOffset get hashCells words
+// (offsets: range ends, as the sort leaves them); sortedIdx comes in with the
+// caller's fill and gets the sorted list in its first n words.
+void ref_hash_bin(const float* predP4, const uint32_t* typeFlag, uint32_t n, const float* worldMin, float cellSize,
+                  const uint32_t* gridRes, uint32_t hashCells, uint32_t* cellCount, uint32_t* cellOffset,
+                  uint32_t* sortedIdx) {
+  const uint32_t NG = (hashCells + 255u) / 256u;
+  std::vector<uint32_t> pred(size_t(n) * 4 + 4, 0u), flags(size_t(n) + 1, 0u), cnt(size_t(hashCells) + 1, 0u),
+      off(size_t(hashCells) + NG + 1, 0u), srt(size_t(n) * 2 + 1, 0u);
+  std::memcpy(pred.data(), predP4, size_t(n) * 16);
+  if (typeFlag) std::memcpy(flags.data(), typeFlag, size_t(n) * 4);
+  std::memcpy(srt.data(), sortedIdx, size_t(n) * 4);
+  enum : uint32_t { kPred = 1, kFlags, kCount, kOffset, kSortedIdx };
+  buffers[kPred].data = pred.data();
+  buffers[kFlags].data = flags.data();
+  buffers[kCount].data = cnt.data();
+  buffers[kOffset].data = off.data();
+  buffers[kSortedIdx].data = srt.data();
+  HashPC c{};
+  c.w[2] = kPred;        // predPIdx
+  c.w[4] = kFlags;       // typeFlagIdx
+  c.w[5] = kCount;       // cellCountIdx
+  c.w[6] = kOffset;      // cellOffsetIdx
+  c.w[7] = kSortedIdx;   // sortedIdxIdx
+  c.w[8] = n;            // particleCount
+  c.w[9] = hashCells;    // hashCells
+  std::memcpy(&c.w[13], &cellSize, 4);
+  std::memcpy(&c.w[16], gridRes, 12);
+  std::memcpy(&c.w[20], worldMin, 12);
+  ref_run_hash_count(&c, n, 1);
+  scanCells(cnt.data(), off.data(), hashCells);
+  ref_run_hash_sort(&c, n, 1);
+  std::memcpy(cellCount, cnt.data(), size_t(hashCells) * 4);
+  std::memcpy(cellOffset, off.data(), size_t(hashCells) * 4);
+  std::memcpy(sortedIdx, srt.data(), size_t(n) * 4);
 }
 
 }  // extern "C"

@@ -8,7 +8,8 @@ of MPMEngine::step.  These tests run that build and the oracle in its "ref32"
 mode on the same seeded inputs and require the results to be identical bit
 for bit: binning, P2G, grid update with forces / colliders / dense SDF, G2P
 for every material model of the reference under APIC, PIC and FLIP (with the
-J-reset and the SDF push-out taken), and multi-substep trajectories.  They
+J-reset and the SDF push-out taken), multi-substep trajectories, and the
+PBF engine's spatial hash (hash_count.comp / hash_sort.comp).  They
 pin the oracle -- the checker of every GPU parity test -- to the reference's
 code itself.  They need no GPU; they are skipped only where neither the
 reference tree nor an earlier build of the library is present.
@@ -197,6 +198,29 @@ def test_substep_pass_by_pass_identical(model, mname, flip, tname):
     for x in (o, r):
         x.g2p()
     assert_same_state(o, r, mname + " " + tname)
+
+
+# ----------------------------------------------------------------------------- PBF spatial hash
+def test_pbf_hash_identical():
+    """The PBF engine's spatial hash (hash_count.comp, the scan passes,
+    hash_sort.comp) against the oracle that checks nebula_hash_bin: a
+    hand-worked case, the fluid layout with its unused slots (type flag 6),
+    and a non-cubic offset grid with particles outside it.  Bit-exact."""
+    from nebula_b200 import hash as H
+    hand = np.array([[0.5, 0.5, 0.5, 1], [1.5, 0.2, 0.1, 1], [0.1, 1.9, 0.0, 1], [1.2, 1.2, 1.2, 1], [0.3, 0.3, 0.3, 0],
+                     [-5.0, 9.0, 0.7, 1], [0.9, 0.1, 0.2, 1], [5.0, 5.0, 5.0, 1]], np.float32)
+    cases = [(hand, np.array([0, 0, 3, 0, 6, 0, 3, 0], np.uint32), (0, 0, 0), 1.0, (2, 2, 2), 8)]
+    p, f = H.fluid_layout()
+    g = H.FluidGrid()
+    cases.append((p, f, g.world_min, g.cell_size, g.grid_res, g.hash_cells))
+    rng = np.random.default_rng(3)
+    g = H.FluidGrid(domain_size=(3.0, 1.0, 2.0), cell_size=0.05, world_min=(-1.0, 0.5, 2.0))
+    q = np.zeros((20000, 4), np.float32)
+    q[:, :3] = rng.uniform(-0.2, 1.2, (20000, 3)) * np.array(g.domain_size) + np.array(g.world_min)
+    cases.append((q, None, g.world_min, g.cell_size, g.grid_res, g.hash_cells))
+    for args in cases:
+        for a, b, name in zip(oracle.hash_bin(*args), R.hash_bin(*args), ("cellCount", "cellOffset", "sortedIdx")):
+            assert np.array_equal(a, b), name
 
 
 # ----------------------------------------------------------------------------- trajectories
