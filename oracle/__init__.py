@@ -13,6 +13,11 @@ and drives it through ctypes.  Modes:
 * ``"mixed"`` -- float state, float64 SVD/stress inside the plastic return
   maps (the CUDA path's precision policy);
 * ``"fp64"``  -- float64 everywhere (error statements, finite differences).
+
+``ref32`` is pinned bit for bit to the reference's own shaders compiled for
+the CPU (``oracle/build_ref.py``, driven by ``oracle/ref.py``;
+``tests/test_ref_shaders.py`` and the golden vectors of
+``tests/golden/ref_shader_fixtures.npz``).
 """
 from __future__ import annotations
 

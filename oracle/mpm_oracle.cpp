@@ -31,6 +31,11 @@
 // (including svd3 writing singular vectors into U[.][i]/V[.][i], i.e. as rows of
 // the GLSL matrix, which the Hencky and return-map products then consume).
 //
+// In "ref32" mode every pass reproduces, bit for bit, the reference's own shaders
+// compiled for the CPU by oracle/build_ref.py (tests/test_ref_shaders.py; golden
+// vectors from that build in tests/golden/ref_shader_fixtures.npz), with the one
+// intended difference named above: the exclusive scan over any number of cells.
+//
 // Precision modes (template parameters R = state/arithmetic type, RP = type of
 // the SVD + stress inside the VON_MISES / DRUCKER_PRAGER / MUD return maps):
 //   0 "ref32"  R=float,  RP=float   -- the shaders' own precision
