@@ -200,6 +200,68 @@ def test_substep_pass_by_pass_identical(model, mname, flip, tname):
     assert_same_state(o, r, mname + " " + tname)
 
 
+# ----------------------------------------------------------------------------- edge cases
+def test_empty_scene_identical():
+    """No particles: every pass runs over an empty set and leaves an empty grid."""
+    sc = S.elastic_block()
+    empty = {f: np.zeros((0, 4), np.float32) for f in oracle.FIELDS}
+    o, r = pair(sc.params, empty)
+    for x in (o, r):
+        x.run(2)
+    assert_same_grid(o, r, "empty")
+    for a, b in zip(o.get_bins(), r.get_bins()):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("model,mname", MODELS, ids=[m for _, m in MODELS])
+def test_global_parameters_without_a_material_table(model, mname):
+    """materialCount 0: P2G takes rho0 and G2P takes mu, lambda, the plastic
+    model, M, q_c and q_max from the push constants (mpm_g2p.comp:139-149,
+    mpm_p2g.comp:50-55); bulkK and the viscosity are then 0."""
+    sc = S.shear_block(model)
+    sp = sc.params
+    sp.materials = []
+    sp.plastic_model = model
+    sp.mu_lame, sp.lambda_lame = S.lame(3e4, 0.3)
+    sp.M_friction, sp.q_cohesion, sp.q_max = 0.6, 5.0, 150.0
+    sp.rho0 = 1200.0
+    o, r = pair(sp, sc.state)
+    o.run(12)
+    r.run(12)
+    assert_same_state(o, r, "global " + mname)
+
+
+def test_material_ids_past_the_table_are_clamped():
+    """Ids at and past the table's end read its last entry (min(id, count - 1))."""
+    sc = S.shear_block(S.MAT_ELASTIC)
+    sc.params.materials = sc.params.materials + [S.preset_mud()]
+    ids = np.arange(sc.state["P"].shape[0], dtype=np.uint32) % 5  # 0..4 over a table of 2
+    sc.state["v"][:, 3] = ids.view(np.float32)
+    o, r = pair(sc.params, sc.state)
+    o.run(10)
+    r.run(10)
+    assert_same_state(o, r, "clamped ids")
+
+
+def test_walls_and_world_clamp_identical():
+    """Particles in the two-node wall band of all six faces and past the
+    1.5-cell margin, moving outward: the grid's wall band and G2P's world
+    clamp (mpm_grid_update.comp:54-60, mpm_g2p.comp:255-263)."""
+    sc = S.shear_block(S.MAT_DRUCKER_PRAGER)
+    rng = np.random.default_rng(5)
+    n = sc.state["P"].shape[0]
+    P, v = sc.state["P"], sc.state["v"]
+    face = rng.integers(0, 6, n)
+    axis, side = face // 2, face % 2
+    depth = rng.uniform(-0.02, 0.04, n).astype(np.float32)  # some past the domain
+    P[np.arange(n), axis] = np.where(side == 0, depth, 1.0 - depth).astype(np.float32)
+    v[np.arange(n), axis] = np.where(side == 0, -3.0, 3.0).astype(np.float32)
+    o, r = pair(sc.params, sc.state)
+    o.run(8)
+    r.run(8)
+    assert_same_state(o, r, "walls")
+
+
 # ----------------------------------------------------------------------------- PBF spatial hash
 def test_pbf_hash_identical():
     """The PBF engine's spatial hash (hash_count.comp, the scan passes,
