@@ -219,7 +219,7 @@ def cpu_reference(sc):
     threads = oracle.num_threads()
     try:
         from oracle import ref as R
-        if R.available():
+        if R.available(prebuilt=True):
             r = R.RefShaders(threads)
             r.set_params(sc.params)
             r.set_sdf(sc.sdf)

@@ -19,8 +19,12 @@ from .build_ref import DEFAULT_REFERENCE, LIB, build
 _lib = None
 
 
-def available(reference: Path = DEFAULT_REFERENCE) -> bool:
-    """True when the library exists or can be built from the reference tree."""
+def available(reference: Path = DEFAULT_REFERENCE, prebuilt: bool = False) -> bool:
+    """True when the library exists or can be built from the reference tree
+    (with ``prebuilt``: only when it exists; the reference tree is not looked
+    at)."""
+    if prebuilt:
+        return LIB.exists()
     try:
         return build(reference) is not None
     except Exception:
@@ -30,7 +34,7 @@ def available(reference: Path = DEFAULT_REFERENCE) -> bool:
 def lib():
     global _lib
     if _lib is None:
-        path = build()
+        path = LIB if LIB.exists() else build()
         if path is None:
             raise RuntimeError("reference shader library not built and the reference tree is absent")
         L = C.CDLL(str(path))

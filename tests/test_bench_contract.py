@@ -22,5 +22,5 @@ def test_reference_arm_prints_the_contract_line():
     assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
     assert line["config"]["workload"] == "slope_flow_1m_256"
     from oracle import ref as R
-    assert line["cpu_baseline"]["kind"] == ("reference" if R.available() else "port") and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["kind"] == ("reference" if R.available(prebuilt=True) else "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
