@@ -212,21 +212,23 @@ def cpu_reference(sc):
     """The CPU implementation of the reference's substep on this host: its own
     MPM shaders compiled for the CPU (``oracle/_ref``, built by
     ``oracle/build_ref.py``; the independent per-invocation passes spread over
-    the host threads) when that library is present, else the CPU oracle that
-    restates them (identical results, ``tests/test_ref_shaders.py``).
+    the host threads; the binning's scan passes give the exclusive prefix they
+    intend, so that the trajectory is a correct one at any grid size) when that
+    library is present, else the CPU oracle that restates them (identical
+    results, ``tests/test_ref_shaders.py``).
     Returns (runner, kind, threads, description)."""
     import oracle
     threads = oracle.num_threads()
     try:
         from oracle import ref as R
         if R.available(prebuilt=True):
-            r = R.RefShaders(threads)
+            r = R.RefShaders(threads, intended_scan=True)
             r.set_params(sc.params)
             r.set_sdf(sc.sdf)
             r.set_state(sc.state)
-            return r, "reference", threads, ("the reference's MPM shaders compiled for the CPU (oracle/_ref), OpenMP; "
-                                             "above 262,144 cells its one-workgroup global scan leaves wrong cell offsets, "
-                                             "so it times the reference's passes, not a correct trajectory")
+            return r, "reference", threads, ("the reference's MPM shaders compiled for the CPU (oracle/_ref), OpenMP, "
+                                             "with the binning scan's intended exclusive prefix (the reference's "
+                                             "one-workgroup global scan is wrong above 262,144 cells)")
     except OSError:
         pass
     o = oracle.Oracle("ref32")

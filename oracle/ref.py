@@ -44,6 +44,7 @@ def lib():
         for name, args in [
             ("ref_destroy", [vp]),
             ("ref_set_threads", [vp, C.c_int]),
+            ("ref_set_intended_scan", [vp, C.c_int]),
             ("ref_set_params", [vp, vp]),
             ("ref_set_tables", [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32]),
             ("ref_set_sdf", [vp, vp]),
@@ -76,12 +77,16 @@ def _ptr(a: np.ndarray):
 
 class RefShaders:
     """One scene run through the reference's shaders on the CPU (float32, as
-    the shaders compute)."""
+    the shaders compute).  ``intended_scan``: the binning's scan passes give
+    the plain exclusive prefix over any number of cells, as they intend (the
+    reference's own single 1024-wide global scan is wrong above 262,144
+    cells); every compiled shader is unchanged either way."""
 
-    def __init__(self, threads: int = 1):
+    def __init__(self, threads: int = 1, intended_scan: bool = False):
         self._L = lib()
         self._h = self._L.ref_create()
         self._L.ref_set_threads(self._h, threads)
+        self._L.ref_set_intended_scan(self._h, int(intended_scan))
         self.n = 0
         self.nc = 0
         self._keep = []

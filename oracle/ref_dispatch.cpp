@@ -80,7 +80,10 @@ struct HashPC {
 // bases are the exclusive prefix of the first 1024 group totals and, for any
 // later group, its own total (the single 1024-invocation global scan);
 // offset[NC, NC + groups) holds the bases.
-void scanCells(const uint32_t* count, uint32_t* offset, uint32_t NC) {
+// With `intended`, every group's base is the exclusive prefix of all group
+// totals: the plain exclusive scan the three passes mean to compute, which
+// they give for up to 1024 groups.
+void scanCells(const uint32_t* count, uint32_t* offset, uint32_t NC, bool intended = false) {
   const uint32_t NG = (NC + 255u) / 256u;
   for (uint32_t g = 0; g < NG; ++g) {
     uint32_t acc = 0;
@@ -93,7 +96,7 @@ void scanCells(const uint32_t* count, uint32_t* offset, uint32_t NC) {
     offset[NC + g] = acc;
   }
   uint32_t acc = 0;
-  for (uint32_t l = 0; l < 1024u && l < NG; ++l) {
+  for (uint32_t l = 0; l < NG && (intended || l < 1024u); ++l) {
     const uint32_t t = offset[NC + l];
     offset[NC + l] = acc;
     acc += t;
@@ -131,6 +134,7 @@ struct RefScene {
   ref_params p{};
   uint32_t N = 0;
   int threads = 1;
+  bool intendedScan = false;
   bool hasSdf = false;
   std::vector<uint32_t> attr[8];  // pos, vel, F0, F1, F2, B0, B1, B2: 4 words per particle
   std::vector<uint32_t> cellCount, cellOffset, sorted, materials, colliders, forces, sdf, gridMom, gridMass;
@@ -214,7 +218,7 @@ struct RefScene {
     SimPC c = pc();
     std::fill(cellCount.begin(), cellCount.end(), 0u);  // zero_cells.comp:11-15
     ref_run_mpm_hash_count(&c, N, 1);
-    scanCells(cellCount.data(), cellOffset.data(), p.hashCells);
+    scanCells(cellCount.data(), cellOffset.data(), p.hashCells, intendedScan);
     ref_run_mpm_hash_sort(&c, N, 1);
   }
 
@@ -255,6 +259,10 @@ extern "C" {
 void* ref_create(void) { return new RefScene(); }
 void ref_destroy(void* h) { delete static_cast<RefScene*>(h); }
 void ref_set_threads(void* h, int n) { static_cast<RefScene*>(h)->threads = n > 0 ? n : 1; }
+// 1: the scan passes give the plain exclusive prefix over any number of
+// groups (their intended result; the MPM binning of the oracle and of the
+// CUDA path); 0 (default): exactly the reference's single 1024-wide global scan.
+void ref_set_intended_scan(void* h, int on) { static_cast<RefScene*>(h)->intendedScan = on != 0; }
 
 void ref_set_params(void* h, const ref_params* p) {
   RefScene& s = *static_cast<RefScene*>(h);

@@ -200,6 +200,25 @@ def test_substep_pass_by_pass_identical(model, mname, flip, tname):
     assert_same_state(o, r, mname + " " + tname)
 
 
+@pytest.mark.parametrize("key,nsub", [("cfg2", 20), ("cfg3", 3)], ids=["cfg2_multimaterial_80k_128", "cfg3_slope_1m_256"])
+def test_configurations_above_1024_scan_groups_with_the_intended_scan(key, nsub):
+    """The two-material scene on 128^3 and the benched slope (1M particles on
+    256^3 over the terrain SDF) through every compiled shader, with the scan
+    passes giving the exclusive prefix they intend: identical to the oracle
+    bit for bit, so at these sizes the oracle differs from the reference's
+    shaders only by the scan's 1024-group limit."""
+    sc = S.load_config(key)
+    o = oracle.Oracle("ref32")
+    r = R.RefShaders(8, intended_scan=True)
+    for x in (o, r):
+        x.set_params(sc.params)
+        x.set_sdf(sc.sdf)
+        x.set_state(sc.state)
+    o.run(nsub)
+    r.run(nsub)
+    assert_same_state(o, r, key)
+
+
 # ----------------------------------------------------------------------------- edge cases
 def test_empty_scene_identical():
     """No particles: every pass runs over an empty set and leaves an empty grid."""
